@@ -1,0 +1,395 @@
+"""Generate golden fixtures by running the reference's OWN Python source
+(dasfadwqd/LBDEM-Taichi, read from /root/reference) under the NumPy Taichi
+stand-in in ``tishim.py``.
+
+Usage (in a container that has the reference checkout):
+    python tests/golden/make_golden.py [/root/reference]
+
+Every scenario writes ``tests/golden/<name>.npz``.  Inputs are seeded; all
+arrays keep the reference's own shapes ((Nx, Ny, Nz[, k]) for lattice fields,
+(n, ...) for particle fields).
+
+Two reference routines are replaced by vectorised equivalents because a
+Python-loop emulation of them over the reference's 2^20-entry hash table
+would take minutes per DEM sub-step; both replacements compute identical
+integers:
+  * ``BPCD._setup_collision`` (bpcd.py:105-112): clear the table, then count
+    particles per hash cell -- the count loop still calls the reference's own
+    ``hash_codef``;
+  * ``PrefixSumExecutor.parallel_fast`` (prefixsum.py:62-84): exclusive scan.
+Everything else (mapping, collision, streaming, force reduction, contact
+search, contact laws, walls, integration) is the reference's code as written.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import tishim  # noqa: E402
+
+ti = tishim.install()
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, REF)
+
+from src.lbm3d.lbm_solver3d import BasicLattice3D  # noqa: E402
+from src.lbm3d.lbm_foecelover import ForcedLattice3D  # noqa: E402
+from src.lbm3d.lbmutils import CellType  # noqa: E402
+from src.lbdem.psclattice3d import PSCLattice3D  # noqa: E402
+from src.hybridlbdem.hybridlattice import HybridLattice3D  # noqa: E402
+from src.dem3d.demsolver import DEMSolver  # noqa: E402
+from src.dem3d.demconfig import (DEMSolverConfig, DomainBounds,  # noqa: E402
+                                 HertzContactConfig, LinearContactConfig)
+from src.dem3d.bpcd import BPCD, PrefixSumExecutor  # noqa: E402
+
+Vector3 = ti.types.vector(3, float)
+
+
+# ---------------------------------------------------------------------------
+# vectorised stand-ins for the two table-sized loops (identical integers)
+# ---------------------------------------------------------------------------
+def _setup_collision_fast(self, positions):
+    ht = self.hash_table
+    ht.offset.arr[...] = 0
+    ht.current.arr[...] = 0
+    ht.count.arr[...] = 0
+    for i in positions:
+        self._count_particles(positions[i])
+
+
+def _parallel_fast(self, output, input, cal_total=False):
+    a = input.arr.astype(np.int64)
+    ex = np.concatenate([[0], np.cumsum(a)[:-1]])
+    output.arr[...] = ex
+    if cal_total:
+        return int(ex[-1] + a[-1])
+
+
+BPCD._setup_collision = _setup_collision_fast
+PrefixSumExecutor.parallel_fast = _parallel_fast
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def write_p4p(path, radius, mass, pos, vel):
+    """Reference p4p format: single spaces, 1-based IDs (demsolver.py:160-177)."""
+    n = len(radius)
+    with open(path, "w") as fp:
+        fp.write("TIMESTEP  PARTICLES\n")
+        fp.write(f"0 {n}\n")
+        fp.write("ID  GROUP  RAD  MASS  PX  PY  PZ  VX  VY  VZ\n")
+        for i in range(n):
+            fp.write(" ".join([str(i + 1), "0", repr(float(radius[i])), repr(float(mass[i])),
+                               repr(float(pos[i, 0])), repr(float(pos[i, 1])), repr(float(pos[i, 2])),
+                               repr(float(vel[i, 0])), repr(float(vel[i, 1])), repr(float(vel[i, 2]))])
+                     + "\n")
+
+
+def make_dem(domain, dt, gravity, contact, radius, density, pos, vel, omega=None,
+             periodic=(False, False, False), E=1e5, nu=0.3, wall_E=1e5, wall_nu=0.3,
+             max_coord=16, model="hertz", freeze=None):
+    mass = density * 4.0 / 3.0 * np.pi * radius ** 3
+    cfg = DEMSolverConfig(domain=DomainBounds(*domain), dt=dt, gravity=Vector3(*gravity),
+                          contact_model=contact)
+    cfg.set_particle_properties(elastic_modulus=E, poisson_ratio=nu, max_coordinate_number=max_coord)
+    cfg.set_wall_properties(elastic_modulus=wall_E, poisson_ratio=wall_nu, density=density)
+    cfg.set_periodic_boundaries(*periodic)
+    fd, path = tempfile.mkstemp(suffix=".p4p")
+    os.close(fd)
+    write_p4p(path, radius, mass, pos, vel)
+    dem = DEMSolver(cfg)
+    dmin = Vector3(domain[0], domain[2], domain[4])
+    dmax = Vector3(domain[1], domain[3], domain[5])
+    dem.init_particle_fields(path, dmin, dmax)
+    os.remove(path)
+    dem.set_contact_model(model)
+    if omega is not None:
+        dem.gf.omega.from_numpy(omega)
+    if freeze is not None:
+        dem.gf.freeze.from_numpy(np.asarray(freeze, dtype=np.int64))
+    return dem
+
+
+def set_walls_z(lattice):
+    ct = lattice.CT.arr
+    ct[:, :, 0] = CellType.OBSTACLE
+    ct[:, :, -1] = CellType.OBSTACLE
+
+
+def random_flow(lattice, rng, amp_u, amp_rho):
+    nx, ny, nz = lattice.Nx, lattice.Ny, lattice.Nz
+    lattice.vel.arr[...] = amp_u * rng.uniform(-1, 1, (nx, ny, nz, 3))
+    lattice.rho.arr[...] = 1.0 + amp_rho * rng.uniform(-1, 1, (nx, ny, nz))
+
+
+def dem_state(dem):
+    gf = dem.gf
+    return {k: getattr(gf, k).to_numpy() for k in (
+        "position", "velocity", "acceleration", "force", "quaternion", "omega",
+        "omega_dot", "moment", "force_fluid", "moment_fluid")}
+
+
+def dem_contacts(dem):
+    cf = dem.cf
+    act = cf.isActive.to_numpy().astype(bool)
+    pairs = np.stack([cf.i.to_numpy()[act], cf.j.to_numpy()[act]], 1) if act.any() else np.zeros((0, 2), int)
+    shear = cf.shear_displacement.to_numpy()[act]
+    wact = dem.wcf.isActive.to_numpy().astype(bool)
+    wshear = dem.wcf.shear_displacement.to_numpy()
+    return pairs, shear, wact, wshear
+
+
+def save(name, **arrs):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrs)
+    print(f"wrote {path}: {sorted(arrs)}")
+
+
+# ---------------------------------------------------------------------------
+# scenarios
+# ---------------------------------------------------------------------------
+def scen_bgk_smag():
+    """BasicLattice3D.collide (Smagorinsky, lbm_solver3d.py:176-192) + stream."""
+    rng = np.random.default_rng(11)
+    nx, ny, nz = 10, 8, 7
+    lat = BasicLattice3D(nx, ny, nz, 1.0 / 0.6, 1.0, 1.0, 1.0)
+    set_walls_z(lat)
+    random_flow(lat, rng, 0.05, 0.01)
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy())
+    lat.initialize()
+    out = {}
+    for s in range(3):
+        lat.collide()
+        out[f"omega_{s}"] = lat.omega.to_numpy()
+        lat.stream()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save("bgk_smag", omega0=np.float64(1.0 / 0.6), cs=np.float64(BasicLattice3D.SmagorinskyConstant),
+         nsteps=np.int64(3), **init, **out)
+
+
+def scen_forced():
+    """ForcedLattice3D.collide (lbm_foecelover.py:52-68) + stream."""
+    rng = np.random.default_rng(12)
+    nx, ny, nz = 9, 8, 8
+    F = (1e-3, -2e-3, 5e-4)
+    lat = ForcedLattice3D(nx, ny, nz, 1.0 / 0.7, 1.0, 1.0, 1.0, Vector3(*F))
+    set_walls_z(lat)
+    random_flow(lat, rng, 0.02, 0.005)
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy())
+    lat.initialize()
+    out = {}
+    for s in range(3):
+        lat.collide()
+        lat.stream()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save("forced", omega0=np.float64(1.0 / 0.7), force=np.array(F), nsteps=np.int64(3), **init, **out)
+
+
+def _psc_particles(dx, xmin):
+    # lattice-unit centres (xc as defined at psclattice3d.py:102-104) -> physical
+    xc = np.array([[5.3, 5.1, 4.7],     # G0: large, has fully covered cells
+                   [9.4, 6.2, 5.5],     # G1: partial overlap with G0 -> winner rule
+                   [10.0, 3.0, 2.2],    # G2: near the z=0 wall
+                   [6.2, 5.6, 5.0]])    # G3: overlaps G0 heavily -> full/full ties
+    rad_lu = np.array([3.2, 2.1, 2.6, 2.4])
+    pos = (xc - 0.5) * dx + xmin
+    return pos, rad_lu * dx
+
+
+def scen_psc():
+    """PSCLattice3D collide (psclattice3d.py:187-358) + stream, physical units."""
+    rng = np.random.default_rng(13)
+    nx, ny, nz = 14, 12, 10
+    dx, dt, rho_phys = 1e-3, 2e-4, 1000.0
+    xmin = np.array([0.0, 0.0, 0.0])
+    pos, rad = _psc_particles(dx, xmin)
+    n = len(rad)
+    vel = 1e-3 * rng.uniform(-1, 1, (n, 3))
+    omg = 0.5 * rng.uniform(-1, 1, (n, 3))
+    domain = (0.0, (nx - 2) * dx, 0.0, (ny - 2) * dx, 0.0, (nz - 2) * dx)
+    dem = make_dem(domain, dt / 5, (0, 0, -9.81), HertzContactConfig(0.3, 0.3, 0.9, 0.9),
+                   rad, 2500.0, pos, vel, omega=omg)
+    lat = PSCLattice3D(nx, ny, nz, 1.0 / 0.65, dx, dt, rho_phys, dem)
+    set_walls_z(lat)
+    random_flow(lat, rng, 0.01, 0.002)
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy(),
+                gpos=pos, grad=rad, gvel=vel, gomega=omg, dx=dx, dt=dt, rho_unit=rho_phys,
+                domain=np.array(domain))
+    lat.initialize()
+    out = dict(id_init=lat.id.to_numpy(), volfrac_init=lat.volfrac.to_numpy(),
+               weight_init=lat.weight.to_numpy(), velsolid_init=lat.velsolid.to_numpy())
+    for s in range(3):
+        lat.collide()
+        for k in ("id", "volfrac", "weight", "velsolid", "hydroforce"):
+            out[f"{k}_{s}"] = getattr(lat, k).to_numpy()
+        out[f"force_fluid_{s}"] = dem.gf.force_fluid.to_numpy()
+        out[f"moment_fluid_{s}"] = dem.gf.moment_fluid.to_numpy()
+        lat.stream()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save("psc", omega0=np.float64(1.0 / 0.65), nsteps=np.int64(3), **init, **out)
+
+
+def scen_hybrid():
+    """HybridLattice3D with coarse grains only = PSC + Smagorinsky
+    (hybridlattice.py:433-503), lattice units."""
+    rng = np.random.default_rng(14)
+    nx, ny, nz = 14, 12, 10
+    dx = dt = rho_phys = 1.0
+    xmin = np.zeros(3)
+    pos, rad = _psc_particles(dx, xmin)
+    n = len(rad)
+    vel = 2e-3 * rng.uniform(-1, 1, (n, 3))
+    omg = 1e-3 * rng.uniform(-1, 1, (n, 3))
+    domain = (0.0, nx - 2.0, 0.0, ny - 2.0, 0.0, nz - 2.0)
+    dem = make_dem(domain, 0.1, (0, 0, -1e-5), HertzContactConfig(0.3, 0.3, 0.9, 0.9),
+                   rad, 2.5, pos, vel, omega=omg)
+    lat = HybridLattice3D(nx, ny, nz, 1.0 / 0.6, dx, dt, rho_phys, dem)
+    set_walls_z(lat)
+    random_flow(lat, rng, 0.04, 0.005)
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy(),
+                gpos=pos, grad=rad, gvel=vel, gomega=omg, domain=np.array(domain))
+    lat.initialize_complete()
+    out = {}
+    for s in range(3):
+        lat.prepare_step()
+        lat.collide()
+        out[f"omega_{s}"] = lat.omega.to_numpy()
+        out[f"weight_{s}"] = lat.coarse_weight.to_numpy()
+        out[f"id_{s}"] = lat.coarse_id.to_numpy()
+        out[f"volfrac_{s}"] = lat.coarse_volfrac.to_numpy()
+        out[f"hydroforce_{s}"] = lat.hydroforce.to_numpy()
+        lat.stream()
+        lat.lattice2grains()
+        out[f"force_fluid_{s}"] = dem.gf.force_fluid.to_numpy()
+        out[f"moment_fluid_{s}"] = dem.gf.moment_fluid.to_numpy()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save("hybrid", omega0=np.float64(1.0 / 0.6), cs=np.float64(BasicLattice3D.SmagorinskyConstant),
+         nsteps=np.int64(3), **init, **out)
+
+
+def _dem_particles(rng):
+    """12 spheres in a 40x30x30 box: approaching pairs, an initially overlapping
+    pair, wall contacts, and one pair that touches only across the periodic x
+    boundary (never proposed by the reference broad phase)."""
+    pos = np.array([
+        [10.0, 10.0, 10.0], [14.9, 10.2, 10.1],    # approaching pair
+        [20.0, 20.0, 6.0], [24.4, 20.5, 6.4],      # overlapping pair
+        [30.0, 8.0, 2.52],                         # on the z=0 wall
+        [5.0, 27.4, 15.0],                         # near y=max wall
+        [1.2, 15.0, 20.0], [38.6, 15.1, 20.2],     # touching across periodic x
+        [15.0, 20.0, 20.0], [15.0, 24.7, 20.3],    # approaching pair (y)
+        [30.0, 22.0, 22.0], [34.6, 22.0, 26.0],
+    ])
+    rad = np.array([2.5, 2.4, 2.2, 2.3, 2.5, 2.6, 1.8, 1.9, 2.4, 2.3, 2.0, 2.7])
+    vel = 0.02 * rng.uniform(-1, 1, (12, 3))
+    vel[0] = [0.05, 0.0, 0.0]
+    vel[1] = [-0.05, 0.0, 0.0]
+    vel[4] = [0.0, 0.0, -0.03]
+    vel[5] = [0.0, 0.04, 0.0]
+    vel[8] = [0.0, 0.04, 0.01]
+    vel[9] = [0.0, -0.04, 0.0]
+    omg = 0.05 * rng.uniform(-1, 1, (12, 3))
+    return pos, rad, vel, omg
+
+
+def _scen_dem(name, contact, model, seed):
+    rng = np.random.default_rng(seed)
+    pos, rad, vel, omg = _dem_particles(rng)
+    domain = (0.0, 40.0, 0.0, 30.0, 0.0, 30.0)
+    dem = make_dem(domain, 0.05, (0.0, 0.0, -2e-3), contact, rad, 2.0, pos, vel, omega=omg,
+                   periodic=(True, False, False), E=1e3, nu=0.3, wall_E=2e3, wall_nu=0.25,
+                   model=model)
+    ff = 1e-3 * rng.uniform(-1, 1, (12, 3))
+    mf = 1e-3 * rng.uniform(-1, 1, (12, 3))
+    dem.gf.force_fluid.from_numpy(ff)
+    dem.gf.moment_fluid.from_numpy(mf)
+    init = dict(gpos=pos, grad=rad, gvel=vel, gomega=omg, force_fluid=ff, moment_fluid=mf,
+                domain=np.array(domain), dt=0.05, gravity=np.array([0.0, 0.0, -2e-3]),
+                periodic=np.array([1, 0, 0]), density=2.0, E=1e3, nu=0.3, wall_E=2e3, wall_nu=0.25,
+                max_coord=16, mass=dem.gf.mass.to_numpy(), table_size=dem.bpcd.hash_table.shape[0],
+                cell_size=dem.bpcd.cell_size)
+    out = {}
+    nsub = 60
+    for s in range(nsub):
+        dem.run_simulation()
+        if (s + 1) % 5 == 0:
+            st = dem_state(dem)
+            for k, v in st.items():
+                out[f"{k}_{s + 1}"] = v
+            pairs, shear, wact, wshear = dem_contacts(dem)
+            out[f"pairs_{s + 1}"] = pairs
+            out[f"shear_{s + 1}"] = shear
+            out[f"wact_{s + 1}"] = wact
+            out[f"wshear_{s + 1}"] = wshear
+    save(name, nsub=np.int64(nsub), **init, **out)
+
+
+def scen_dem_hertz():
+    _scen_dem("dem_hertz", HertzContactConfig(pp_friction=0.3, pw_friction=0.4,
+                                              pp_restitution=0.9, pw_restitution=0.8), "hertz", 21)
+
+
+def scen_dem_linear():
+    _scen_dem("dem_linear", LinearContactConfig(stiffness_normal=200.0, stiffness_tangential=100.0,
+                                                damping_normal=0.2, damping_tangential=0.1,
+                                                pp_friction=0.3, pw_friction=0.4), "linear", 22)
+
+
+def scen_coupled():
+    """Driver loop of single_particle_settle.py:230-241 (collide, stream,
+    DEM x subCycles) on a small box, lattice units, two spheres near the floor."""
+    rng = np.random.default_rng(31)
+    nx, ny, nz = 12, 12, 16
+    pos = np.array([[5.5, 5.6, 3.4], [6.1, 6.0, 9.2]])   # physical = lattice - 0.5 at xmin=0
+    rad = np.array([3.0, 2.6])
+    vel = np.array([[0.0, 0.0, -0.01], [0.002, 0.0, -0.02]])
+    omg = 1e-3 * rng.uniform(-1, 1, (2, 3))
+    domain = (0.0, nx - 2.0, 0.0, ny - 2.0, 0.0, nz - 2.0)
+    sub = 4
+    dem = make_dem(domain, 1.0 / sub, (0.0, 0.0, -1e-4), HertzContactConfig(0.3, 0.3, 0.9, 0.9),
+                   rad, 2.5, pos, vel, omega=omg, periodic=(True, True, False))
+    lat = PSCLattice3D(nx, ny, nz, 1.0 / 0.6, 1.0, 1.0, 1.0, dem)
+    set_walls_z(lat)
+    init = dict(ct=lat.CT.to_numpy(), gpos=pos, grad=rad, gvel=vel, gomega=omg,
+                domain=np.array(domain), sub=np.int64(sub), dt_dem=1.0 / sub,
+                gravity=np.array([0.0, 0.0, -1e-4]), density=2.5)
+    lat.initialize()
+    out = {}
+    nsteps = 4
+    for s in range(nsteps):
+        lat.collide()
+        lat.stream()
+        for _ in range(sub):
+            dem.run_simulation()
+        for k, v in dem_state(dem).items():
+            out[f"{k}_{s}"] = v
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+        out[f"id_{s}"] = lat.id.to_numpy()
+    out["f_last"] = lat.f.to_numpy()
+    save("coupled", omega0=np.float64(1.0 / 0.6), nsteps=np.int64(nsteps), **init, **out)
+
+
+SCENARIOS = {
+    "bgk_smag": scen_bgk_smag, "forced": scen_forced, "psc": scen_psc, "hybrid": scen_hybrid,
+    "dem_hertz": scen_dem_hertz, "dem_linear": scen_dem_linear, "coupled": scen_coupled,
+}
+
+if __name__ == "__main__":
+    names = sys.argv[2:] or list(SCENARIOS)
+    for nm in names:
+        SCENARIOS[nm]()
