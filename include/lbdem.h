@@ -1,0 +1,205 @@
+/*
+ * lbdem.h -- C ABI of the B200 (sm_100a) resolved LBM-DEM step library
+ * (liblbdem.so).  Plain pointers, sizes and POD descriptors; no torch types.
+ *
+ * Conventions
+ *  - Every entry point is asynchronous on the caller's CUDA stream (`stream`
+ *    is a cudaStream_t passed as void*; NULL = legacy default stream).
+ *  - The library never allocates or frees device memory: every buffer is
+ *    owned by the caller and passed in (the Python layer uses torch tensors).
+ *  - Return value: LBDEM_OK or an LBDEM_ERR_* code (argument/launch errors,
+ *    detected on the host).  Numerical/capacity faults found on the device are
+ *    OR-ed into a caller-provided int32 status word (LBDEM_ST_* bits) that the
+ *    caller reads at a synchronisation point of its choice.
+ *  - Lattice arrays are structure-of-arrays, x fastest: cell (x, y, z) ->
+ *    (z*Ny + y)*Nx + x; population q of a cell at q*Ncells + cell.
+ *    (The reference's Taichi fields are indexed [i, j, k] = [x, y, z].)
+ *  - Populations are stored as deviations from the lattice weights,
+ *    d_q = f_q - w_q (FP32 form), or h_q = (f_q - w_q) * scale16 / w_q
+ *    (FP16 / BF16 forms); arithmetic is FP32 in every form.
+ *  - Particle (DEM) state is FP64, array-of-structures (n, 3) like the
+ *    reference's Grain fields.
+ *
+ * Reference interfaces replaced (dasfadwqd/LBDEM-Taichi):
+ *  lbdem_lattice_init     <- PSCLattice3D.initialize      src/lbdem/psclattice3d.py:60-78
+ *  lbdem_psc_map          <- PSCLattice3D.grains2lattice  src/lbdem/psclattice3d.py:84-182
+ *  lbdem_psc_step_*       <- PSCLattice3D.collide + BasicLattice3D.stream
+ *                            src/lbdem/psclattice3d.py:187-358,
+ *                            src/lbm3d/lbm_solver3d.py:176-342,460-513,
+ *                            src/lbm3d/lbm_foecelover.py:52-68
+ *  lbdem_stream_moments_* <- BasicLattice3D.stream (+compute_rho_vel)
+ *                            src/lbm3d/lbm_solver3d.py:197-303
+ *  lbdem_psc_decode       <- PSCLattice3D fields id/volfrac/weight/velsolid
+ *                            src/lbdem/psclattice3d.py:45-52
+ *  lbdem_dem_bin,
+ *  lbdem_dem_substeps     <- DEMSolver.run_simulation     src/dem3d/demsolver/demsolver.py:848-862
+ *                            (BPCD bpcd.py:67-152, resolve :638-740,
+ *                             resolve_wall :809-838, update :514-636,
+ *                             hertz.py:45-153, linear.py:43-152)
+ *  lbdem_build_links      <- CellType dispatch in BasicLattice3D.stream
+ *                            src/lbm3d/lbm_solver3d.py:203-236
+ *  lbdem_global_sums_f64  <- (no counterpart; FP64 conservation totals)
+ */
+#ifndef LBDEM_H
+#define LBDEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBDEM_ABI_VERSION 1
+
+/* return codes */
+#define LBDEM_OK 0
+#define LBDEM_ERR_ARG 1
+#define LBDEM_ERR_LAUNCH 2
+#define LBDEM_ERR_UNSUPPORTED 3
+
+/* device status bits (OR-ed into *status) */
+#define LBDEM_ST_NAN 1u              /* non-finite population or moment */
+#define LBDEM_ST_RHO 2u              /* density <= 0 in a fluid cell */
+#define LBDEM_ST_VELMAX 4u           /* |u| >= sqrt(2/3) (lbm_solver3d.py:94,301) */
+#define LBDEM_ST_CONTACT_OVERFLOW 8u /* more contacts than max_coordinate_number */
+#define LBDEM_ST_GRID_OVERFLOW 16u   /* particle outside the broad-phase grid */
+#define LBDEM_ST_GID_OVERFLOW 32u    /* more than 2^24-1 particles in the PSC map */
+
+/* storage forms */
+#define LBDEM_F32 0
+#define LBDEM_F16 1
+#define LBDEM_BF16 2
+
+/* Smagorinsky modes */
+#define LBDEM_SMAG_OFF 0
+#define LBDEM_SMAG_REFERENCE 1 /* lagged: feq and omega of the previous collide (lbm_solver3d.py:460-513) */
+#define LBDEM_SMAG_LOCAL 2     /* current feq, omega0 prefactor; no per-cell state */
+
+/* CellType bits (src/lbm3d/lbmutils.py:69-97) */
+#define LBDEM_CT_FLUID 1
+#define LBDEM_CT_OBSTACLE 8
+#define LBDEM_CT_FREE_SLIP 16
+#define LBDEM_CT_VEL_LADD 32
+#define LBDEM_CT_VEL_ZOUHE 64
+#define LBDEM_CT_VEL_EXIT 128
+#define LBDEM_CT_PRE_ZOUHE 256
+#define LBDEM_CT_VEL_INLET_LADD 262144
+
+typedef struct lbdem_lattice {
+    int32_t nx, ny, nz;
+    int32_t storage;       /* LBDEM_F32 / LBDEM_F16 / LBDEM_BF16 */
+    float omega0;          /* 1/tau */
+    float smag_cs;         /* Smagorinsky constant */
+    int32_t smag_mode;     /* LBDEM_SMAG_* */
+    int32_t force_on;      /* 1: add w_q rho (c_q . F)/cs^2 to post-collision populations */
+    float force[3];        /* body force, lattice units */
+    float scale16;         /* storage scale of the 16-bit forms */
+    void *f[2];            /* population buffers, 19*Ncells elements of the storage type */
+    float *rho;            /* Ncells, FP32 (moments; also the initial state) */
+    float *vel;            /* 3*Ncells, FP32 SoA (ux | uy | uz) */
+    void *aux;             /* LBDEM_SMAG_REFERENCE: 5*Ncells of the storage type, else NULL */
+    const uint32_t *links; /* per-cell link mask from lbdem_build_links */
+    const uint8_t *row_simple; /* per (y,z) row: 1 = row and its 8 neighbour rows all plain FLUID */
+    int32_t *status;       /* device status word */
+} lbdem_lattice;
+
+typedef struct lbdem_grains {
+    int32_t n;
+    const double *pos;     /* (n,3) physical */
+    const double *radius;  /* (n) */
+    const double *vel;     /* (n,3) */
+    const double *omega;   /* (n,3) */
+    double *force_fluid;   /* (n,3) written by lbdem_psc_step_* (physical units) */
+    double *moment_fluid;  /* (n,3) */
+} lbdem_grains;
+
+typedef struct lbdem_psc {
+    double dx, dt, rho_unit;   /* UnitConverter(dx, dt, rho) */
+    double xmin, ymin, zmin;   /* DEM domain minimum (config.domain) */
+    int32_t skip_inlet;        /* 1: VEL_INLET_LADD cells are also skipped by the map */
+    uint32_t *key;             /* Ncells owner keys (0 = no solid) */
+    float *table;              /* 16*n floats per particle: floor(centre), frac(centre), v*dt/dx, omega*dt */
+    double *prev;              /* 4*n: lattice centre and mapping radius of the previous map */
+    int32_t have_prev;         /* 1: prev holds a map to clear */
+    float *hydro_out;          /* optional per-cell hydrodynamic force (3*Ncells) or NULL */
+} lbdem_psc;
+
+typedef struct lbdem_dem {
+    int32_t n, maxc;
+    int32_t model;                 /* 0 Hertz-Mindlin, 1 linear */
+    double dt, g[3];
+    double dom_min[3], dom_max[3]; /* config.domain */
+    int32_t periodic[3];
+    double bp_min[3];              /* broad-phase origin (init_particle_fields domain_min) */
+    double cell_size;              /* 4 * max radius (bpcd.py:42) */
+    int32_t gdim[3];               /* dense broad-phase grid, cells -1 .. gdim-2 per axis */
+    /* materials: [0] particles, [1] walls */
+    double E[2], nu[2], mu[2], e[2], kn[2], ks[2], dpn[2], dps[2];
+    double wall_n[18], wall_d[6];
+    int32_t wall_periodic[6];
+    /* grains (n,...) */
+    double *pos, *vel, *acc, *force, *quat, *omega, *omega_dot, *moment, *inertia, *mass, *radius;
+    double *force_fluid, *moment_fluid;
+    int32_t *freeze, *fixvel;
+    /* contacts: n*maxc slots owned by the lower index, wall contacts n*6 */
+    int32_t *cf_j, *cf_active, *cfn;
+    double *cf_shear, *cf_pos, *cf_force;
+    int32_t *wcf_active;
+    double *wcf_shear, *wcf_pos, *wcf_force;
+    /* broad-phase scratch (caller-owned) */
+    int32_t *cell_count;   /* 2 * prod(gdim), zero-initialised once */
+    int32_t *cell_start;   /* prod(gdim) */
+    int32_t *pcell;        /* n: cell of each particle */
+    int32_t *prank;        /* n: rank of the particle within its cell */
+    int32_t *sorted;       /* n: particle ids grouped by cell */
+    int32_t parity;        /* which half of cell_count holds the current binning */
+    int32_t *status;
+} lbdem_dem;
+
+int lbdem_abi_version(void);
+const char *lbdem_last_error(void);
+
+int lbdem_build_links(const int32_t *ct, int32_t nx, int32_t ny, int32_t nz, int32_t skip_inlet,
+                      uint32_t *links, uint8_t *row_simple, void *stream);
+
+int lbdem_lattice_init(const lbdem_lattice *L, int32_t buf, void *stream);
+
+int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G, void *stream);
+
+/* One fused pass: [stream of the pending post-collision populations in
+ * f[src] (gather=1) | read populations in place (gather=0)] -> moments ->
+ * Smagorinsky omega -> equilibrium -> PSC / BGK collision -> body force ->
+ * post-collision populations into f[dst]; hydrodynamic force and torque of
+ * every particle accumulated into G->force_fluid / G->moment_fluid
+ * (zeroed by lbdem_psc_map).  P/G may be NULL for a particle-free lattice. */
+int lbdem_psc_step_f32(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
+                       int32_t dst, int32_t gather, void *stream);
+int lbdem_psc_step_f16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
+                       int32_t dst, int32_t gather, void *stream);
+int lbdem_psc_step_bf16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
+                        int32_t dst, int32_t gather, void *stream);
+
+/* Stream the post-collision populations of f[src] into f[dst] and write
+ * rho/vel of FLUID cells (the reference's stream(), no collision). */
+int lbdem_stream_moments(const lbdem_lattice *L, int32_t src, int32_t dst, void *stream);
+
+/* Expand the owner keys into the reference's per-cell PSC fields. */
+int lbdem_psc_decode(const lbdem_lattice *L, const lbdem_psc *P, int32_t *id, float *volfrac,
+                     float *weight, float *velsolid, void *stream);
+
+int lbdem_dem_bin(lbdem_dem *D, void *stream);
+int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream);
+
+/* FP64 totals over the updated (non-skipped) cells of population buffer
+ * f[buf]: out[0] = sum of rho, out[1..3] = sum of momentum.  Valid in either
+ * state of the buffer (post-stream or post-collision: streaming conserves
+ * both).  `partials` is caller scratch of LBDEM_SUM_PARTIALS doubles. */
+#define LBDEM_SUM_BLOCKS 1184
+#define LBDEM_SUM_PARTIALS (4 * LBDEM_SUM_BLOCKS)
+int lbdem_global_sums_f64(const lbdem_lattice *L, int32_t buf, double *out, double *partials,
+                          void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBDEM_H */

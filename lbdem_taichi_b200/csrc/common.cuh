@@ -1,0 +1,86 @@
+// Shared device definitions: D3Q19 lattice, storage forms, link masks, errors.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/lbdem.h"
+
+namespace lbdem {
+
+// D3Q19 velocity set, weights and opposite directions
+// (src/lbm3d/lbm_solver3d.py:46-91: same ordering as the reference).
+constexpr int Q = 19;
+__host__ __device__ constexpr int cx(int q) {
+    return q == 1 || q == 7 || q == 9 || q == 11 || q == 13 ? 1
+         : q == 2 || q == 8 || q == 10 || q == 12 || q == 14 ? -1 : 0;
+}
+__host__ __device__ constexpr int cy(int q) {
+    return q == 3 || q == 7 || q == 10 || q == 15 || q == 17 ? 1
+         : q == 4 || q == 8 || q == 9 || q == 16 || q == 18 ? -1 : 0;
+}
+__host__ __device__ constexpr int cz(int q) {
+    return q == 5 || q == 11 || q == 14 || q == 15 || q == 18 ? 1
+         : q == 6 || q == 12 || q == 13 || q == 16 || q == 17 ? -1 : 0;
+}
+__host__ __device__ constexpr int qinv(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
+__host__ __device__ constexpr float wq(int q) {
+    return q == 0 ? 1.0f / 3.0f : (q <= 6 ? 1.0f / 18.0f : 1.0f / 36.0f);
+}
+constexpr float CS2 = 1.0f / 3.0f;
+
+// Per-cell link mask (built once from CellType by lbdem_build_links)
+constexpr uint32_t LINK_SKIP = 1u << 19;   // cell is not updated (OBSTACLE / VEL_LADD / FREE_SLIP [/ INLET])
+constexpr uint32_t LINK_FLUID = 1u << 20;  // FLUID: moments are recomputed
+constexpr uint32_t LINK_MAP_SKIP = 1u << 21;  // PSC map skips the cell
+__host__ __device__ constexpr uint32_t LINK_BB(int q) { return 1u << q; }  // neighbour x-c_q is OBSTACLE
+
+// Storage forms.  FP32 stores d = f - w; 16-bit forms store
+// h = (f - w) * scale / w (scale = scale16), decoded as d = h * w / scale.
+template <typename T> struct Store;
+template <> struct Store<float> {
+    static constexpr int kind = LBDEM_F32;
+    __device__ __forceinline__ static float dec(float v, float /*wscale*/) { return v; }
+    __device__ __forceinline__ static float enc(float d, float /*inv_wscale*/) { return d; }
+    __device__ __forceinline__ static float ld(const float *p) { return __ldg(p); }
+};
+template <> struct Store<__half> {
+    static constexpr int kind = LBDEM_F16;
+    __device__ __forceinline__ static float dec(__half v, float wscale) { return __half2float(v) * wscale; }
+    __device__ __forceinline__ static __half enc(float d, float inv_wscale) { return __float2half_rn(d * inv_wscale); }
+    __device__ __forceinline__ static __half ld(const __half *p) { return __ldg(p); }
+};
+template <> struct Store<__nv_bfloat16> {
+    static constexpr int kind = LBDEM_BF16;
+    __device__ __forceinline__ static float dec(__nv_bfloat16 v, float wscale) { return __bfloat162float(v) * wscale; }
+    __device__ __forceinline__ static __nv_bfloat16 enc(float d, float inv_wscale) {
+        return __float2bfloat16_rn(d * inv_wscale);
+    }
+    __device__ __forceinline__ static __nv_bfloat16 ld(const __nv_bfloat16 *p) { return __ldg(p); }
+};
+
+// Auxiliary (lagged Smagorinsky) state is kept in the population storage
+// type; 16-bit forms store it unscaled.
+template <typename T> __device__ __forceinline__ float aux_dec(T v);
+template <> __device__ __forceinline__ float aux_dec<float>(float v) { return v; }
+template <> __device__ __forceinline__ float aux_dec<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float aux_dec<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename T> __device__ __forceinline__ T aux_enc(float v);
+template <> __device__ __forceinline__ float aux_enc<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half aux_enc<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 aux_enc<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+// PSC owner key: full(1) | count(7) | (0xFFFFFF - gid)(24); atomicMax picks
+// the reference's winner (psclattice3d.py:100-138): lowest-id full cover,
+// else largest sub-sample count, ties to the lowest id.
+constexpr uint32_t KEY_FULL = 1u << 31;
+__host__ __device__ inline uint32_t key_gid(uint32_t k) { return 0xFFFFFFu - (k & 0xFFFFFFu); }
+__host__ __device__ inline int key_count(uint32_t k) { return (int)((k >> 24) & 0x7Fu); }
+
+// Host-side error reporting
+void set_error(const char *fmt, ...);
+int check_launch(const char *what);
+
+}  // namespace lbdem

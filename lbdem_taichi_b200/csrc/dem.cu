@@ -1,0 +1,555 @@
+// DEM sub-step on the GPU (DEMSolver.run_simulation, demsolver.py:848-862).
+//
+// Broad phase: the reference hashes cells of size 4*r_max with a Morton code
+// into a 2^20..2^22 table and probes each particle's own cell plus the seven
+// cells of its octant (bpcd.py:114-152), proposing pairs i < j.  Here the same
+// cells are kept in a dense grid (no hash), binned by a counting sort, and
+// probed with the same octant rule, which proposes the same pairs whenever
+// distinct cells do not alias in the reference's hash (checked on the host).
+//
+// Per sub-step: k_scan (one block: exclusive scan of the cell counts, scatter
+// the particle ids, clear force/moment), k_contacts (one thread per particle:
+// candidate pairs j > i with contact history owned by i, then the six walls),
+// k_integrate (body + fluid force, improved Verlet, quaternion update,
+// contact-list compaction, then bin the new positions for the next sub-step).
+// FP64 throughout; compiled with -fmad=false to follow the reference's
+// operation order (and the FP64 oracle) closely.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace lbdem {
+
+struct M3 {
+    double m[3][3];
+};
+
+__device__ __forceinline__ void cross3(const double *a, const double *b, double *o) {
+    const double t0 = a[1] * b[2] - a[2] * b[1], t1 = a[2] * b[0] - a[0] * b[2], t2 = a[0] * b[1] - a[1] * b[0];
+    o[0] = t0; o[1] = t1; o[2] = t2;
+}
+__device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+__device__ __forceinline__ void mv(const M3 &M, const double *v, double *o) {
+    double t[3];
+    for (int r = 0; r < 3; ++r) t[r] = M.m[r][0] * v[0] + M.m[r][1] * v[1] + M.m[r][2] * v[2];
+    o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
+}
+__device__ M3 inv3(const M3 &A) {
+    const double(*a)[3] = A.m;
+    const double det = a[0][0] * (a[1][1] * a[2][2] - a[2][1] * a[1][2]) -
+                       a[1][0] * (a[0][1] * a[2][2] - a[2][1] * a[0][2]) +
+                       a[2][0] * (a[0][1] * a[1][2] - a[1][1] * a[0][2]);
+    const double id = 1.0 / det;
+    M3 o;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            o.m[j][i] = id * (a[(i + 1) % 3][(j + 1) % 3] * a[(i + 2) % 3][(j + 2) % 3] -
+                              a[(i + 2) % 3][(j + 1) % 3] * a[(i + 1) % 3][(j + 2) % 3]);
+    return o;
+}
+
+// rotation taking unit vector a onto +x (demsolver.py:686-701, :757-773)
+__device__ M3 rot_to_x(const double *a) {
+    const double b[3] = {1.0, 0.0, 0.0};
+    double v[3];
+    cross3(a, b, v);
+    const double s = sqrt(dot3(v, v));
+    const double c = dot3(a, b);
+    M3 R;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) R.m[i][j] = 0.0;
+    if (s < 1e-12) {
+        if (c > 0.0) {
+            R.m[0][0] = R.m[1][1] = R.m[2][2] = 1.0;
+        } else {
+            R.m[0][0] = -1.0; R.m[1][1] = 1.0; R.m[2][2] = -1.0;
+        }
+    } else {
+        const double vx[3][3] = {{0.0, -v[2], v[1]}, {v[2], 0.0, -v[0]}, {-v[1], v[0], 0.0}};
+        const double coef = (1.0 - c) / (s * s);
+        for (int r = 0; r < 3; ++r)
+            for (int q = 0; q < 3; ++q) {
+                double acc = 0.0;
+                for (int t = 0; t < 3; ++t) acc += (coef * vx[r][t]) * vx[t][q];
+                R.m[r][q] = ((r == q ? 1.0 : 0.0) + vx[r][q]) + acc;
+            }
+    }
+    return R;
+}
+
+struct DemArgs {
+    lbdem_dem d;
+    int ncell;
+    int parity;
+};
+
+__device__ __forceinline__ int cell_index(const lbdem_dem &d, int cx_, int cy_, int cz_) {
+    // grid covers reference cells -1 .. gdim-2 per axis
+    const int gx = cx_ + 1, gy = cy_ + 1, gz = cz_ + 1;
+    if (gx < 0 || gy < 0 || gz < 0 || gx >= d.gdim[0] || gy >= d.gdim[1] || gz >= d.gdim[2]) return -1;
+    return (gz * d.gdim[1] + gy) * d.gdim[0] + gx;
+}
+
+__device__ __forceinline__ void ref_cell(const lbdem_dem &d, const double *p, int *ijk) {
+    // bpcd.py:191-194
+    for (int a = 0; a < 3; ++a) ijk[a] = (int)floor((p[a] - d.bp_min[a]) / d.cell_size);
+}
+
+__device__ __forceinline__ void bin_particle(const lbdem_dem &d, int i, int32_t *count) {
+    int ijk[3];
+    ref_cell(d, d.pos + 3 * i, ijk);
+    const int c = cell_index(d, ijk[0], ijk[1], ijk[2]);
+    if (c < 0) {
+        atomicOr(d.status, (int)LBDEM_ST_GRID_OVERFLOW);
+        d.pcell[i] = -1;
+        d.prank[i] = 0;
+        return;
+    }
+    d.pcell[i] = c;
+    d.prank[i] = atomicAdd(count + c, 1);
+}
+
+__global__ void k_bin(const __grid_constant__ DemArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.d.n) return;
+    bin_particle(A.d, i, A.d.cell_count + (size_t)A.parity * A.ncell);
+}
+
+// one block: exclusive scan of the cell counts, scatter ids, clear force/moment
+__global__ void __launch_bounds__(1024) k_scan(const __grid_constant__ DemArgs A) {
+    const lbdem_dem &d = A.d;
+    const int32_t *count = d.cell_count + (size_t)A.parity * A.ncell;
+    const int nt = blockDim.x, t = threadIdx.x;
+    const int per = (A.ncell + nt - 1) / nt;
+    const int b0 = min(A.ncell, t * per), b1 = min(A.ncell, b0 + per);
+    int local = 0;
+    for (int c = b0; c < b1; ++c) local += count[c];
+    __shared__ int sh[1024];
+    sh[t] = local;
+    __syncthreads();
+    for (int off = 1; off < nt; off <<= 1) {   // Hillis-Steele inclusive scan
+        const int v = t >= off ? sh[t - off] : 0;
+        __syncthreads();
+        sh[t] += v;
+        __syncthreads();
+    }
+    int run = sh[t] - local;
+    for (int c = b0; c < b1; ++c) {
+        d.cell_start[c] = run;
+        run += count[c];
+    }
+    __syncthreads();
+    for (int i = t; i < d.n; i += nt) {
+        const int c = d.pcell[i];
+        if (c >= 0) d.sorted[d.cell_start[c] + d.prank[i]] = i;
+        for (int a = 0; a < 3; ++a) d.force[3 * i + a] = d.moment[3 * i + a] = 0.0;   // clear_state :422-429
+    }
+}
+
+// ------------------------------- contact laws ------------------------------
+// hertz.py:45-97 / linear.py:43-101 (particle-particle), hertz.py:99-153 /
+// linear.py:103-152 (particle-wall).  `wall` selects the wall variant.
+__device__ void contact_force(const lbdem_dem &d, int i, int j, bool wall, double *shear, double delta_n,
+                              const double *vc, double *F) {
+    const double gap = -1 * delta_n;
+    const double dt = d.dt;
+    double inc[3] = {vc[0] * dt, vc[1] * dt, vc[2] * dt};
+    inc[0] = 0.0;
+    double kt, gt, F0, mu;
+    const int tj = wall ? 1 : 0;
+    if (d.model == 0) {
+        const double Ys = 1.0 / ((1.0 - d.nu[0] * d.nu[0]) / d.E[0] + (1.0 - d.nu[tj] * d.nu[tj]) / d.E[tj]);
+        const double Gs = 1.0 / (2.0 * (2.0 - d.nu[0]) * (1.0 + d.nu[0]) / d.E[0] +
+                                 2.0 * (2.0 - d.nu[tj]) * (1.0 + d.nu[tj]) / d.E[tj]);
+        double Rs, ms, e;
+        if (wall) {
+            Rs = d.radius[i];
+            ms = d.mass[i];
+            e = d.e[1];
+            mu = d.mu[1];
+        } else {
+            Rs = 1.0 / (1.0 / d.radius[i] + 1.0 / d.radius[j]);
+            ms = 1.0 / (1.0 / d.mass[i] + 1.0 / d.mass[j]);
+            e = 0.5 * (d.e[0] + d.e[0]);
+            mu = 0.5 * (d.mu[0] + d.mu[0]);
+        }
+        const double lne = log(e);
+        const double beta = lne / sqrt(lne * lne + M_PI * M_PI);
+        const double Sn = 2.0 * Ys * sqrt(Rs * delta_n);
+        const double St = 8.0 * Gs * sqrt(Rs * delta_n);
+        const double kn = 4.0 / 3.0 * Ys * sqrt(Rs * delta_n);
+        const double gn = -2.0 * beta * sqrt(5.0 / 6.0 * Sn * ms);
+        kt = 8.0 * Gs * sqrt(Rs * delta_n);
+        gt = -2.0 * beta * sqrt(5.0 / 6.0 * St * ms);
+        F0 = -kn * gap - gn * vc[0];
+    } else {
+        double kns, kss, dpn, dps, ms;
+        if (wall) {
+            kns = d.kn[0]; kss = d.ks[0]; dpn = d.dpn[0]; dps = d.dps[0];
+            ms = d.mass[i];
+            mu = d.mu[1];
+        } else {
+            kns = d.kn[0] * d.kn[0] / (d.kn[0] + d.kn[0]);
+            kss = d.ks[0] * d.ks[0] / (d.ks[0] + d.ks[0]);
+            dpn = 0.5 * (d.dpn[0] + d.dpn[0]);
+            dps = 0.5 * (d.dps[0] + d.dps[0]);
+            ms = 1.0 / (1.0 / d.mass[i] + 1.0 / d.mass[j]);
+            mu = 0.5 * (d.mu[0] + d.mu[0]);
+        }
+        const double Cn = 2. * dpn * sqrt(kns * ms);
+        const double Ct = 2. * dps * sqrt(kns * ms);
+        kt = kss;
+        gt = Ct;
+        F0 = -kns * gap - Cn * vc[0];
+    }
+    for (int a = 0; a < 3; ++a) shear[a] += inc[a];
+    const double ts[3] = {-kt * shear[0], -kt * shear[1], -kt * shear[2]};
+    const double tl = sqrt(dot3(ts, ts));
+    F[0] = F0;
+    if (tl >= mu * F0 && tl > 0.0) {
+        const double ratio = mu * F0 / tl;
+        F[1] = ts[1] * ratio;
+        F[2] = ts[2] * ratio;
+        shear[1] = -F[1] / kt;
+        shear[2] = -F[2] / kt;
+    } else {
+        F[1] = ts[1] - gt * vc[1];
+        F[2] = ts[2] - gt * vc[2];
+    }
+}
+
+__device__ __forceinline__ void periodic_delta(const lbdem_dem &d, const double *pi, const double *pj, double *dv) {
+    // demsolver.py:483-512
+    for (int a = 0; a < 3; ++a) {
+        dv[a] = pj[a] - pi[a];
+        if (d.periodic[a]) {
+            const double L = d.dom_max[a] - d.dom_min[a];
+            if (dv[a] > 0.5 * L) dv[a] -= L;
+            else if (dv[a] < -0.5 * L) dv[a] += L;
+        }
+    }
+}
+
+// resolve(i, j) (demsolver.py:638-740); forces on i accumulated in Fi/Mi,
+// forces on j added atomically.
+__device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, double *Mi_acc) {
+    const size_t base = (size_t)i * d.maxc;
+    int n_i = d.cfn[i];
+    int off = -1;
+    for (int o = 0; o < n_i && o < d.maxc; ++o)
+        if (d.cf_j[base + o] == j && d.cf_active[base + o]) {
+            off = o;
+            break;
+        }
+    double dv[3];
+    periodic_delta(d, d.pos + 3 * i, d.pos + 3 * j, dv);
+    const double distance = sqrt(dot3(dv, dv));
+    const double gap = distance - d.radius[i] - d.radius[j];
+    bool eval = false;
+    if (off >= 0) {
+        if (gap < 0) eval = true;
+        else d.cf_active[base + off] = 0;
+    } else if (gap < 0) {
+        if (n_i >= d.maxc) {
+            atomicOr(d.status, (int)LBDEM_ST_CONTACT_OVERFLOW);
+            return;
+        }
+        off = n_i;
+        d.cfn[i] = n_i + 1;
+        d.cf_j[base + off] = j;
+        d.cf_active[base + off] = 1;
+        for (int a = 0; a < 3; ++a)
+            d.cf_shear[3 * (base + off) + a] = d.cf_pos[3 * (base + off) + a] = d.cf_force[3 * (base + off) + a] = 0.0;
+        eval = true;
+    }
+    if (!eval) return;
+    const size_t s = base + off;
+    const double len = sqrt(dot3(dv, dv));
+    const double a[3] = {dv[0] / len, dv[1] / len, dv[2] / len};
+    const M3 R = rot_to_x(a);
+    const double delta_n = -gap;
+    const double *pi = d.pos + 3 * i;
+    double cp[3], ri[3], rj[3];
+    for (int t = 0; t < 3; ++t) {
+        cp[t] = pi[t] + a[t] * (d.radius[i] - delta_n);
+        d.cf_pos[3 * s + t] = cp[t];
+    }
+    for (int t = 0; t < 3; ++t) {
+        ri[t] = cp[t] - pi[t];
+        rj[t] = cp[t] - (pi[t] + dv[t]);
+    }
+    double vci[3], vcj[3], dvc[3], vc[3];
+    cross3(d.omega + 3 * i, ri, vci);
+    cross3(d.omega + 3 * j, rj, vcj);
+    for (int t = 0; t < 3; ++t) {
+        vci[t] += d.vel[3 * i + t];
+        vcj[t] += d.vel[3 * j + t];
+        dvc[t] = vcj[t] - vci[t];
+    }
+    mv(R, dvc, vc);
+    double sh[3] = {d.cf_shear[3 * s], d.cf_shear[3 * s + 1], d.cf_shear[3 * s + 2]};
+    double F[3];
+    contact_force(d, i, j, false, sh, delta_n, vc, F);
+    for (int t = 0; t < 3; ++t) {
+        d.cf_shear[3 * s + t] = sh[t];
+        d.cf_force[3 * s + t] = F[t];
+    }
+    const M3 Ri = inv3(R);
+    const double mF[3] = {-F[0], -F[1], -F[2]};
+    double Fi[3], Fj[3], Mi[3], Mj[3];
+    mv(Ri, mF, Fi);
+    mv(Ri, F, Fj);
+    cross3(ri, Fi, Mi);
+    cross3(rj, Fj, Mj);
+    for (int t = 0; t < 3; ++t) {
+        Fi_acc[t] += Fi[t];
+        Mi_acc[t] += Mi[t];
+        atomicAdd(d.force + 3 * j + t, Fj[t]);
+        atomicAdd(d.moment + 3 * j + t, Mj[t]);
+    }
+}
+
+// evaluate_wall (demsolver.py:742-807)
+__device__ void wall_contact(const lbdem_dem &d, int i, int w, double *Fi_acc, double *Mi_acc) {
+    const double *nrm = d.wall_n + 3 * w;
+    const M3 R = rot_to_x(nrm);
+    const double *p = d.pos + 3 * i;
+    const double delta_n = (dot3(p, nrm) - d.wall_d[w]) + d.radius[i];
+    const double distance = d.radius[i] - delta_n;
+    const size_t s = (size_t)i * 6 + w;
+    double ri[3];
+    for (int t = 0; t < 3; ++t) {
+        ri[t] = distance * nrm[t];
+        d.wcf_pos[3 * s + t] = p[t] + ri[t];
+    }
+    double vci[3], m[3], vc[3];
+    cross3(d.omega + 3 * i, ri, vci);
+    for (int t = 0; t < 3; ++t) m[t] = -(vci[t] + d.vel[3 * i + t]);
+    mv(R, m, vc);
+    double sh[3] = {d.wcf_shear[3 * s], d.wcf_shear[3 * s + 1], d.wcf_shear[3 * s + 2]};
+    double F[3];
+    contact_force(d, i, -1, true, sh, delta_n, vc, F);
+    for (int t = 0; t < 3; ++t) {
+        d.wcf_shear[3 * s + t] = sh[t];
+        d.wcf_force[3 * s + t] = F[t];
+    }
+    const M3 Ri = inv3(R);
+    const double mF[3] = {-F[0], -F[1], -F[2]};
+    double Fi[3], Mi[3];
+    mv(Ri, mF, Fi);
+    cross3(ri, Fi, Mi);
+    for (int t = 0; t < 3; ++t) {
+        Fi_acc[t] += Fi[t];
+        Mi_acc[t] += Mi[t];
+    }
+}
+
+__global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArgs A) {
+    const lbdem_dem &d = A.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int32_t *count = d.cell_count + (size_t)A.parity * A.ncell;
+    double Fi[3] = {0.0, 0.0, 0.0}, Mi[3] = {0.0, 0.0, 0.0};
+    const double *o = d.pos + 3 * i;
+    int ijk[3], dd[3];
+    ref_cell(d, o, ijk);
+    for (int a = 0; a < 3; ++a) {
+        const double center = (ijk[a] + 0.5) * d.cell_size + d.bp_min[a];
+        dd[a] = (o[a] > center) ? 1 : -1;
+    }
+    // own cell + octant neighbours in the reference's probe order (bpcd.py:133-142)
+    const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 1, 1}};
+    for (int k = 0; k < 8; ++k) {
+        const int c = cell_index(d, ijk[0] + off[k][0] * dd[0], ijk[1] + off[k][1] * dd[1], ijk[2] + off[k][2] * dd[2]);
+        if (c < 0) continue;
+        const int n = count[c], s0 = d.cell_start[c];
+        for (int t = 0; t < n; ++t) {
+            const int j = d.sorted[s0 + t];
+            if (j > i) resolve_pair(d, i, j, Fi, Mi);
+        }
+    }
+    // resolve_wall (demsolver.py:809-838)
+    for (int w = 0; w < 6; ++w) {
+        if (d.wall_periodic[w]) continue;
+        const size_t s = (size_t)i * 6 + w;
+        const double sep = -(dot3(o, d.wall_n + 3 * w) - d.wall_d[w]);
+        if (d.wcf_active[s]) {
+            if (sep > d.radius[i]) d.wcf_active[s] = 0;
+            else wall_contact(d, i, w, Fi, Mi);
+        } else if (sep <= d.radius[i]) {
+            d.wcf_active[s] = 1;
+            for (int t = 0; t < 3; ++t) d.wcf_shear[3 * s + t] = d.wcf_pos[3 * s + t] = d.wcf_force[3 * s + t] = 0.0;
+            wall_contact(d, i, w, Fi, Mi);
+        }
+    }
+    for (int t = 0; t < 3; ++t) {
+        atomicAdd(d.force + 3 * i + t, Fi[t]);
+        atomicAdd(d.moment + 3 * i + t, Mi[t]);
+    }
+}
+
+// quaternion to rotation matrix (demsolver/utils.py:34-61)
+__device__ M3 quat2rot(const double *q) {
+    const double w2 = q[0] * q[0], i2 = q[1] * q[1], j2 = q[2] * q[2], k2 = q[3] * q[3];
+    const double twoij = 2.0 * q[1] * q[2], twoik = 2.0 * q[1] * q[3], twojk = 2.0 * q[2] * q[3];
+    const double twoiw = 2.0 * q[1] * q[0], twojw = 2.0 * q[2] * q[0], twokw = 2.0 * q[3] * q[0];
+    M3 r;
+    r.m[0][0] = w2 + i2 - j2 - k2; r.m[0][1] = twoij - twokw; r.m[0][2] = twojw + twoik;
+    r.m[1][0] = twoij + twokw; r.m[1][1] = w2 - i2 + j2 - k2; r.m[1][2] = twojk - twoiw;
+    r.m[2][0] = twoik - twojw; r.m[2][1] = twojk + twoiw; r.m[2][2] = w2 - i2 - j2 + k2;
+    return r;
+}
+
+__device__ void rotate_update(const lbdem_dem &d, int i) {
+    const double dt = d.dt;
+    const M3 Rm = quat2rot(d.quat + 4 * i);
+    M3 I;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) I.m[r][c] = d.inertia[9 * i + 3 * r + c];
+    double ml[3], wl[3], Iw[3], cw[3], rhs[3], wdl[3], alpha[3];
+    mv(Rm, d.moment + 3 * i, ml);
+    mv(Rm, d.omega + 3 * i, wl);
+    mv(I, wl, Iw);
+    cross3(wl, Iw, cw);
+    for (int t = 0; t < 3; ++t) rhs[t] = ml[t] - cw[t];
+    mv(inv3(I), rhs, wdl);
+    mv(inv3(Rm), wdl, alpha);
+    double *w = d.omega + 3 * i, *q = d.quat + 4 * i;
+    for (int t = 0; t < 3; ++t) w[t] += 0.5 * (d.omega_dot[3 * i + t] + alpha[t]) * dt;
+    const double dq0 = -0.5 * (q[1] * w[0] + q[2] * w[1] + q[3] * w[2]);
+    const double dq1 = +0.5 * (q[0] * w[0] - q[3] * w[1] + q[2] * w[2]);
+    const double dq2 = +0.5 * (q[3] * w[0] + q[0] * w[1] + q[1] * w[2]);
+    const double dq3 = +0.5 * (-q[2] * w[0] + q[1] * w[1] + q[0] * w[2]);
+    q[0] += dq0 * dt; q[1] += dq1 * dt; q[2] += dq2 * dt; q[3] += dq3 * dt;
+    const double ql = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for (int t = 0; t < 4; ++t) q[t] = q[t] / ql;
+    for (int t = 0; t < 3; ++t) d.omega_dot[3 * i + t] = alpha[t];
+}
+
+__device__ __forceinline__ void wrap_position(const lbdem_dem &d, double *p) {
+    // demsolver.py:451-480
+    for (int a = 0; a < 3; ++a) {
+        if (!d.periodic[a]) continue;
+        const double L = d.dom_max[a] - d.dom_min[a];
+        if (p[a] > d.dom_max[a]) p[a] = p[a] - L;
+        else if (p[a] < d.dom_min[a]) p[a] = p[a] + L;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemArgs A) {
+    const lbdem_dem &d = A.d;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    // clear the counts consumed by this sub-step (the other half receives the new binning)
+    int32_t *used = d.cell_count + (size_t)A.parity * A.ncell;
+    for (int c = tid; c < A.ncell; c += gridDim.x * blockDim.x) used[c] = 0;
+    const int i = tid;
+    if (i >= d.n) return;
+    const double dt = d.dt;
+    // apply_body_force (demsolver.py:437-448)
+    for (int t = 0; t < 3; ++t) {
+        d.force[3 * i + t] += d.mass[i] * d.g[t];
+        d.moment[3 * i + t] += 0.0;
+        d.force[3 * i + t] += d.force_fluid[3 * i + t];
+        d.moment[3 * i + t] += d.moment_fluid[3 * i + t];
+    }
+    // update (demsolver.py:514-636)
+    double *p = d.pos + 3 * i, *v = d.vel + 3 * i;
+    if (!d.freeze[i]) {
+        if (d.fixvel[i]) {
+            for (int t = 0; t < 3; ++t) p[t] += v[t] * dt;
+            wrap_position(d, p);
+            rotate_update(d, i);
+        } else {
+            double a[3];
+            for (int t = 0; t < 3; ++t) a[t] = d.force[3 * i + t] / d.mass[i];
+            for (int t = 0; t < 3; ++t) v[t] += 0.5 * (d.acc[3 * i + t] + a[t]) * dt;
+            for (int t = 0; t < 3; ++t) p[t] += v[t] * dt + 0.5 * a[t] * (dt * dt);
+            wrap_position(d, p);
+            for (int t = 0; t < 3; ++t) d.acc[3 * i + t] = a[t];
+            rotate_update(d, i);
+        }
+    }
+    // late_clear_state / remove_inactive_contact (demsolver.py:371-386, 431-436)
+    const size_t base = (size_t)i * d.maxc;
+    const int cnt = min(d.cfn[i], d.maxc);
+    int w = 0;
+    for (int o = 0; o < cnt; ++o) {
+        if (!d.cf_active[base + o]) continue;
+        if (w != o) {
+            const size_t dd = base + w, ss = base + o;
+            d.cf_j[dd] = d.cf_j[ss];
+            d.cf_active[dd] = 1;
+            for (int t = 0; t < 3; ++t) {
+                d.cf_shear[3 * dd + t] = d.cf_shear[3 * ss + t];
+                d.cf_pos[3 * dd + t] = d.cf_pos[3 * ss + t];
+                d.cf_force[3 * dd + t] = d.cf_force[3 * ss + t];
+            }
+        }
+        ++w;
+    }
+    for (int o = w; o < cnt; ++o) d.cf_active[base + o] = 0;
+    d.cfn[i] = w;
+    // bin the new position for the next sub-step
+    bin_particle(d, i, d.cell_count + (size_t)(A.parity ^ 1) * A.ncell);
+}
+
+static int check_dem(const lbdem_dem *D) {
+    if (!D || D->n < 0 || D->maxc < 0 || !D->status) {
+        set_error("dem: bad descriptor");
+        return LBDEM_ERR_ARG;
+    }
+    if (D->n > 0 && (!D->pos || !D->vel || !D->cell_count || !D->cell_start || !D->pcell || !D->prank ||
+                     !D->sorted || !D->cfn || !D->wcf_active)) {
+        set_error("dem: missing buffers");
+        return LBDEM_ERR_ARG;
+    }
+    if (D->gdim[0] <= 0 || D->gdim[1] <= 0 || D->gdim[2] <= 0 || !(D->cell_size > 0.0)) {
+        set_error("dem: bad broad-phase grid");
+        return LBDEM_ERR_ARG;
+    }
+    return LBDEM_OK;
+}
+
+}  // namespace lbdem
+
+using namespace lbdem;
+
+extern "C" {
+
+// (Re)bin the current positions into the active half of cell_count.
+int lbdem_dem_bin(lbdem_dem *D, void *stream) {
+    int rc = check_dem(D);
+    if (rc) return rc;
+    if (D->n == 0) return LBDEM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    DemArgs A;
+    A.d = *D;
+    A.ncell = D->gdim[0] * D->gdim[1] * D->gdim[2];
+    A.parity = D->parity;
+    if (cudaMemsetAsync(D->cell_count + (size_t)A.parity * A.ncell, 0, sizeof(int32_t) * A.ncell, st) != cudaSuccess)
+        return check_launch("dem_bin memset");
+    k_bin<<<(D->n + 127) / 128, 128, 0, st>>>(A);
+    return check_launch("dem_bin");
+}
+
+int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
+    int rc = check_dem(D);
+    if (rc) return rc;
+    if (D->n == 0 || nsub <= 0) return LBDEM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    DemArgs A;
+    A.d = *D;
+    A.ncell = D->gdim[0] * D->gdim[1] * D->gdim[2];
+    const int nb = (D->n + 127) / 128;
+    const int nb_int = max(nb, min(148, (A.ncell + 127) / 128));
+    for (int s = 0; s < nsub; ++s) {
+        A.parity = D->parity;
+        k_scan<<<1, 1024, 0, st>>>(A);
+        k_contacts<<<nb, 128, 0, st>>>(A);
+        k_integrate<<<nb_int, 128, 0, st>>>(A);
+        D->parity ^= 1;
+    }
+    return check_launch("dem_substeps");
+}
+
+}  // extern "C"

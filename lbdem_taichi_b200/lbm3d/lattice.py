@@ -1,0 +1,345 @@
+"""D3Q19 lattice on the GPU (API of src/lbm3d/lbm_solver3d.py:17-513 and
+src/lbm3d/lbm_foecelover.py:15-68).
+
+Device layout: populations f[buf][q][z][y][x] (x fastest) in two buffers of
+the storage type, stored as deviations from the lattice weights; macroscopic
+rho/u in FP32; per-cell link masks built once from CellType.  Python-scope
+field access uses the reference's index order [i, j, k] = [x, y, z] and
+shapes (Nx, Ny, Nz[, k]).
+
+Collide/stream: ``collide()`` launches ONE fused kernel that streams the
+pending post-collision populations (pull), takes moments, applies the
+collision and writes new post-collision populations; ``stream()`` only marks
+them as pending.  Reading populations or moments materialises the stream
+(one extra pass) so reads always see the reference's post-stream state.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from .. import _native as N
+from .lbmutils import CellType, UnitConverter
+
+_STORAGE = {"f32": (N.F32, torch.float32, 1.0), "f16": (N.F16, torch.float16, 4096.0),
+            "bf16": (N.BF16, torch.bfloat16, 1.0)}
+_SMAG = {"off": N.SMAG_OFF, "reference": N.SMAG_REFERENCE, "local": N.SMAG_LOCAL}
+_UNSUPPORTED = (CellType.FREE_SLIP | CellType.VEL_LADD | CellType.VEL_ZOUHE | CellType.VEL_EXIT
+                | CellType.Pre_ZOUHE | CellType.VEL_INLET_LADD | CellType.INTERFACE | CellType.GAS)
+
+W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+C_Q = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+                [1, 1, 0], [-1, -1, 0], [1, -1, 0], [-1, 1, 0], [1, 0, 1], [-1, 0, -1], [1, 0, -1],
+                [-1, 0, 1], [0, 1, 1], [0, -1, -1], [0, 1, -1], [0, -1, 1]], dtype=np.float64)
+QINV = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17])
+
+
+def to_ref(a):
+    """device order (..., z, y, x) -> reference order (x, y, z, ...)."""
+    a = np.asarray(a)
+    if a.ndim == 3:
+        return np.ascontiguousarray(a.transpose(2, 1, 0))
+    return np.ascontiguousarray(a.transpose(3, 2, 1, 0))
+
+
+def from_ref(a, comps=None):
+    a = np.asarray(a)
+    if comps is None:
+        return np.ascontiguousarray(a.transpose(2, 1, 0))
+    return np.ascontiguousarray(a.transpose(3, 2, 1, 0))
+
+
+class LatticeField:
+    """Reference-shaped view of one lattice field.
+
+    Element writes (``lattice.CT[i, j, k] = ...``) go to a host mirror and are
+    uploaded before the next kernel launch; reads download once and are served
+    from the mirror until the device changes the field.
+    """
+
+    def __init__(self, owner, name, shape, dtype, pull, push=None):
+        self._owner, self._name = owner, name
+        self._shape, self._dtype = shape, dtype
+        self._pull, self._push = pull, push
+        self._host = None
+        self._dirty = False
+
+    @property
+    def shape(self):
+        return self._shape
+
+    def _get_host(self):
+        if self._host is None:
+            self._host = np.asarray(self._pull(), dtype=self._dtype).reshape(self._shape)
+        return self._host
+
+    def invalidate(self):
+        if not self._dirty:
+            self._host = None
+
+    def to_numpy(self):
+        return self._get_host().copy()
+
+    def __getitem__(self, idx):
+        v = self._get_host()[idx]
+        return v.copy() if isinstance(v, np.ndarray) else v
+
+    def _writable(self):
+        if self._push is None:
+            raise AttributeError(f"field '{self._name}' is read-only")
+        h = self._get_host()
+        self._dirty = True
+        self._owner._host_dirty(self._name)
+        return h
+
+    def __setitem__(self, idx, v):
+        self._writable()[idx] = v
+
+    def fill(self, v):
+        self._writable()[...] = v
+
+    def from_numpy(self, a):
+        self._writable()[...] = np.asarray(a).reshape(self._shape)
+
+    def flush(self):
+        if self._dirty:
+            self._push(self._host)
+            self._dirty = False
+
+
+class LatticeEngine:
+    """Device state + kernels shared by BasicLattice3D / ForcedLattice3D / PSCLattice3D."""
+    D = 3
+    Q = 19
+    c = C_Q
+    w = W
+    qinv = QINV
+    cssq = 1.0 / 3.0
+    velmax = (2.0 / 3.0) ** 0.5
+    SmagorinskyConstant = 0.1
+
+    def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, smagorinsky="off", body_force=None,
+                 storage="f32", skip_inlet=True):
+        N.require_cuda()
+        if storage not in _STORAGE:
+            raise ValueError(f"storage must be one of {sorted(_STORAGE)}")
+        if smagorinsky not in _SMAG:
+            raise ValueError(f"smagorinsky must be one of {sorted(_SMAG)}")
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.omega0 = float(omega)
+        self.unit = UnitConverter(dx, dt, rho)
+        self.storage = storage
+        self.smagorinsky = smagorinsky
+        self.skip_inlet = skip_inlet
+        kind, tdtype, scale = _STORAGE[storage]
+        self._kind, self._tdtype, self._scale = kind, tdtype, scale
+        self.body_force = None if body_force is None else np.asarray(body_force, np.float64)
+        nc = self.Nx * self.Ny * self.Nz
+        self.ncells = nc
+        dev = "cuda"
+        self._f = [torch.zeros((19, nc), dtype=tdtype, device=dev) for _ in range(2)]
+        self._rho = torch.ones(nc, dtype=torch.float32, device=dev)
+        self._vel = torch.zeros((3, nc), dtype=torch.float32, device=dev)
+        self._aux = (torch.zeros((5, nc), dtype=tdtype, device=dev)
+                     if smagorinsky == "reference" else None)
+        self._links = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self._rows = torch.zeros(self.Ny * self.Nz, dtype=torch.uint8, device=dev)
+        self._ct_dev = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self._status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._sum_out = torch.zeros(4, dtype=torch.float64, device=dev)
+        self._sum_part = torch.zeros(N.SUM_PARTIALS, dtype=torch.float64, device=dev)
+        self._links_dirty = True
+        self._initialized = False
+        self._cur = 0
+        self._cur_kind = "f"
+        self._collided = None
+        self._macro_valid = True
+        self._host_ct = np.full((self.Nx, self.Ny, self.Nz), CellType.FLUID, np.int32)
+
+        shp = (self.Nx, self.Ny, self.Nz)
+        self.CT = LatticeField(self, "CT", shp, np.int32, lambda: self._host_ct, self._push_ct)
+        self.CT._host = self._host_ct
+        self.rho = LatticeField(self, "rho", shp, np.float64, self._pull_rho, self._push_rho)
+        self.vel = LatticeField(self, "vel", shp + (3,), np.float64, self._pull_vel, self._push_vel)
+        self.f = LatticeField(self, "f", shp + (19,), np.float64, self._pull_f)
+        self.omega = LatticeField(self, "omega", shp, np.float64, self._pull_omega)
+        self._lat = N.Lattice()
+        self._fill_desc()
+
+    # ------------------------------------------------------------ descriptor
+    def _fill_desc(self):
+        L = self._lat
+        L.nx, L.ny, L.nz = self.Nx, self.Ny, self.Nz
+        L.storage = self._kind
+        L.omega0 = self.omega0
+        L.smag_cs = float(type(self).SmagorinskyConstant)
+        L.smag_mode = _SMAG[self.smagorinsky]
+        if self.body_force is not None:
+            L.force_on = 1
+            L.force[:] = [float(v) for v in self.body_force]
+        else:
+            L.force_on = 0
+        L.scale16 = self._scale
+        L.f[0], L.f[1] = N.ptr(self._f[0]), N.ptr(self._f[1])
+        L.rho, L.vel = N.ptr(self._rho), N.ptr(self._vel)
+        L.aux = N.ptr(self._aux)
+        L.links, L.row_simple = N.ptr(self._links), N.ptr(self._rows)
+        L.status = N.ptr(self._status)
+
+    # ------------------------------------------------------------ host mirrors
+    def _host_dirty(self, name):
+        if name == "CT":
+            self._links_dirty = True
+
+    def _push_ct(self, host):
+        bad = np.bitwise_and(host, _UNSUPPORTED)
+        if bad.any():
+            raise NotImplementedError(
+                "cell types other than FLUID and OBSTACLE (moving walls, Zou-He, exits, free slip, "
+                "free surface) are not supported by the fused kernel")
+        self._ct_dev.copy_(torch.from_numpy(from_ref(host.astype(np.int32)).reshape(-1)))
+
+    def _push_rho(self, host):
+        self._rho.copy_(torch.from_numpy(from_ref(host).reshape(-1).astype(np.float32)))
+
+    def _push_vel(self, host):
+        self._vel.copy_(torch.from_numpy(from_ref(host, 3).reshape(3, -1).astype(np.float32)))
+
+    def _sync_inputs(self):
+        self.CT.flush()
+        if self._links_dirty:
+            N.call("lbdem_build_links", N.ptr(self._ct_dev), self.Nx, self.Ny, self.Nz, int(self.skip_inlet),
+                   N.ptr(self._links), N.ptr(self._rows), N.stream_handle())
+            self._links_dirty = False
+        self.rho.flush()
+        self.vel.flush()
+
+    # ------------------------------------------------------------ populations
+    def _decode(self, buf):
+        d = self._f[buf].float().cpu().numpy().astype(np.float64)
+        if self._kind != N.F32:
+            d = d * (W[:, None] / self._scale)
+        return d + W[:, None]
+
+    def _materialize(self):
+        """Bring the lattice to the reference's post-stream state on the device."""
+        if self._collided is not None:
+            src, dst, gather = self._collided
+            if gather:
+                raise RuntimeError("populations between collide() and stream() are not resident; "
+                                   "read them after stream()")
+            return src
+        if self._cur_kind == "fpc":
+            src = self._cur
+            N.call("lbdem_stream_moments", C.byref(self._lat), src, 1 - src, N.stream_handle())
+            self._cur = 1 - src
+            self._cur_kind = "f"
+            self._macro_valid = True
+        return self._cur
+
+    def _pull_f(self):
+        buf = self._materialize()
+        d = self._decode(buf).reshape(19, self.Nz, self.Ny, self.Nx)
+        return to_ref(d)
+
+    def _pull_rho(self):
+        self._materialize()
+        return to_ref(self._rho.cpu().numpy().reshape(self.Nz, self.Ny, self.Nx).astype(np.float64))
+
+    def _pull_vel(self):
+        self._materialize()
+        return to_ref(self._vel.cpu().numpy().reshape(3, self.Nz, self.Ny, self.Nx).astype(np.float64))
+
+    def _pull_omega(self):
+        if self._aux is None:
+            return np.full((self.Nx, self.Ny, self.Nz), self.omega0)
+        om = self._aux[4].float().cpu().numpy().astype(np.float64).reshape(self.Nz, self.Ny, self.Nx)
+        ct = self._host_ct
+        out = to_ref(om)
+        skip = (ct & (CellType.OBSTACLE | CellType.VEL_LADD | CellType.FREE_SLIP | CellType.VEL_INLET_LADD)) != 0
+        out[skip] = self.omega0
+        return out
+
+    def _invalidate_views(self):
+        for fld in (self.rho, self.vel, self.f, self.omega):
+            fld.invalidate()
+
+    # ------------------------------------------------------------ kernels
+    def initialize(self):
+        """f = feq(rho, vel) on updated cells (lbm_solver3d.py:157-171)."""
+        self._sync_inputs()
+        N.call("lbdem_lattice_init", C.byref(self._lat), 0, N.stream_handle())
+        self._cur, self._cur_kind, self._collided = 0, "f", None
+        self._initialized = True
+        self._invalidate_views()
+
+    def _step_fn(self):
+        return {N.F32: "lbdem_psc_step_f32", N.F16: "lbdem_psc_step_f16", N.BF16: "lbdem_psc_step_bf16"}[self._kind]
+
+    def _launch_step(self, psc=None, grains=None):
+        if not self._initialized:
+            raise RuntimeError("call initialize() before collide()")
+        self._sync_inputs()
+        if self._collided is not None:
+            src, dst, gather = self._collided
+        else:
+            src, dst, gather = self._cur, 1 - self._cur, int(self._cur_kind == "fpc")
+        ev = getattr(self, "_kernel_events", None)
+        if ev:
+            ev[0].record()
+        N.call(self._step_fn(), C.byref(self._lat), psc, grains, src, dst, gather, N.stream_handle())
+        if ev:
+            ev[1].record()
+        self._collided = (src, dst, gather)
+        self._invalidate_views()
+
+    def collide(self):
+        self._launch_step()
+
+    def stream(self):
+        """Streaming (lbm_solver3d.py:197-250); the fused kernel performs it at
+        the next collide() or when populations/moments are read."""
+        if self._collided is None:
+            raise RuntimeError("stream() must follow collide()")
+        _, dst, _ = self._collided
+        self._cur, self._cur_kind, self._collided = dst, "fpc", None
+        self._invalidate_views()
+
+    def global_sums(self):
+        """FP64 [mass, momentum_x, momentum_y, momentum_z] of the updated cells."""
+        self._sync_inputs()
+        buf = self._collided[0] if self._collided is not None else self._cur
+        N.call("lbdem_global_sums_f64", C.byref(self._lat), buf, N.ptr(self._sum_out), N.ptr(self._sum_part),
+               N.stream_handle())
+        return self._sum_out.cpu().numpy().copy()
+
+    def check_status(self):
+        s = int(self._status.item())
+        if s:
+            bits = [txt for b, txt in N.STATUS_TEXT.items() if s & b]
+            raise N.LbdemError("lattice fault: " + "; ".join(bits))
+
+    def clear_status(self):
+        self._status.zero_()
+
+
+class BasicLattice3D(LatticeEngine):
+    """BGK + Smagorinsky lattice (BasicLattice3D.collide, lbm_solver3d.py:176-192:
+    computeOmega with the previous step's feq and omega, then BGK)."""
+
+    def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, storage="f32", smagorinsky="reference"):
+        super().__init__(Nx, Ny, Nz, omega, dx, dt, rho, smagorinsky=smagorinsky, storage=storage,
+                         skip_inlet=True)
+
+
+class ForcedLattice3D(LatticeEngine):
+    """BGK with the simple body-force term w_q rho (c_q . F)/cs^2
+    (lbm_foecelover.py:15-68).  F is a physical acceleration."""
+
+    def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, F, *, storage="f32"):
+        unit = UnitConverter(dx, dt, rho)
+        super().__init__(Nx, Ny, Nz, omega, dx, dt, rho, smagorinsky="off",
+                         body_force=unit.getLbAccel(np.asarray(F, np.float64)), storage=storage, skip_inlet=False)
+        self.F = self.body_force
