@@ -33,7 +33,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MLUPS & HBM-roofline % for D3Q19 PSC step, FP16-store vs FP32 at ≤1e-3 drag err"
 NX = NY = NZ = 256
-NP = 2000
+NP = 2000       # overridable (--size/--particles) only for small profiling cases
 SUB = 10
 TAU = 0.6
 CS = 0.1
@@ -96,7 +96,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -159,19 +159,28 @@ def run_gpu(args):
 
     # ---- device-resident throughput (inputs already in HBM); the populations
     # (1.27 GB FP32) exceed L2, so no flush is needed between steps
-    ev_step = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    ev_step = [(mk(), mk()) for _ in range(args.steps)]
+    ev_phase = [(mk(), mk(), mk()) for _ in range(args.steps)]   # before map, after step kernel, after DEM
     lat._kernel_events = []
     Nat.reset_launch_count()
     barrier()
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    cpu0 = time.perf_counter()
     with Clocks(local) as clk:
         t0.record(st)
         for k in range(args.steps):
             lat._kernel_events = ev_step[k]
-            lat.step(SUB)
+            ev_phase[k][0].record(st)
+            lat.collide()
+            lat.stream()
+            ev_phase[k][1].record(st)
+            dem.run_substeps(SUB)
+            ev_phase[k][2].record(st)
         t1.record(st)
+        cpu_launch_ms = (time.perf_counter() - cpu0) * 1e3 / args.steps
         torch.cuda.synchronize()
     lat._kernel_events = None
     launches = Nat.launch_count()
@@ -182,6 +191,8 @@ def run_gpu(args):
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms = float(ms_t.item())
     kern_ms = statistics.mean(a.elapsed_time(b) for a, b in ev_step)
+    lbm_ms = statistics.mean(a.elapsed_time(b) for a, b, _ in ev_phase)
+    dem_ms = statistics.mean(b.elapsed_time(c) for _, b, c in ev_phase)
     lat.check_status()
     dem.check_status()
     clocks = clk.summary()
@@ -242,6 +253,8 @@ def run_gpu(args):
         "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 2 * NP * 3 * 8,
                 "d2h_bytes_per_step": 4 * NP * 3 * 8},
         "gpu_launches": launches,
+        "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4), "dem_10_substeps": round(dem_ms, 4),
+                      "host_launch_per_step": round(cpu_launch_ms, 4)},
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -330,7 +343,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=256, help="cube edge; non-default only for profiling")
+    ap.add_argument("--particles", type=int, default=2000, help="non-default only for profiling")
     args = ap.parse_args()
+    global NX, NY, NZ, NP
+    NX = NY = NZ = args.size
+    NP = args.particles
     args.steps_ref = max(1, min(args.steps, 3))
     args.warmup_ref = 1
     if args.impl == "reference":

@@ -141,8 +141,10 @@ typedef struct lbdem_dem {
     double *pos, *vel, *acc, *force, *quat, *omega, *omega_dot, *moment, *inertia, *mass, *radius;
     double *force_fluid, *moment_fluid;
     int32_t *freeze, *fixvel;
-    /* contacts: n*maxc slots owned by the lower index, wall contacts n*6 */
-    int32_t *cf_j, *cf_active, *cfn;
+    /* contacts: n*maxc slots owned by the lower index, wall contacts n*6;
+     * cfn = slots in use at the start of a sub-step, cf_add = slots appended
+     * during it (zero between sub-steps) */
+    int32_t *cf_j, *cf_active, *cfn, *cf_add;
     double *cf_shear, *cf_pos, *cf_force;
     int32_t *wcf_active;
     double *wcf_shear, *wcf_pos, *wcf_force;
@@ -152,6 +154,9 @@ typedef struct lbdem_dem {
     int32_t *pcell;        /* n: cell of each particle */
     int32_t *prank;        /* n: rank of the particle within its cell */
     int32_t *sorted;       /* n: particle ids grouped by cell */
+    double *acc_force;     /* (n,3) contact force accumulator, zero between sub-steps */
+    double *acc_moment;    /* (n,3) contact moment accumulator, zero between sub-steps */
+    uint32_t *blocks_done; /* 1 word, zero-initialised: last-block counter of the integrator */
     int32_t parity;        /* which half of cell_count holds the current binning */
     int32_t *status;
 } lbdem_dem;

@@ -52,9 +52,9 @@ class Psc(C.Structure):
 
 
 _DEM_PTRS = ("pos", "vel", "acc", "force", "quat", "omega", "omega_dot", "moment", "inertia", "mass", "radius",
-             "force_fluid", "moment_fluid", "freeze", "fixvel", "cf_j", "cf_active", "cfn", "cf_shear", "cf_pos",
+             "force_fluid", "moment_fluid", "freeze", "fixvel", "cf_j", "cf_active", "cfn", "cf_add", "cf_shear", "cf_pos",
              "cf_force", "wcf_active", "wcf_shear", "wcf_pos", "wcf_force", "cell_count", "cell_start", "pcell",
-             "prank", "sorted")
+             "prank", "sorted", "acc_force", "acc_moment", "blocks_done")
 
 
 class Dem(C.Structure):
@@ -89,7 +89,7 @@ _lib = None
 # kernels launched per call (for the launch count reported by bench.py)
 KERNELS_PER_CALL = {"lbdem_build_links": 2, "lbdem_lattice_init": 1, "lbdem_psc_map": 2,
                     "lbdem_psc_step_f32": 1, "lbdem_psc_step_f16": 1, "lbdem_psc_step_bf16": 1,
-                    "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
+                    "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 3,
                     "lbdem_global_sums_f64": 2}
 _launches = [0]
 
@@ -126,7 +126,7 @@ def load(path: str = LIB_PATH):
 
 def call(name: str, *args):
     rc = getattr(load(), name)(*args)
-    _launches[0] += 3 * int(args[1]) if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
+    _launches[0] += 2 * int(args[1]) if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
     if rc != LBDEM_OK:
         msg = load().lbdem_last_error().decode(errors="replace")
         raise LbdemError(f"{name} failed (code {rc}): {msg}")

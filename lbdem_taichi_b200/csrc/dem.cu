@@ -7,11 +7,12 @@
 // probed with the same octant rule, which proposes the same pairs whenever
 // distinct cells do not alias in the reference's hash (checked on the host).
 //
-// Per sub-step: k_scan (one block: exclusive scan of the cell counts, scatter
-// the particle ids, clear force/moment), k_contacts (one thread per particle:
-// candidate pairs j > i with contact history owned by i, then the six walls),
-// k_integrate (body + fluid force, improved Verlet, quaternion update,
-// contact-list compaction, then bin the new positions for the next sub-step).
+// Per sub-step two launches: k_contacts (eight lanes per particle: candidate
+// pairs j > i with contact history owned by i, and the six walls; forces go
+// to accumulators) and k_integrate (accumulated + body + fluid force, improved
+// Verlet, quaternion update, contact-list compaction, binning of the new
+// positions; the last block to finish scans the counts and builds the cell
+// lists for the next sub-step).
 // FP64 throughout; compiled with -fmad=false to follow the reference's
 // operation order (and the FP64 oracle) closely.
 #include <math.h>
@@ -115,15 +116,15 @@ __global__ void k_bin(const __grid_constant__ DemArgs A) {
     bin_particle(A.d, i, A.d.cell_count + (size_t)A.parity * A.ncell);
 }
 
-// one block: exclusive scan of the cell counts, scatter ids, clear force/moment
-__global__ void __launch_bounds__(1024) k_scan(const __grid_constant__ DemArgs A) {
-    const lbdem_dem &d = A.d;
-    const int32_t *count = d.cell_count + (size_t)A.parity * A.ncell;
+// Exclusive scan of the cell counts and scatter of the particle ids into
+// cell order, by one thread block (any size <= 1024).  Counts were produced
+// with atomics by other blocks, so they are read through L2 (__ldcg).
+__device__ void block_scan_scatter(const lbdem_dem &d, const int32_t *count, int ncell) {
     const int nt = blockDim.x, t = threadIdx.x;
-    const int per = (A.ncell + nt - 1) / nt;
-    const int b0 = min(A.ncell, t * per), b1 = min(A.ncell, b0 + per);
+    const int per = (ncell + nt - 1) / nt;
+    const int b0 = min(ncell, t * per), b1 = min(ncell, b0 + per);
     int local = 0;
-    for (int c = b0; c < b1; ++c) local += count[c];
+    for (int c = b0; c < b1; ++c) local += __ldcg(count + c);
     __shared__ int sh[1024];
     sh[t] = local;
     __syncthreads();
@@ -136,14 +137,17 @@ __global__ void __launch_bounds__(1024) k_scan(const __grid_constant__ DemArgs A
     int run = sh[t] - local;
     for (int c = b0; c < b1; ++c) {
         d.cell_start[c] = run;
-        run += count[c];
+        run += __ldcg(count + c);
     }
     __syncthreads();
     for (int i = t; i < d.n; i += nt) {
-        const int c = d.pcell[i];
-        if (c >= 0) d.sorted[d.cell_start[c] + d.prank[i]] = i;
-        for (int a = 0; a < 3; ++a) d.force[3 * i + a] = d.moment[3 * i + a] = 0.0;   // clear_state :422-429
+        const int c = __ldcg(d.pcell + i);
+        if (c >= 0) d.sorted[__ldcg(d.cell_start + c) + __ldcg(d.prank + i)] = i;
     }
+}
+
+__global__ void __launch_bounds__(1024) k_scan(const __grid_constant__ DemArgs A) {
+    block_scan_scatter(A.d, A.d.cell_count + (size_t)A.parity * A.ncell, A.ncell);
 }
 
 // ------------------------------- contact laws ------------------------------
@@ -234,7 +238,7 @@ __device__ __forceinline__ void periodic_delta(const lbdem_dem &d, const double 
 // forces on j added atomically.
 __device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, double *Mi_acc) {
     const size_t base = (size_t)i * d.maxc;
-    int n_i = d.cfn[i];
+    const int n_i = d.cfn[i];   // slots in use when the sub-step started
     int off = -1;
     for (int o = 0; o < n_i && o < d.maxc; ++o)
         if (d.cf_j[base + o] == j && d.cf_active[base + o]) {
@@ -250,12 +254,13 @@ __device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, d
         if (gap < 0) eval = true;
         else d.cf_active[base + off] = 0;
     } else if (gap < 0) {
-        if (n_i >= d.maxc) {
+        // append_contact_offset (demsolver.py:352-359); several lanes of the
+        // same particle may append in one sub-step
+        off = n_i + atomicAdd(d.cf_add + i, 1);
+        if (off >= d.maxc) {
             atomicOr(d.status, (int)LBDEM_ST_CONTACT_OVERFLOW);
             return;
         }
-        off = n_i;
-        d.cfn[i] = n_i + 1;
         d.cf_j[base + off] = j;
         d.cf_active[base + off] = 1;
         for (int a = 0; a < 3; ++a)
@@ -304,8 +309,8 @@ __device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, d
     for (int t = 0; t < 3; ++t) {
         Fi_acc[t] += Fi[t];
         Mi_acc[t] += Mi[t];
-        atomicAdd(d.force + 3 * j + t, Fj[t]);
-        atomicAdd(d.moment + 3 * j + t, Mj[t]);
+        atomicAdd(d.acc_force + 3 * j + t, Fj[t]);
+        atomicAdd(d.acc_moment + 3 * j + t, Mj[t]);
     }
 }
 
@@ -344,48 +349,61 @@ __device__ void wall_contact(const lbdem_dem &d, int i, int w, double *Fi_acc, d
     }
 }
 
+// Eight lanes per particle: lane k probes the k-th cell of the reference's
+// probe list (own cell + octant, bpcd.py:133-142) and, for k < 6, wall k
+// (demsolver.py:809-838); the lanes' forces on the particle are summed with
+// shuffles before one atomic per component.
 __global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArgs A) {
     const lbdem_dem &d = A.d;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
-    const int32_t *count = d.cell_count + (size_t)A.parity * A.ncell;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = tid >> 3, k = tid & 7;
+    const bool act = i < d.n;
     double Fi[3] = {0.0, 0.0, 0.0}, Mi[3] = {0.0, 0.0, 0.0};
-    const double *o = d.pos + 3 * i;
-    int ijk[3], dd[3];
-    ref_cell(d, o, ijk);
-    for (int a = 0; a < 3; ++a) {
-        const double center = (ijk[a] + 0.5) * d.cell_size + d.bp_min[a];
-        dd[a] = (o[a] > center) ? 1 : -1;
-    }
-    // own cell + octant neighbours in the reference's probe order (bpcd.py:133-142)
-    const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 1, 1}};
-    for (int k = 0; k < 8; ++k) {
-        const int c = cell_index(d, ijk[0] + off[k][0] * dd[0], ijk[1] + off[k][1] * dd[1], ijk[2] + off[k][2] * dd[2]);
-        if (c < 0) continue;
-        const int n = count[c], s0 = d.cell_start[c];
-        for (int t = 0; t < n; ++t) {
-            const int j = d.sorted[s0 + t];
-            if (j > i) resolve_pair(d, i, j, Fi, Mi);
+    if (act) {
+        const int32_t *count = d.cell_count + (size_t)A.parity * A.ncell;
+        const double *o = d.pos + 3 * i;
+        int ijk[3], dd[3];
+        ref_cell(d, o, ijk);
+        for (int a = 0; a < 3; ++a) {
+            const double center = (ijk[a] + 0.5) * d.cell_size + d.bp_min[a];
+            dd[a] = (o[a] > center) ? 1 : -1;
+        }
+        const int ox = (k == 1 || k == 5 || k == 6 || k == 7) ? dd[0] : 0;
+        const int oy = (k == 2 || k == 4 || k == 6 || k == 7) ? dd[1] : 0;
+        const int oz = (k == 3 || k == 4 || k == 5 || k == 7) ? dd[2] : 0;
+        const int c = cell_index(d, ijk[0] + ox, ijk[1] + oy, ijk[2] + oz);
+        if (c >= 0) {
+            const int n = count[c], s0 = d.cell_start[c];
+            for (int t = 0; t < n; ++t) {
+                const int j = d.sorted[s0 + t];
+                if (j > i) resolve_pair(d, i, j, Fi, Mi);
+            }
+        }
+        if (k < 6 && !d.wall_periodic[k]) {
+            const int w = k;
+            const size_t s = (size_t)i * 6 + w;
+            const double sep = -(dot3(o, d.wall_n + 3 * w) - d.wall_d[w]);
+            if (d.wcf_active[s]) {
+                if (sep > d.radius[i]) d.wcf_active[s] = 0;
+                else wall_contact(d, i, w, Fi, Mi);
+            } else if (sep <= d.radius[i]) {
+                d.wcf_active[s] = 1;
+                for (int t = 0; t < 3; ++t) d.wcf_shear[3 * s + t] = d.wcf_pos[3 * s + t] = d.wcf_force[3 * s + t] = 0.0;
+                wall_contact(d, i, w, Fi, Mi);
+            }
         }
     }
-    // resolve_wall (demsolver.py:809-838)
-    for (int w = 0; w < 6; ++w) {
-        if (d.wall_periodic[w]) continue;
-        const size_t s = (size_t)i * 6 + w;
-        const double sep = -(dot3(o, d.wall_n + 3 * w) - d.wall_d[w]);
-        if (d.wcf_active[s]) {
-            if (sep > d.radius[i]) d.wcf_active[s] = 0;
-            else wall_contact(d, i, w, Fi, Mi);
-        } else if (sep <= d.radius[i]) {
-            d.wcf_active[s] = 1;
-            for (int t = 0; t < 3; ++t) d.wcf_shear[3 * s + t] = d.wcf_pos[3 * s + t] = d.wcf_force[3 * s + t] = 0.0;
-            wall_contact(d, i, w, Fi, Mi);
+#pragma unroll
+    for (int off = 1; off < 8; off <<= 1)
+        for (int t = 0; t < 3; ++t) {
+            Fi[t] += __shfl_xor_sync(0xffffffffu, Fi[t], off);
+            Mi[t] += __shfl_xor_sync(0xffffffffu, Mi[t], off);
         }
-    }
-    for (int t = 0; t < 3; ++t) {
-        atomicAdd(d.force + 3 * i + t, Fi[t]);
-        atomicAdd(d.moment + 3 * i + t, Mi[t]);
-    }
+    if (act && k == 0)
+        for (int t = 0; t < 3; ++t) {
+            atomicAdd(d.acc_force + 3 * i + t, Fi[t]);
+            atomicAdd(d.acc_moment + 3 * i + t, Mi[t]);
+        }
 }
 
 // quaternion to rotation matrix (demsolver/utils.py:34-61)
@@ -436,21 +454,43 @@ __device__ __forceinline__ void wrap_position(const lbdem_dem &d, double *p) {
     }
 }
 
-__global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemArgs A) {
+__device__ void integrate_particle(const DemArgs &A, int i);
+
+__global__ void __launch_bounds__(256) k_integrate(const __grid_constant__ DemArgs A) {
     const lbdem_dem &d = A.d;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     // clear the counts consumed by this sub-step (the other half receives the new binning)
     int32_t *used = d.cell_count + (size_t)A.parity * A.ncell;
     for (int c = tid; c < A.ncell; c += gridDim.x * blockDim.x) used[c] = 0;
-    const int i = tid;
-    if (i >= d.n) return;
+    if (tid < d.n) integrate_particle(A, tid);
+    // the last block to finish builds the cell lists of the new positions
+    // (threadfence/counter pattern: no block waits for another)
+    __threadfence();
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(d.blocks_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        block_scan_scatter(d, d.cell_count + (size_t)(A.parity ^ 1) * A.ncell, A.ncell);
+        if (threadIdx.x == 0) *d.blocks_done = 0u;
+    }
+}
+
+__device__ void integrate_particle(const DemArgs &A, int i) {
+    const lbdem_dem &d = A.d;
     const double dt = d.dt;
-    // apply_body_force (demsolver.py:437-448)
+    // clear_state (demsolver.py:422-429) + contacts, then apply_body_force (:437-448)
     for (int t = 0; t < 3; ++t) {
-        d.force[3 * i + t] += d.mass[i] * d.g[t];
-        d.moment[3 * i + t] += 0.0;
-        d.force[3 * i + t] += d.force_fluid[3 * i + t];
-        d.moment[3 * i + t] += d.moment_fluid[3 * i + t];
+        double f = d.acc_force[3 * i + t], m = d.acc_moment[3 * i + t];
+        d.acc_force[3 * i + t] = 0.0;
+        d.acc_moment[3 * i + t] = 0.0;
+        f += d.mass[i] * d.g[t];
+        m += 0.0;
+        f += d.force_fluid[3 * i + t];
+        m += d.moment_fluid[3 * i + t];
+        d.force[3 * i + t] = f;
+        d.moment[3 * i + t] = m;
     }
     // update (demsolver.py:514-636)
     double *p = d.pos + 3 * i, *v = d.vel + 3 * i;
@@ -471,7 +511,7 @@ __global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemAr
     }
     // late_clear_state / remove_inactive_contact (demsolver.py:371-386, 431-436)
     const size_t base = (size_t)i * d.maxc;
-    const int cnt = min(d.cfn[i], d.maxc);
+    const int cnt = min(d.cfn[i] + d.cf_add[i], d.maxc);
     int w = 0;
     for (int o = 0; o < cnt; ++o) {
         if (!d.cf_active[base + o]) continue;
@@ -489,6 +529,7 @@ __global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemAr
     }
     for (int o = w; o < cnt; ++o) d.cf_active[base + o] = 0;
     d.cfn[i] = w;
+    d.cf_add[i] = 0;
     // bin the new position for the next sub-step
     bin_particle(d, i, d.cell_count + (size_t)(A.parity ^ 1) * A.ncell);
 }
@@ -499,7 +540,8 @@ static int check_dem(const lbdem_dem *D) {
         return LBDEM_ERR_ARG;
     }
     if (D->n > 0 && (!D->pos || !D->vel || !D->cell_count || !D->cell_start || !D->pcell || !D->prank ||
-                     !D->sorted || !D->cfn || !D->wcf_active)) {
+                     !D->sorted || !D->cfn || !D->cf_add || !D->wcf_active || !D->acc_force || !D->acc_moment ||
+                     !D->blocks_done)) {
         set_error("dem: missing buffers");
         return LBDEM_ERR_ARG;
     }
@@ -529,6 +571,7 @@ int lbdem_dem_bin(lbdem_dem *D, void *stream) {
     if (cudaMemsetAsync(D->cell_count + (size_t)A.parity * A.ncell, 0, sizeof(int32_t) * A.ncell, st) != cudaSuccess)
         return check_launch("dem_bin memset");
     k_bin<<<(D->n + 127) / 128, 128, 0, st>>>(A);
+    k_scan<<<1, 1024, 0, st>>>(A);
     return check_launch("dem_bin");
 }
 
@@ -540,13 +583,12 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     DemArgs A;
     A.d = *D;
     A.ncell = D->gdim[0] * D->gdim[1] * D->gdim[2];
-    const int nb = (D->n + 127) / 128;
-    const int nb_int = max(nb, min(148, (A.ncell + 127) / 128));
+    const int nb_int = max((D->n + 255) / 256, min(148, (A.ncell + 255) / 256));
+    const int nb_con = (int)((8ll * D->n + 127) / 128);
     for (int s = 0; s < nsub; ++s) {
         A.parity = D->parity;
-        k_scan<<<1, 1024, 0, st>>>(A);
-        k_contacts<<<nb, 128, 0, st>>>(A);
-        k_integrate<<<nb_int, 128, 0, st>>>(A);
+        k_contacts<<<nb_con, 128, 0, st>>>(A);
+        k_integrate<<<nb_int, 256, 0, st>>>(A);
         D->parity ^= 1;
     }
     return check_launch("dem_substeps");

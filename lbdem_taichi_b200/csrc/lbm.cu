@@ -114,17 +114,30 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
         for (int q = 0; q < Q; ++q) d[q] = 0.f;
     }
 
-    // moments (compute_rho_vel, lbm_solver3d.py:276-303), deviation form
-    float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    // D3Q19 directions come in opposite pairs (q, q+1) for odd q (c_{q+1} = -c_q):
+    // symmetric sums sp = d_q + d_{q+1} and antisymmetric sums am = d_q - d_{q+1}
+    // carry every moment needed below.
+    float sp[9], am[9];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        drho += d[q];
-        if (cx(q)) jx += cx(q) * d[q];
-        if (cy(q)) jy += cy(q) * d[q];
-        if (cz(q)) jz += cz(q) * d[q];
+    for (int p = 0; p < 9; ++p) {
+        sp[p] = d[2 * p + 1] + d[2 * p + 2];
+        am[p] = d[2 * p + 1] - d[2 * p + 2];
+    }
+    // moments (compute_rho_vel, lbm_solver3d.py:276-303), deviation form
+    float drho = d[0];
+#pragma unroll
+    for (int p = 0; p < 9; ++p) drho += sp[p];
+    float jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        const int q = 2 * p + 1;
+        if (cx(q)) jx += cx(q) * am[p];
+        if (cy(q)) jy += cy(q) * am[p];
+        if (cz(q)) jz += cz(q) * am[p];
     }
     const float rho = 1.f + drho;
-    const float ux = jx / rho, uy = jy / rho, uz = jz / rho;
+    const float irho = 1.f / rho;
+    const float ux = jx * irho, uy = jy * irho, uz = jz * irho;
     const float usq = ux * ux + uy * uy + uz * uz;
     if (act) {
         uint32_t bad = 0;
@@ -139,13 +152,14 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
     if (SMAG != LBDEM_SMAG_OFF) {
         float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            if (cx(q)) sxx += d[q];
-            if (cy(q)) syy += d[q];
-            if (cz(q)) szz += d[q];
-            if (cx(q) * cy(q)) sxy += cx(q) * cy(q) * d[q];
-            if (cx(q) * cz(q)) sxz += cx(q) * cz(q) * d[q];
-            if (cy(q) * cz(q)) syz += cy(q) * cz(q) * d[q];
+        for (int p = 0; p < 9; ++p) {
+            const int q = 2 * p + 1;
+            if (cx(q)) sxx += sp[p];
+            if (cy(q)) syy += sp[p];
+            if (cz(q)) szz += sp[p];
+            if (cx(q) * cy(q)) sxy += cx(q) * cy(q) * sp[p];
+            if (cx(q) * cz(q)) sxz += cx(q) * cz(q) * sp[p];
+            if (cy(q) * cz(q)) syz += cy(q) * cz(q) * sp[p];
         }
         // second moment of the equilibrium: rho cs^2 delta + rho u u
         float er, eux, euy, euz, pref;
@@ -173,9 +187,9 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
         const float pxz = sxz - erho * eux * euz;
         const float pyz = syz - erho * euy * euz;
         const float pi = sqrtf(2.f * (pxx * pxx + pyy * pyy + pzz * pzz + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz)));
-        const float rate = pref / (2.f * CS2 * rho) * pi;
+        const float rate = pref * (0.5f / CS2) * irho * pi;
         const float nut = a.smag_c2 * rate;
-        om = 1.f / (a.inv_omega0 + nut / CS2);
+        om = 1.f / (a.inv_omega0 + nut * (1.f / CS2));
         if (SMAG == LBDEM_SMAG_REFERENCE && act) {
             T *ax = (T *)a.aux;
             ax[cell] = aux_enc<T>(drho);
@@ -186,13 +200,13 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
         }
     }
 
-    // equilibrium deviations feq_q - w_q (compute_feq, lbm_solver3d.py:255-271)
-    float fe[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
-        fe[q] = wq(q) * (drho + rho * (3.f * cu + 4.5f * cu * cu - 1.5f * usq));
-    }
+    // Collision, one opposite pair (q, q+1) at a time, in place in d[].
+    // Equilibrium deviations feq - w (compute_feq, lbm_solver3d.py:255-271):
+    // fe_q = A + B, fe_{q+1} = A - B with A = w (drho + rho (4.5 cu^2 - 1.5 u^2)),
+    // B = 3 w rho cu.  Body force w rho (c . F)/cs^2 (lbm_foecelover.py:150-164)
+    // is odd in c: +g on q, -g on q+1 (g = 0 when no force is set).
+    const float base = -1.5f * usq;
+    const float gx = rho * a.f3x, gy = rho * a.f3y, gz = rho * a.f3z;
 
     uint32_t key = 0;
     if (a.key != nullptr && act) key = a.key[cell];
@@ -200,11 +214,14 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
     float hx = 0.f, hy = 0.f, hz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
     if (key) {
         // PSC weighted collision (psclattice3d.py:240-261; B from the current
-        // omega as hybridlattice.py:236-245; solid velocity :160-182)
+        // omega as hybridlattice.py:236-245; solid velocity :160-182):
+        // fpc = f + B Os + (1-B) Of, Os_q = f_{qbar} - feq_{qbar} + feqs_q - f_q,
+        // Of = -omega (f - feq), hydroforce -= B Os_q c_q
         gid = (int)key_gid(key);
         const float eps = (key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f);
         const float taum = 1.f / om - 0.5f;
-        const float B = eps * taum / ((1.f - eps) + taum);
+        const float Bw = eps * taum / ((1.f - eps) + taum);
+        const float Bf = (1.f - Bw) * om;
         const float4 t0 = a.table[4 * gid + 0], t1 = a.table[4 * gid + 1];
         const float4 t2 = a.table[4 * gid + 2], t3 = a.table[4 * gid + 3];
         const float rx = ((float)x - t0.x) - t1.x;
@@ -213,21 +230,32 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
         const float sx = t2.x + (t3.y * rz - t3.z * ry);
         const float sy = t2.y + (t3.z * rx - t3.x * rz);
         const float sz = t2.z + (t3.x * ry - t3.y * rx);
-        const float ssq = sx * sx + sy * sy + sz * sz;
-        float out[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const float cus = cx(q) * sx + cy(q) * sy + cz(q) * sz;
-            const float fs = wq(q) * (drho + rho * (3.f * cus + 4.5f * cus * cus - 1.5f * ssq));
-            const float oms = d[qinv(q)] - fe[qinv(q)] + fs - d[q];
-            const float omf = -om * (d[q] - fe[q]);
-            out[q] = d[q] + B * oms + (1.f - B) * omf;
-            if (cx(q)) hx -= B * oms * cx(q);
-            if (cy(q)) hy -= B * oms * cy(q);
-            if (cz(q)) hz -= B * oms * cz(q);
+        const float sbase = -1.5f * (sx * sx + sy * sy + sz * sz);
+        {
+            const float fe0 = wq(0) * (drho + rho * base);
+            const float fs0 = wq(0) * (drho + rho * sbase);
+            d[0] = d[0] + Bw * (fs0 - fe0) - Bf * (d[0] - fe0);
         }
 #pragma unroll
-        for (int q = 0; q < Q; ++q) d[q] = out[q];
+        for (int p = 0; p < 9; ++p) {
+            const int q = 2 * p + 1;
+            const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
+            const float A = wq(q) * (drho + rho * (4.5f * cu * cu + base));
+            const float B = wq(q) * 3.f * rho * cu;
+            const float cus = cx(q) * sx + cy(q) * sy + cz(q) * sz;
+            const float As = wq(q) * (drho + rho * (4.5f * cus * cus + sbase));
+            const float Bs = wq(q) * 3.f * rho * cus;
+            const float dq = d[q], db = d[q + 1];
+            const float osq = db - (A - B) + (As + Bs) - dq;
+            const float osb = dq - (A + B) + (As - Bs) - db;
+            const float g = wq(q) * (cx(q) * gx + cy(q) * gy + cz(q) * gz);
+            d[q] = dq + Bw * osq - Bf * (dq - (A + B)) + g;
+            d[q + 1] = db + Bw * osb - Bf * (db - (A - B)) - g;
+            const float m = Bw * (osq - osb);   // B Os_q c_q + B Os_{q+1} c_{q+1}
+            if (cx(q)) hx -= cx(q) * m;
+            if (cy(q)) hy -= cy(q) * m;
+            if (cz(q)) hz -= cz(q) * m;
+        }
         tx = ry * hz - rz * hy;
         ty = rz * hx - rx * hz;
         tz = rx * hy - ry * hx;
@@ -237,14 +265,17 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
             a.hydro_out[2 * nc + cell] = hz;
         }
     } else {
+        d[0] = d[0] + om * (wq(0) * (drho + rho * base) - d[0]);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) d[q] = d[q] + om * (fe[q] - d[q]);
-    }
-
-    if (a.force_on) {
-        // ForcedLattice3D source term (lbm_foecelover.py:150-164)
-#pragma unroll
-        for (int q = 1; q < Q; ++q) d[q] += wq(q) * rho * (cx(q) * a.f3x + cy(q) * a.f3y + cz(q) * a.f3z);
+        for (int p = 0; p < 9; ++p) {
+            const int q = 2 * p + 1;
+            const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
+            const float A = wq(q) * (drho + rho * (4.5f * cu * cu + base));
+            const float B = wq(q) * 3.f * rho * cu;
+            const float g = wq(q) * (cx(q) * gx + cy(q) * gy + cz(q) * gz);
+            d[q] = d[q] + om * ((A + B) - d[q]) + g;
+            d[q + 1] = d[q + 1] + om * ((A - B) - d[q + 1]) - g;
+        }
     }
 
     if (act) {

@@ -5,9 +5,10 @@
 // can touch and claims them with atomicMax on a 32-bit owner key that encodes
 // the reference's winner rule, so the result is identical for any order.
 //
-// The geometry is FP64 with the reference's operation order; this file is
-// compiled with -fmad=false so no multiply-add is contracted and the 5^3
-// sub-sample counts match the reference bit for bit.
+// Decisions are the reference's FP64 comparisons (operation order kept, and
+// this file is compiled with -fmad=false so nothing is contracted); an FP32
+// pre-classification with a proven margin decides the clear cases, so the 5^3
+// sub-sample counts match the reference bit for bit at FP32 speed.
 #include <math.h>
 
 #include "common.cuh"
@@ -51,11 +52,12 @@ __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
             const int z0 = max(0, (int)floor(pzc - lim)), z1 = min(a.nz - 1, (int)ceil(pzc + lim));
             const int ex = x1 - x0 + 1, ey = y1 - y0 + 1, ez = z1 - z0 + 1;
             if (ex > 0 && ey > 0 && ez > 0) {
-                const long long tot = (long long)ex * ey * ez;
-                const double lim2 = lim * lim;
-                for (long long t = threadIdx.x; t < tot; t += blockDim.x) {
-                    const int i = x0 + (int)(t % ex), j = y0 + (int)((t / ex) % ey), k = z0 + (int)(t / ((long long)ex * ey));
-                    const double ddx = pxc - i, ddy = pyc - j, ddz = pzc - k;
+                const unsigned exy = (unsigned)ex * (unsigned)ey, tot = exy * (unsigned)ez;
+                const float lim2 = (float)(lim * lim) + 1e-3f;
+                for (unsigned t = threadIdx.x; t < tot; t += blockDim.x) {
+                    const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex;
+                    const int i = x0 + (int)(rem - jy * (unsigned)ex), j = y0 + (int)jy, k = z0 + (int)kz;
+                    const float ddx = (float)(pxc - i), ddy = (float)(pyc - j), ddz = (float)(pzc - k);
                     if (ddx * ddx + ddy * ddy + ddz * ddz < lim2)
                         a.key[((size_t)k * a.ny + j) * a.nx + i] = 0u;
                 }
@@ -79,40 +81,32 @@ __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
     }
 }
 
-// 5^3 sub-cell count (psclattice3d.py:121-131): sqrt(s) < r decided exactly;
-// s is formed in the reference's order ((dx^2 + dy^2) + dz^2), the square
-// root is only evaluated when s lies within a few ulps of r^2.
-__device__ __forceinline__ int subcell_count(double xc, double yc, double zc, int i, int j, int k, double r) {
-    if (!(r > 0.0)) return 0;
-    double sx2[5], sy2[5], sz2[5];
-#pragma unroll
-    for (int t = 0; t < 5; ++t) {
-        const double ox = xc - (((double)i - 0.4) + 0.2 * t);
-        const double oy = yc - (((double)j - 0.4) + 0.2 * t);
-        const double oz = zc - (((double)k - 0.4) + 0.2 * t);
-        sx2[t] = ox * ox;
-        sy2[t] = oy * oy;
-        sz2[t] = oz * oz;
-    }
-    const double rr = r * r;
-    const double lo = rr * (1.0 - 0x1p-45), hi = rr * (1.0 + 0x1p-45);
-    int cnt = 0;
-#pragma unroll
-    for (int ii = 0; ii < 5; ++ii)
-#pragma unroll
-        for (int jj = 0; jj < 5; ++jj) {
-            const double sxy = sx2[ii] + sy2[jj];
-#pragma unroll
-            for (int kk = 0; kk < 5; ++kk) {
-                const double s = sxy + sz2[kk];
-                if (s < lo) cnt++;
-                else if (s <= hi && sqrt(s) < r) cnt++;
-            }
-        }
-    return cnt;
+// Exact FP64 sub-cell test, in the reference's operation order
+// (psclattice3d.py:125-128): sqrt(dx^2 + dy^2 + dz^2) < r.
+__device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, double zc, int i, int j, int k, int ii,
+                                                     int jj, int kk, double r) {
+    const double ox = xc - (((double)i - 0.4) + 0.2 * ii);
+    const double oy = yc - (((double)j - 0.4) + 0.2 * jj);
+    const double oz = zc - (((double)k - 0.4) + 0.2 * kk);
+    return sqrt((ox * ox + oy * oy) + oz * oz) < r;
 }
 
+// One block per particle, two phases per chunk of its bounding box:
+//  1. each thread classifies one cell -- outside / fully covered / partial
+//     (psclattice3d.py:108-113).  FP32 with a safety margin decides the clear
+//     cases; the exact FP64 comparisons run only for cells near a threshold.
+//     Full covers are claimed at once; partial cells go to a shared list.
+//  2. one warp per partial cell counts its 5^3 sub-points
+//     (psclattice3d.py:121-131): lane (ii, jj) < 25 tests the column of five
+//     kk sub-points, the warp sums with __reduce_add_sync.  A sub-point whose
+//     FP32 squared distance lies within 1e-4 (1 + r^2) of r^2 is re-tested
+//     with the reference's exact FP64 expression (|s32 - s64| < 2e-5 (1 + r^2)
+//     for these offsets), so counts are bit-exact.
+constexpr int MAP_CHUNK = 2048;
+
 __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
+    __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32, w = local index
+    __shared__ int s_n;
     const int g = blockIdx.x;
     double xc, yc, zc, r;
     particle_lattice(a, g, xc, yc, zc, r);
@@ -127,23 +121,77 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     const int ex = x1 - x0 + 1, ey = y1 - y0 + 1, ez = z1 - z0 + 1;
     if (ex <= 0 || ey <= 0 || ez <= 0) return;
     const uint32_t gbits = 0xFFFFFFu - (uint32_t)g;
-    const long long tot = (long long)ex * ey * ez;
-    for (long long t = threadIdx.x; t < tot; t += blockDim.x) {
-        const int i = x0 + (int)(t % ex), j = y0 + (int)((t / ex) % ey), k = z0 + (int)(t / ((long long)ex * ey));
-        const size_t c = ((size_t)k * a.ny + j) * a.nx + i;
-        if (a.links[c] & LINK_MAP_SKIP) continue;
-        const double ddx = xc - i, ddy = yc - j, ddz = zc - k;
-        const double dist = sqrt((ddx * ddx + ddy * ddy) + ddz * ddz);
-        if (dist >= t_out) continue;
-        uint32_t kv;
-        if (dist <= t_in) {
-            kv = KEY_FULL | gbits;
-        } else {
-            const int cnt = subcell_count(xc, yc, zc, i, j, k, r);
-            if (cnt == 0) continue;   // eps = 0 never beats the empty cell (strict >)
-            kv = ((uint32_t)cnt << 24) | gbits;
+    const float out2 = (float)(t_out * t_out), marg_o = (float)(1e-4 * (1.0 + t_out * t_out));
+    const float in2 = t_in > 0.0 ? (float)(t_in * t_in) : -1.f, marg_i = (float)(1e-4 * (1.0 + t_in * t_in));
+    const double rr = r > 0.0 ? r * r : 0.0;
+    const float band = (float)(1e-4 * (1.0 + rr));
+    const float lo = (float)rr - band, hi = (float)rr + band;
+    const unsigned exy = (unsigned)ex * (unsigned)ey;
+    const unsigned tot = exy * (unsigned)ez;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int ii = lane / 5, jj = lane % 5;
+    for (unsigned base = 0; base < tot; base += MAP_CHUNK) {
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        const unsigned lim = min(tot, base + MAP_CHUNK);
+        for (unsigned t = base + threadIdx.x; t < lim; t += blockDim.x) {
+            const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex, ix = rem - jy * (unsigned)ex;
+            const int i = x0 + (int)ix, j = y0 + (int)jy, k = z0 + (int)kz;
+            const float fx = (float)(xc - (double)i), fy = (float)(yc - (double)j), fz = (float)(zc - (double)k);
+            const float d2 = (fx * fx + fy * fy) + fz * fz;
+            if (d2 > out2 + marg_o) continue;                 // certainly dist >= t_out
+            const size_t c = ((size_t)k * a.ny + j) * a.nx + i;
+            if (a.links[c] & LINK_MAP_SKIP) continue;
+            int full;
+            if (d2 < in2 - marg_i) {
+                full = 1;                                     // certainly dist <= t_in
+            } else if (d2 < out2 - marg_o && d2 > in2 + marg_i) {
+                full = 0;                                     // certainly partial
+            } else {
+                const double ddx = xc - i, ddy = yc - j, ddz = zc - k;
+                const double dist = sqrt((ddx * ddx + ddy * ddy) + ddz * ddz);
+                if (dist >= t_out) continue;
+                full = dist <= t_in;
+            }
+            if (full) {
+                atomicMax(a.key + c, KEY_FULL | gbits);
+            } else if (r > 0.0) {
+                const int slot = atomicAdd(&s_n, 1);
+                s_off[slot] = make_float4(fx, fy, fz, __int_as_float((int)(t - base)));
+            }
         }
-        atomicMax(a.key + c, kv);
+        __syncthreads();
+        const int n = s_n;
+        for (int e = warp; e < n; e += nwarp) {
+            const float4 o = s_off[e];
+            int cnt = 0;
+            if (lane < 25) {
+                const float ox = o.x + (0.4f - 0.2f * (float)ii);
+                const float oy = o.y + (0.4f - 0.2f * (float)jj);
+                const float sxy = ox * ox + oy * oy;
+#pragma unroll
+                for (int kk = 0; kk < 5; ++kk) {
+                    const float oz = o.z + (0.4f - 0.2f * (float)kk);
+                    const float s = sxy + oz * oz;
+                    if (s < lo) {
+                        ++cnt;
+                    } else if (s <= hi) {
+                        const unsigned t = base + (unsigned)__float_as_int(o.w);
+                        const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex;
+                        const int i = x0 + (int)(rem - jy * (unsigned)ex), j = y0 + (int)jy, k = z0 + (int)kz;
+                        cnt += subcell_inside_exact(xc, yc, zc, i, j, k, ii, jj, kk, r);
+                    }
+                }
+            }
+            cnt = __reduce_add_sync(0xffffffffu, cnt);
+            if (lane == 0 && cnt > 0) {   // eps = 0 never beats the empty cell (strict >)
+                const unsigned t = base + (unsigned)__float_as_int(o.w);
+                const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex;
+                const int i = x0 + (int)(rem - jy * (unsigned)ex), j = y0 + (int)jy, k = z0 + (int)kz;
+                atomicMax(a.key + ((size_t)k * a.ny + j) * a.nx + i, ((uint32_t)cnt << 24) | gbits);
+            }
+        }
+        __syncthreads();
     }
 }
 

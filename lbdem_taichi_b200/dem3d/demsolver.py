@@ -198,6 +198,7 @@ class DEMSolver:
         self.cf_j = torch.zeros(ns, **i32)
         self.cf_active = torch.zeros(ns, **i32)
         self.cfn = torch.zeros(max(n, 1), **i32)
+        self.cf_add = torch.zeros(max(n, 1), **i32)
         self.cf_shear = torch.zeros((ns, 3), **f64)
         self.cf_pos = torch.zeros((ns, 3), **f64)
         self.cf_force = torch.zeros((ns, 3), **f64)
@@ -222,6 +223,9 @@ class DEMSolver:
         self.pcell = torch.zeros(max(n, 1), **i32)
         self.prank = torch.zeros(max(n, 1), **i32)
         self.sorted = torch.zeros(max(n, 1), **i32)
+        self.acc_force = torch.zeros((max(n, 1), 3), **f64)
+        self.acc_moment = torch.zeros((max(n, 1), 3), **f64)
+        self.blocks_done = torch.zeros(1, **i32)
         # the reference hashes cells into a 2^k table: distinct cells alias when
         # their coordinates agree in the low bits kept by Morton-code mod 2^k
         T = reference_table_size(rmax, dmin, dmax) if n else 1 << 20
@@ -254,12 +258,14 @@ class DEMSolver:
                           ("omega_dot", t["omega_dot"]), ("moment", t["moment"]), ("inertia", t["inertia"]),
                           ("mass", t["mass"]), ("radius", t["radius"]), ("force_fluid", t["force_fluid"]),
                           ("moment_fluid", t["moment_fluid"]), ("freeze", t["freeze"]), ("fixvel", t["fixvel"]),
-                          ("cf_j", self.cf_j), ("cf_active", self.cf_active), ("cfn", self.cfn),
+                          ("cf_j", self.cf_j), ("cf_active", self.cf_active), ("cfn", self.cfn), ("cf_add", self.cf_add),
                           ("cf_shear", self.cf_shear), ("cf_pos", self.cf_pos), ("cf_force", self.cf_force),
                           ("wcf_active", self.wcf_active), ("wcf_shear", self.wcf_shear),
                           ("wcf_pos", self.wcf_pos), ("wcf_force", self.wcf_force),
                           ("cell_count", self.cell_count), ("cell_start", self.cell_start),
-                          ("pcell", self.pcell), ("prank", self.prank), ("sorted", self.sorted)):
+                          ("pcell", self.pcell), ("prank", self.prank), ("sorted", self.sorted),
+                          ("acc_force", self.acc_force), ("acc_moment", self.acc_moment),
+                          ("blocks_done", self.blocks_done)):
             setattr(d, name, N.ptr(ten))
         d.parity = 0
         d.status = N.ptr(self.status)
