@@ -64,6 +64,8 @@ extern "C" {
 #define LBDEM_ST_CONTACT_OVERFLOW 8u /* more contacts than max_coordinate_number */
 #define LBDEM_ST_GRID_OVERFLOW 16u   /* particle outside the broad-phase grid */
 #define LBDEM_ST_GID_OVERFLOW 32u    /* more than 2^24-1 particles in the PSC map */
+#define LBDEM_ST_CELL_OVERFLOW 64u   /* a broad-phase cell holds more than cell_cap particles */
+#define LBDEM_ST_WAIT_TIMEOUT 128u   /* a bounded wait for an asynchronous copy gave up */
 
 /* storage forms */
 #define LBDEM_F32 0
@@ -149,14 +151,11 @@ typedef struct lbdem_dem {
     int32_t *wcf_active;
     double *wcf_shear, *wcf_pos, *wcf_force;
     /* broad-phase scratch (caller-owned) */
-    int32_t *cell_count;   /* 2 * prod(gdim), zero-initialised once */
-    int32_t *cell_start;   /* prod(gdim) */
-    int32_t *pcell;        /* n: cell of each particle */
-    int32_t *prank;        /* n: rank of the particle within its cell */
-    int32_t *sorted;       /* n: particle ids grouped by cell */
+    int32_t cell_cap;      /* particles a broad-phase cell can list */
+    int32_t *cell_count;   /* 2 * prod(gdim), zero-initialised once (double-buffered counts) */
+    int32_t *cell_list;    /* prod(gdim) * cell_cap particle ids */
     double *acc_force;     /* (n,3) contact force accumulator, zero between sub-steps */
     double *acc_moment;    /* (n,3) contact moment accumulator, zero between sub-steps */
-    uint32_t *blocks_done; /* 1 word, zero-initialised: last-block counter of the integrator */
     int32_t parity;        /* which half of cell_count holds the current binning */
     int32_t *status;
 } lbdem_dem;

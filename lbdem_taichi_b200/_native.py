@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "_build", "liblbdem.so")
 
 LBDEM_OK = 0
 ST_NAN, ST_RHO, ST_VELMAX = 1, 2, 4
-ST_CONTACT_OVERFLOW, ST_GRID_OVERFLOW, ST_GID_OVERFLOW = 8, 16, 32
+ST_CONTACT_OVERFLOW, ST_GRID_OVERFLOW, ST_GID_OVERFLOW, ST_CELL_OVERFLOW = 8, 16, 32, 64
+ST_WAIT_TIMEOUT = 128
 F32, F16, BF16 = 0, 1, 2
 SMAG_OFF, SMAG_REFERENCE, SMAG_LOCAL = 0, 1, 2
 SUM_BLOCKS = 1184
@@ -26,6 +27,8 @@ STATUS_TEXT = {
     ST_CONTACT_OVERFLOW: "contact count exceeds max_coordinate_number",
     ST_GRID_OVERFLOW: "particle left the broad-phase grid",
     ST_GID_OVERFLOW: "too many particles for the PSC owner key",
+    ST_CELL_OVERFLOW: "a broad-phase cell holds more particles than its list capacity",
+    ST_WAIT_TIMEOUT: "a bounded wait for an asynchronous copy gave up",
 }
 
 vp = C.c_void_p
@@ -53,8 +56,7 @@ class Psc(C.Structure):
 
 _DEM_PTRS = ("pos", "vel", "acc", "force", "quat", "omega", "omega_dot", "moment", "inertia", "mass", "radius",
              "force_fluid", "moment_fluid", "freeze", "fixvel", "cf_j", "cf_active", "cfn", "cf_add", "cf_shear", "cf_pos",
-             "cf_force", "wcf_active", "wcf_shear", "wcf_pos", "wcf_force", "cell_count", "cell_start", "pcell",
-             "prank", "sorted", "acc_force", "acc_moment", "blocks_done")
+             "cf_force", "wcf_active", "wcf_shear", "wcf_pos", "wcf_force")
 
 
 class Dem(C.Structure):
@@ -65,7 +67,9 @@ class Dem(C.Structure):
                 ("E", C.c_double * 2), ("nu", C.c_double * 2), ("mu", C.c_double * 2), ("e", C.c_double * 2),
                 ("kn", C.c_double * 2), ("ks", C.c_double * 2), ("dpn", C.c_double * 2), ("dps", C.c_double * 2),
                 ("wall_n", C.c_double * 18), ("wall_d", C.c_double * 6), ("wall_periodic", C.c_int32 * 6)] + \
-               [(n, vp) for n in _DEM_PTRS] + [("parity", C.c_int32), ("status", vp)]
+               [(n, vp) for n in _DEM_PTRS] + \
+               [("cell_cap", C.c_int32), ("cell_count", vp), ("cell_list", vp), ("acc_force", vp),
+                ("acc_moment", vp), ("parity", C.c_int32), ("status", vp)]
 
 
 EXPORTS = {
@@ -89,7 +93,7 @@ _lib = None
 # kernels launched per call (for the launch count reported by bench.py)
 KERNELS_PER_CALL = {"lbdem_build_links": 2, "lbdem_lattice_init": 1, "lbdem_psc_map": 2,
                     "lbdem_psc_step_f32": 1, "lbdem_psc_step_f16": 1, "lbdem_psc_step_bf16": 1,
-                    "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 3,
+                    "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
                     "lbdem_global_sums_f64": 2}
 _launches = [0]
 

@@ -3,21 +3,27 @@
 // Broad phase: the reference hashes cells of size 4*r_max with a Morton code
 // into a 2^20..2^22 table and probes each particle's own cell plus the seven
 // cells of its octant (bpcd.py:114-152), proposing pairs i < j.  Here the same
-// cells are kept in a dense grid (no hash), binned by a counting sort, and
-// probed with the same octant rule, which proposes the same pairs whenever
-// distinct cells do not alias in the reference's hash (checked on the host).
+// cells are kept in a dense grid (no hash) and probed with the same octant
+// rule, which proposes the same pairs whenever distinct cells do not alias in
+// the reference's hash (checked on the host).
 //
-// Per sub-step two launches: k_contacts (eight lanes per particle: candidate
-// pairs j > i with contact history owned by i, and the six walls; forces go
-// to accumulators) and k_integrate (accumulated + body + fluid force, improved
-// Verlet, quaternion update, contact-list compaction, binning of the new
-// positions; the last block to finish scans the counts and builds the cell
-// lists for the next sub-step).
+// Cells keep fixed-capacity particle lists filled by the binning atomics, so
+// no scan is needed.  Per sub-step two launches: k_contacts (eight lanes per
+// particle: candidate pairs j > i with contact history owned by i, and the six
+// walls; forces go to accumulators) and k_integrate (accumulated + body +
+// fluid force, improved Verlet, quaternion update, contact-list compaction,
+// binning of the new positions into the other half of the counts).
 // FP64 throughout; compiled with -fmad=false to follow the reference's
 // operation order (and the FP64 oracle) closely.
 #include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cooperative_groups.h>
 
 #include "common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace lbdem {
 
@@ -96,58 +102,25 @@ __device__ __forceinline__ void ref_cell(const lbdem_dem &d, const double *p, in
     for (int a = 0; a < 3; ++a) ijk[a] = (int)floor((p[a] - d.bp_min[a]) / d.cell_size);
 }
 
+// Bin particle i into its reference cell: the atomic rank is its slot in the
+// cell's fixed-capacity list (no scan needed).
 __device__ __forceinline__ void bin_particle(const lbdem_dem &d, int i, int32_t *count) {
     int ijk[3];
     ref_cell(d, d.pos + 3 * i, ijk);
     const int c = cell_index(d, ijk[0], ijk[1], ijk[2]);
     if (c < 0) {
         atomicOr(d.status, (int)LBDEM_ST_GRID_OVERFLOW);
-        d.pcell[i] = -1;
-        d.prank[i] = 0;
         return;
     }
-    d.pcell[i] = c;
-    d.prank[i] = atomicAdd(count + c, 1);
+    const int rank = atomicAdd(count + c, 1);
+    if (rank < d.cell_cap) d.cell_list[(size_t)c * d.cell_cap + rank] = i;
+    else atomicOr(d.status, (int)LBDEM_ST_CELL_OVERFLOW);
 }
 
 __global__ void k_bin(const __grid_constant__ DemArgs A) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.d.n) return;
     bin_particle(A.d, i, A.d.cell_count + (size_t)A.parity * A.ncell);
-}
-
-// Exclusive scan of the cell counts and scatter of the particle ids into
-// cell order, by one thread block (any size <= 1024).  Counts were produced
-// with atomics by other blocks, so they are read through L2 (__ldcg).
-__device__ void block_scan_scatter(const lbdem_dem &d, const int32_t *count, int ncell) {
-    const int nt = blockDim.x, t = threadIdx.x;
-    const int per = (ncell + nt - 1) / nt;
-    const int b0 = min(ncell, t * per), b1 = min(ncell, b0 + per);
-    int local = 0;
-    for (int c = b0; c < b1; ++c) local += __ldcg(count + c);
-    __shared__ int sh[1024];
-    sh[t] = local;
-    __syncthreads();
-    for (int off = 1; off < nt; off <<= 1) {   // Hillis-Steele inclusive scan
-        const int v = t >= off ? sh[t - off] : 0;
-        __syncthreads();
-        sh[t] += v;
-        __syncthreads();
-    }
-    int run = sh[t] - local;
-    for (int c = b0; c < b1; ++c) {
-        d.cell_start[c] = run;
-        run += __ldcg(count + c);
-    }
-    __syncthreads();
-    for (int i = t; i < d.n; i += nt) {
-        const int c = __ldcg(d.pcell + i);
-        if (c >= 0) d.sorted[__ldcg(d.cell_start + c) + __ldcg(d.prank + i)] = i;
-    }
-}
-
-__global__ void __launch_bounds__(1024) k_scan(const __grid_constant__ DemArgs A) {
-    block_scan_scatter(A.d, A.d.cell_count + (size_t)A.parity * A.ncell, A.ncell);
 }
 
 // ------------------------------- contact laws ------------------------------
@@ -353,14 +326,13 @@ __device__ void wall_contact(const lbdem_dem &d, int i, int w, double *Fi_acc, d
 // probe list (own cell + octant, bpcd.py:133-142) and, for k < 6, wall k
 // (demsolver.py:809-838); the lanes' forces on the particle are summed with
 // shuffles before one atomic per component.
-__global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArgs A) {
-    const lbdem_dem &d = A.d;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+// One lane of the contact phase: lane k of particle i = tid / 8.  All 32 lanes
+// of the warp must call it together (shuffle reduction over groups of 8).
+__device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *count, int tid) {
     const int i = tid >> 3, k = tid & 7;
     const bool act = i < d.n;
     double Fi[3] = {0.0, 0.0, 0.0}, Mi[3] = {0.0, 0.0, 0.0};
     if (act) {
-        const int32_t *count = d.cell_count + (size_t)A.parity * A.ncell;
         const double *o = d.pos + 3 * i;
         int ijk[3], dd[3];
         ref_cell(d, o, ijk);
@@ -373,9 +345,10 @@ __global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArg
         const int oz = (k == 3 || k == 4 || k == 5 || k == 7) ? dd[2] : 0;
         const int c = cell_index(d, ijk[0] + ox, ijk[1] + oy, ijk[2] + oz);
         if (c >= 0) {
-            const int n = count[c], s0 = d.cell_start[c];
+            const int n = min(count[c], d.cell_cap);
+            const int32_t *lst = d.cell_list + (size_t)c * d.cell_cap;
             for (int t = 0; t < n; ++t) {
-                const int j = d.sorted[s0 + t];
+                const int j = lst[t];
                 if (j > i) resolve_pair(d, i, j, Fi, Mi);
             }
         }
@@ -404,6 +377,10 @@ __global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArg
             atomicAdd(d.acc_force + 3 * i + t, Fi[t]);
             atomicAdd(d.acc_moment + 3 * i + t, Mi[t]);
         }
+}
+
+__global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArgs A) {
+    contact_lane(A.d, A.d.cell_count + (size_t)A.parity * A.ncell, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // quaternion to rotation matrix (demsolver/utils.py:34-61)
@@ -454,31 +431,18 @@ __device__ __forceinline__ void wrap_position(const lbdem_dem &d, double *p) {
     }
 }
 
-__device__ void integrate_particle(const DemArgs &A, int i);
+__device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, int i);
 
-__global__ void __launch_bounds__(256) k_integrate(const __grid_constant__ DemArgs A) {
+__global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemArgs A) {
     const lbdem_dem &d = A.d;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     // clear the counts consumed by this sub-step (the other half receives the new binning)
     int32_t *used = d.cell_count + (size_t)A.parity * A.ncell;
     for (int c = tid; c < A.ncell; c += gridDim.x * blockDim.x) used[c] = 0;
-    if (tid < d.n) integrate_particle(A, tid);
-    // the last block to finish builds the cell lists of the new positions
-    // (threadfence/counter pattern: no block waits for another)
-    __threadfence();
-    __shared__ int last;
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(d.blocks_done, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (last) {
-        __threadfence();
-        block_scan_scatter(d, d.cell_count + (size_t)(A.parity ^ 1) * A.ncell, A.ncell);
-        if (threadIdx.x == 0) *d.blocks_done = 0u;
-    }
+    if (tid < d.n) integrate_particle(d, A.ncell, A.parity, tid);
 }
 
-__device__ void integrate_particle(const DemArgs &A, int i) {
-    const lbdem_dem &d = A.d;
+__device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, int i) {
     const double dt = d.dt;
     // clear_state (demsolver.py:422-429) + contacts, then apply_body_force (:437-448)
     for (int t = 0; t < 3; ++t) {
@@ -531,7 +495,31 @@ __device__ void integrate_particle(const DemArgs &A, int i) {
     d.cfn[i] = w;
     d.cf_add[i] = 0;
     // bin the new position for the next sub-step
-    bin_particle(d, i, d.cell_count + (size_t)(A.parity ^ 1) * A.ncell);
+    bin_particle(d, i, d.cell_count + (size_t)(parity ^ 1) * ncell);
+}
+
+// All sub-steps of one call in ONE launch: a single thread-block cluster (up
+// to 16 CTAs) grid-strides over the contact lanes, then over the particles;
+// the two phases of every sub-step are separated by hardware cluster
+// barriers (barrier.cluster arrive.release / wait.acquire), which order the
+// global-memory writes of one phase before the reads of the next for every
+// thread of the cluster.  Same per-lane/per-particle code as the two kernels.
+__global__ void __launch_bounds__(512) k_dem_cluster(const __grid_constant__ DemArgs A, int nsub) {
+    cg::cluster_group cl = cg::this_cluster();
+    const lbdem_dem &d = A.d;
+    const int nthr = (int)cl.num_threads();
+    const int me = (int)cl.thread_rank();
+    const int nlanes = 8 * d.n;
+    for (int s = 0; s < nsub; ++s) {
+        const int parity = (A.parity + s) & 1;
+        const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
+        for (int base = 0; base < nlanes; base += nthr) contact_lane(d, count, base + me);
+        cl.sync();
+        int32_t *used = d.cell_count + (size_t)parity * A.ncell;
+        for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
+        for (int i = me; i < d.n; i += nthr) integrate_particle(d, A.ncell, parity, i);
+        cl.sync();
+    }
 }
 
 static int check_dem(const lbdem_dem *D) {
@@ -539,9 +527,9 @@ static int check_dem(const lbdem_dem *D) {
         set_error("dem: bad descriptor");
         return LBDEM_ERR_ARG;
     }
-    if (D->n > 0 && (!D->pos || !D->vel || !D->cell_count || !D->cell_start || !D->pcell || !D->prank ||
-                     !D->sorted || !D->cfn || !D->cf_add || !D->wcf_active || !D->acc_force || !D->acc_moment ||
-                     !D->blocks_done)) {
+    if (D->n > 0 && (!D->pos || !D->vel || !D->cell_count ||
+                     !D->cfn || !D->cf_add || !D->wcf_active || !D->acc_force || !D->acc_moment || !D->cell_list ||
+                     D->cell_cap <= 0)) {
         set_error("dem: missing buffers");
         return LBDEM_ERR_ARG;
     }
@@ -571,7 +559,6 @@ int lbdem_dem_bin(lbdem_dem *D, void *stream) {
     if (cudaMemsetAsync(D->cell_count + (size_t)A.parity * A.ncell, 0, sizeof(int32_t) * A.ncell, st) != cudaSuccess)
         return check_launch("dem_bin memset");
     k_bin<<<(D->n + 127) / 128, 128, 0, st>>>(A);
-    k_scan<<<1, 1024, 0, st>>>(A);
     return check_launch("dem_bin");
 }
 
@@ -583,12 +570,47 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     DemArgs A;
     A.d = *D;
     A.ncell = D->gdim[0] * D->gdim[1] * D->gdim[2];
-    const int nb_int = max((D->n + 255) / 256, min(148, (A.ncell + 255) / 256));
+    const int nb_int = max((D->n + 127) / 128, min(148, (A.ncell + 127) / 128));
     const int nb_con = (int)((8ll * D->n + 127) / 128);
+    // "cluster": all sub-steps in one launch of a single thread-block cluster
+    // (opt-in: it confines the contact phase to <= 16 SMs and measured slower
+    // than two launches per sub-step spread over the whole GPU)
+    const char *mode = getenv("LBDEM_DEM_KERNELS");
+    if (mode && strcmp(mode, "cluster") == 0) {
+        // one cluster of up to 16 CTAs x 512 threads, sized to the contact lanes
+        int ncta = (int)((8ll * D->n + 511) / 512);
+        ncta = ncta < 1 ? 1 : (ncta > 16 ? 16 : ncta);
+        cudaFuncSetAttribute(k_dem_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        for (; ncta >= 1; ncta >>= 1) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(ncta, 1, 1);
+            cfg.blockDim = dim3(512, 1, 1);
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = ncta;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, k_dem_cluster, &cfg) != cudaSuccess || nclusters < 1) {
+                cudaGetLastError();
+                continue;
+            }
+            A.parity = D->parity;
+            if (cudaLaunchKernelEx(&cfg, k_dem_cluster, A, (int)nsub) == cudaSuccess) {
+                D->parity ^= (nsub & 1);
+                return check_launch("dem_substeps (cluster)");
+            }
+            cudaGetLastError();
+        }
+    }
     for (int s = 0; s < nsub; ++s) {
         A.parity = D->parity;
         k_contacts<<<nb_con, 128, 0, st>>>(A);
-        k_integrate<<<nb_int, 256, 0, st>>>(A);
+        k_integrate<<<nb_int, 128, 0, st>>>(A);
         D->parity ^= 1;
     }
     return check_launch("dem_substeps");

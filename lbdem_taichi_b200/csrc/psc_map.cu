@@ -105,7 +105,7 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
 constexpr int MAP_CHUNK = 2048;
 
 __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
-    __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32, w = local index
+    __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32; w = global cell index
     __shared__ int s_n;
     const int g = blockIdx.x;
     double xc, yc, zc, r;
@@ -126,21 +126,28 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     const double rr = r > 0.0 ? r * r : 0.0;
     const float band = (float)(1e-4 * (1.0 + rr));
     const float lo = (float)rr - band, hi = (float)rr + band;
-    const unsigned exy = (unsigned)ex * (unsigned)ey;
-    const unsigned tot = exy * (unsigned)ez;
+    const unsigned tot = (unsigned)ex * (unsigned)ey * (unsigned)ez;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int ii = lane / 5, jj = lane % 5;
+    // this thread's first cell, then advance by blockDim cells with carries
+    const unsigned bd = blockDim.x;
+    const int adx = (int)(bd % (unsigned)ex), ady = (int)((bd / (unsigned)ex) % (unsigned)ey);
+    const int adz = (int)(bd / ((unsigned)ex * (unsigned)ey));
+    int ix = (int)(threadIdx.x % (unsigned)ex), jy = (int)((threadIdx.x / (unsigned)ex) % (unsigned)ey);
+    int kz = (int)(threadIdx.x / ((unsigned)ex * (unsigned)ey));
     for (unsigned base = 0; base < tot; base += MAP_CHUNK) {
         if (threadIdx.x == 0) s_n = 0;
         __syncthreads();
         const unsigned lim = min(tot, base + MAP_CHUNK);
-        for (unsigned t = base + threadIdx.x; t < lim; t += blockDim.x) {
-            const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex, ix = rem - jy * (unsigned)ex;
-            const int i = x0 + (int)ix, j = y0 + (int)jy, k = z0 + (int)kz;
+        for (unsigned t = base + threadIdx.x; t < lim; t += bd) {
+            const int i = x0 + ix, j = y0 + jy, k = z0 + kz;
+            ix += adx; jy += ady; kz += adz;
+            if (ix >= ex) { ix -= ex; ++jy; }
+            if (jy >= ey) { jy -= ey; ++kz; }
             const float fx = (float)(xc - (double)i), fy = (float)(yc - (double)j), fz = (float)(zc - (double)k);
             const float d2 = (fx * fx + fy * fy) + fz * fz;
             if (d2 > out2 + marg_o) continue;                 // certainly dist >= t_out
-            const size_t c = ((size_t)k * a.ny + j) * a.nx + i;
+            const unsigned c = ((unsigned)k * (unsigned)a.ny + (unsigned)j) * (unsigned)a.nx + (unsigned)i;
             if (a.links[c] & LINK_MAP_SKIP) continue;
             int full;
             if (d2 < in2 - marg_i) {
@@ -157,39 +164,44 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
                 atomicMax(a.key + c, KEY_FULL | gbits);
             } else if (r > 0.0) {
                 const int slot = atomicAdd(&s_n, 1);
-                s_off[slot] = make_float4(fx, fy, fz, __int_as_float((int)(t - base)));
+                s_off[slot] = make_float4(fx, fy, fz, __uint_as_float(c));
             }
         }
         __syncthreads();
         const int n = s_n;
+        const float oxl = 0.4f - 0.2f * (float)ii, oyl = 0.4f - 0.2f * (float)jj;
         for (int e = warp; e < n; e += nwarp) {
             const float4 o = s_off[e];
-            int cnt = 0;
+            int cnt = 0, amb = 0;
             if (lane < 25) {
-                const float ox = o.x + (0.4f - 0.2f * (float)ii);
-                const float oy = o.y + (0.4f - 0.2f * (float)jj);
+                const float ox = o.x + oxl, oy = o.y + oyl;
                 const float sxy = ox * ox + oy * oy;
 #pragma unroll
                 for (int kk = 0; kk < 5; ++kk) {
                     const float oz = o.z + (0.4f - 0.2f * (float)kk);
                     const float s = sxy + oz * oz;
-                    if (s < lo) {
-                        ++cnt;
-                    } else if (s <= hi) {
-                        const unsigned t = base + (unsigned)__float_as_int(o.w);
-                        const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex;
-                        const int i = x0 + (int)(rem - jy * (unsigned)ex), j = y0 + (int)jy, k = z0 + (int)kz;
-                        cnt += subcell_inside_exact(xc, yc, zc, i, j, k, ii, jj, kk, r);
+                    cnt += s < lo;
+                    amb |= (s >= lo) & (s <= hi);
+                }
+            }
+            const unsigned c = __float_as_uint(o.w);
+            if (__any_sync(0xffffffffu, amb)) {
+                // rare: re-test the sub-points near the surface exactly (FP64)
+                const int i = (int)(c % (unsigned)a.nx), j = (int)((c / (unsigned)a.nx) % (unsigned)a.ny);
+                const int k = (int)(c / ((unsigned)a.nx * (unsigned)a.ny));
+                if (amb) {
+                    const float ox = o.x + oxl, oy = o.y + oyl;
+                    const float sxy = ox * ox + oy * oy;
+                    for (int kk = 0; kk < 5; ++kk) {
+                        const float oz = o.z + (0.4f - 0.2f * (float)kk);
+                        const float s = sxy + oz * oz;
+                        if (s >= lo && s <= hi) cnt += subcell_inside_exact(xc, yc, zc, i, j, k, ii, jj, kk, r);
                     }
                 }
             }
             cnt = __reduce_add_sync(0xffffffffu, cnt);
-            if (lane == 0 && cnt > 0) {   // eps = 0 never beats the empty cell (strict >)
-                const unsigned t = base + (unsigned)__float_as_int(o.w);
-                const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex;
-                const int i = x0 + (int)(rem - jy * (unsigned)ex), j = y0 + (int)jy, k = z0 + (int)kz;
-                atomicMax(a.key + ((size_t)k * a.ny + j) * a.nx + i, ((uint32_t)cnt << 24) | gbits);
-            }
+            if (lane == 0 && cnt > 0)   // eps = 0 never beats the empty cell (strict >)
+                atomicMax(a.key + c, ((uint32_t)cnt << 24) | gbits);
         }
         __syncthreads();
     }

@@ -218,14 +218,16 @@ class DEMSolver:
         gdim = ext + 4          # reference cells -1 .. ext+2
         self.gdim = gdim
         ncell = int(np.prod(gdim))
+        # list capacity of a broad-phase cell: the most spheres of the smallest
+        # diameter a cube of edge cell_size can hold at random close packing
+        # (0.64), doubled, at least 16
+        rmin = float(radius.min()) if n else rmax
+        cap = int(np.ceil(2.0 * 0.64 * self.cell_size ** 3 / (4.0 / 3.0 * np.pi * rmin ** 3)))
+        self.cell_cap = int(min(max(16, cap), 1024))
         self.cell_count = torch.zeros(2 * ncell, **i32)
-        self.cell_start = torch.zeros(ncell, **i32)
-        self.pcell = torch.zeros(max(n, 1), **i32)
-        self.prank = torch.zeros(max(n, 1), **i32)
-        self.sorted = torch.zeros(max(n, 1), **i32)
+        self.cell_list = torch.zeros(ncell * self.cell_cap, **i32)
         self.acc_force = torch.zeros((max(n, 1), 3), **f64)
         self.acc_moment = torch.zeros((max(n, 1), 3), **f64)
-        self.blocks_done = torch.zeros(1, **i32)
         # the reference hashes cells into a 2^k table: distinct cells alias when
         # their coordinates agree in the low bits kept by Morton-code mod 2^k
         T = reference_table_size(rmax, dmin, dmax) if n else 1 << 20
@@ -262,11 +264,10 @@ class DEMSolver:
                           ("cf_shear", self.cf_shear), ("cf_pos", self.cf_pos), ("cf_force", self.cf_force),
                           ("wcf_active", self.wcf_active), ("wcf_shear", self.wcf_shear),
                           ("wcf_pos", self.wcf_pos), ("wcf_force", self.wcf_force),
-                          ("cell_count", self.cell_count), ("cell_start", self.cell_start),
-                          ("pcell", self.pcell), ("prank", self.prank), ("sorted", self.sorted),
-                          ("acc_force", self.acc_force), ("acc_moment", self.acc_moment),
-                          ("blocks_done", self.blocks_done)):
+                          ("cell_count", self.cell_count), ("cell_list", self.cell_list),
+                          ("acc_force", self.acc_force), ("acc_moment", self.acc_moment)):
             setattr(d, name, N.ptr(ten))
+        d.cell_cap = self.cell_cap
         d.parity = 0
         d.status = N.ptr(self.status)
         self._binned = False
