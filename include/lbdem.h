@@ -203,6 +203,21 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream);
 int lbdem_global_sums_f64(const lbdem_lattice *L, int32_t buf, double *out, double *partials,
                           void *stream);
 
+/* Same totals as lbdem_global_sums_f64 without any caller scratch and without
+ * allocating: for callers that own the lattice buffers but have no device
+ * allocator of their own -- a host reaching the library only through this C
+ * ABI with buffers lent by another component, or a process whose GPU memory is
+ * fully reserved by a framework's caching allocator.  No counterpart in the
+ * reference.  The block partials live in a library-owned device array of
+ * 4 * 4096 doubles (32 KB, held by every GPU that loads the library until the
+ * process exits), which covers lattices of up to 2^28 cells; larger lattices
+ * return LBDEM_ERR_ARG.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Every call shares the array: calls that may overlap on the GPU
+ * (different streams without ordering) race; each call overwrites every
+ * partial it reads, so no clearing is needed between calls. */
+int lbdem_global_sums_f64_noalloc(const lbdem_lattice *L, int32_t buf, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

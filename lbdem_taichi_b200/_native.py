@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liblbdem.so")
 
 LBDEM_OK = 0
+LBDEM_ERR_ARG, LBDEM_ERR_LAUNCH, LBDEM_ERR_UNSUPPORTED = 1, 2, 3
 ST_NAN, ST_RHO, ST_VELMAX = 1, 2, 4
 ST_CONTACT_OVERFLOW, ST_GRID_OVERFLOW, ST_GID_OVERFLOW, ST_CELL_OVERFLOW = 8, 16, 32, 64
 ST_WAIT_TIMEOUT = 128
@@ -86,6 +87,7 @@ EXPORTS = {
     "lbdem_dem_bin": ([vp, vp], C.c_int),
     "lbdem_dem_substeps": ([vp, C.c_int32, vp], C.c_int),
     "lbdem_global_sums_f64": ([vp, C.c_int32, vp, vp, vp], C.c_int),
+    "lbdem_global_sums_f64_noalloc": ([vp, C.c_int32, vp, vp], C.c_int),
 }
 
 _lib = None
@@ -94,7 +96,7 @@ _lib = None
 KERNELS_PER_CALL = {"lbdem_build_links": 2, "lbdem_lattice_init": 1, "lbdem_psc_map": 2,
                     "lbdem_psc_step_f32": 1, "lbdem_psc_step_f16": 1, "lbdem_psc_step_bf16": 1,
                     "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
-                    "lbdem_global_sums_f64": 2}
+                    "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2}
 _launches = [0]
 
 

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -1257,6 +1258,66 @@ static int launch_sums(const lbdem_lattice *L, int buf, double *out, double *par
     return check_launch("global_sums");
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free FP64 totals: the block partials live in a file-scope device
+// array instead of caller scratch.  One block per NOALLOC_CELLS_PER_BLOCK
+// cells, at most NOALLOC_MAX_BLOCKS blocks, so lattices of up to
+// 4096 * 65536 = 2^28 cells are covered (32 KB of device memory, held by every
+// GPU that loads the library until the process exits).
+// ---------------------------------------------------------------------------
+constexpr int NOALLOC_MAX_BLOCKS = 4096;
+constexpr size_t NOALLOC_CELLS_PER_BLOCK = 65536;
+static __device__ __align__(256) double g_noalloc_partials[4 * NOALLOC_MAX_BLOCKS];
+
+// Device address of g_noalloc_partials for the current device, looked up once
+// per device (the host-side symbol is only a stand-in and must never be passed
+// to a kernel).
+static double *noalloc_partials_address() {
+    static std::mutex mu;
+    static double *addr[256] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+        set_error("global_sums_f64_noalloc: no current CUDA device");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || !p) {
+            set_error("global_sums_f64_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return nullptr;
+        }
+        addr[dev] = static_cast<double *>(p);
+    }
+    return addr[dev];
+}
+
+template <typename T>
+static int launch_sums_noalloc(const lbdem_lattice *L, int buf, double *out, cudaStream_t st) {
+    StepArgs a;
+    int rc = fill_args(L, a);
+    if (rc) return rc;
+    if (buf < 0 || buf > 1 || !out) {
+        set_error("global_sums_f64_noalloc: bad arguments");
+        return LBDEM_ERR_ARG;
+    }
+    const size_t nb = (a.nc + NOALLOC_CELLS_PER_BLOCK - 1) / NOALLOC_CELLS_PER_BLOCK;
+    if (nb > (size_t)NOALLOC_MAX_BLOCKS) {
+        set_error("global_sums_f64_noalloc: lattice has %zu cells; the allocation-free sums cover at most %zu "
+                  "cells (use lbdem_global_sums_f64 with caller scratch)",
+                  a.nc, (size_t)NOALLOC_MAX_BLOCKS * NOALLOC_CELLS_PER_BLOCK);
+        return LBDEM_ERR_ARG;
+    }
+    double *partials = noalloc_partials_address();
+    if (!partials) return LBDEM_ERR_LAUNCH;
+    a.src = L->f[buf];
+    // every block writes its own four partials, so nothing needs clearing
+    k_sums<T><<<(unsigned)nb, 256, 0, st>>>(a, partials);
+    k_sums_final<<<1, 32, 0, st>>>(partials, (int)nb, out);
+    return check_launch("global_sums_f64_noalloc");
+}
+
 }  // namespace lbdem
 
 using namespace lbdem;
@@ -1331,6 +1392,18 @@ int lbdem_psc_decode(const lbdem_lattice *L, const lbdem_psc *P, int32_t *id, fl
         case LBDEM_F32: return launch_decode<float>(L, P, id, volfrac, weight, velsolid, st);
         case LBDEM_F16: return launch_decode<__half>(L, P, id, volfrac, weight, velsolid, st);
         case LBDEM_BF16: return launch_decode<__nv_bfloat16>(L, P, id, volfrac, weight, velsolid, st);
+    }
+    set_error("unknown storage form %d", L->storage);
+    return LBDEM_ERR_ARG;
+}
+
+int lbdem_global_sums_f64_noalloc(const lbdem_lattice *L, int32_t buf, double *out, void *stream) {
+    if (!L) return LBDEM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (L->storage) {
+        case LBDEM_F32: return launch_sums_noalloc<float>(L, buf, out, st);
+        case LBDEM_F16: return launch_sums_noalloc<__half>(L, buf, out, st);
+        case LBDEM_BF16: return launch_sums_noalloc<__nv_bfloat16>(L, buf, out, st);
     }
     set_error("unknown storage form %d", L->storage);
     return LBDEM_ERR_ARG;
