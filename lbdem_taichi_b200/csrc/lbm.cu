@@ -55,6 +55,7 @@ struct StepArgs {
     float *hydro_out;
     int32_t *status;
     int kernel_choice;         // LBDEM_STEP_KERNEL: 0 default, 1 one cell/thread, 2 two cells/thread, 3 staged rows
+    uint32_t qoff[Q];          // q * Ncells: element offset of population q (kernel-parameter constants)
 };
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
@@ -469,31 +470,38 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
     const uint32_t cell = inb ? (uint32_t)(z * ny + y) * (uint32_t)nx + (uint32_t)x : 0u;
     // Issue the 19 gather loads first (their addresses never depend on the
     // link mask), then resolve the link mask and re-fetch bounce-back
-    // directions on the few cells next to an obstacle.
+    // directions on the few cells next to an obstacle.  Element indices are
+    // 32-bit: the source cell of direction q is a wrapped row base (9 per
+    // thread) plus a wrapped x offset, plus q*Ncells from the parameters.
     const int xc_ = inb ? x : 0, yc_ = inb ? y : 0;
     const uint32_t cellc = inb ? cell : 0u;
+    const uint32_t unx = (uint32_t)nx, nxy = (uint32_t)nx * (uint32_t)ny;
     const T *__restrict__ src = (const T *)a.src;
     T raw[Q];
     if (GATHER) {
-        const int xm = xc_ == 0 ? nx - 1 : xc_ - 1, xp = xc_ == nx - 1 ? 0 : xc_ + 1;
-        const int ym = yc_ == 0 ? ny - 1 : yc_ - 1, yp = yc_ == ny - 1 ? 0 : yc_ + 1;
-        const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+        const uint32_t r0 = (uint32_t)(z * ny + yc_) * unx;
+        const uint32_t dym = yc_ == 0 ? (uint32_t)(ny - 1) * unx : (uint32_t)(-(int)nx);
+        const uint32_t dyp = yc_ == ny - 1 ? (uint32_t)(-(int)((ny - 1) * nx)) : unx;
+        const uint32_t dzm = z == 0 ? (uint32_t)(nz - 1) * nxy : (uint32_t)(-(int)nxy);
+        const uint32_t dzp = z == nz - 1 ? (uint32_t)(-(int)((nz - 1) * nxy)) : nxy;
+        const uint32_t xm = xc_ == 0 ? (uint32_t)(nx - 1) : (uint32_t)(xc_ - 1);
+        const uint32_t xp = xc_ == nx - 1 ? 0u : (uint32_t)(xc_ + 1);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const int xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : xc_);
-            const int ys = cy(q) == 1 ? ym : (cy(q) == -1 ? yp : yc_);
-            const int zs = cz(q) == 1 ? zm : (cz(q) == -1 ? zp : z);
-            raw[q] = Store<T>::ld(src + (size_t)q * nc + ((uint32_t)(zs * ny + ys) * (uint32_t)nx + xs));
+            const uint32_t ry = cy(q) == 1 ? dym : (cy(q) == -1 ? dyp : 0u);
+            const uint32_t rz = cz(q) == 1 ? dzm : (cz(q) == -1 ? dzp : 0u);
+            const uint32_t xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : (uint32_t)xc_);
+            raw[q] = Store<T>::ld(src + (r0 + ry + rz + xs + a.qoff[q]));
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) raw[q] = Store<T>::ld(src + (size_t)q * nc + cellc);
+        for (int q = 0; q < Q; ++q) raw[q] = Store<T>::ld(src + (cellc + a.qoff[q]));
     }
     float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
     if (SMAG == LBDEM_SMAG_REFERENCE && inb) {
         const T *ax = (const T *)a.aux;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ax[k * nc + cell]);
+        for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ax[cell + a.qoff[k]]);
     }
     const uint32_t key = (a.key != nullptr && inb) ? a.key[cell] : 0u;
     uint32_t lk = LINK_FLUID;
@@ -502,7 +510,7 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
     if (GATHER && (lk & 0x7FFFEu)) {
 #pragma unroll
         for (int q = 1; q < Q; ++q)
-            if (lk & LINK_BB(q)) raw[q] = Store<T>::ld(src + (size_t)qinv(q) * nc + cellc);
+            if (lk & LINK_BB(q)) raw[q] = Store<T>::ld(src + (cellc + a.qoff[qinv(q)]));
     }
     float d[Q];
 #pragma unroll
@@ -513,11 +521,11 @@ __global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
     if (act) {
         T *dst = (T *)a.dst;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) dst[(size_t)q * nc + cell] = Store<T>::enc(d[q], a.enc / wq(q));
+        for (int q = 0; q < Q; ++q) dst[cell + a.qoff[q]] = Store<T>::enc(d[q], a.enc / wq(q));
         if (SMAG == LBDEM_SMAG_REFERENCE) {
             T *ax = (T *)a.aux;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) ax[k * nc + cell] = aux_enc<T>(aux[k]);
+            for (int k = 0; k < 5; ++k) ax[cell + a.qoff[k]] = aux_enc<T>(aux[k]);
         }
     }
     if (a.key != nullptr) reduce_forces(a, gid, hx, hy, hz, tx, ty, tz);
@@ -599,17 +607,22 @@ __global__ void __launch_bounds__(128) k_psc_step2(const StepArgs a) {
     const unsigned lane = lane_id();
     const T *__restrict__ src = (const T *)a.src;
     V rv[Q];   // streamed populations of cells (x0, x0+1)
+    const uint32_t unx = (uint32_t)nx, nxy = (uint32_t)nx * (uint32_t)ny;
     if (GATHER) {
-        const int ym = yc_ == 0 ? ny - 1 : yc_ - 1, yp = yc_ == ny - 1 ? 0 : yc_ + 1;
-        const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+        const uint32_t r0 = (uint32_t)(z * ny + yc_) * unx;
+        const uint32_t dym = yc_ == 0 ? (uint32_t)(ny - 1) * unx : (uint32_t)(-(int)nx);
+        const uint32_t dyp = yc_ == ny - 1 ? (uint32_t)(-(int)((ny - 1) * nx)) : unx;
+        const uint32_t dzm = z == 0 ? (uint32_t)(nz - 1) * nxy : (uint32_t)(-(int)nxy);
+        const uint32_t dzp = z == nz - 1 ? (uint32_t)(-(int)((nz - 1) * nxy)) : nxy;
         // x of the element just left of this warp's 64 cells, and just right of them
         const int wx0 = x0 - 2 * (int)lane;
-        const int xl = wx0 == 0 ? nx - 1 : wx0 - 1, xr = wx0 + 64 == nx ? 0 : wx0 + 64;
+        const uint32_t xl = wx0 == 0 ? (uint32_t)(nx - 1) : (uint32_t)(wx0 - 1);
+        const uint32_t xr = wx0 + 64 == nx ? 0u : (uint32_t)(wx0 + 64);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const int ys = cy(q) == 1 ? ym : (cy(q) == -1 ? yp : yc_);
-            const int zs = cz(q) == 1 ? zm : (cz(q) == -1 ? zp : z);
-            const T *row = src + (size_t)q * nc + (uint32_t)(zs * ny + ys) * (uint32_t)nx;
+            const uint32_t ry = cy(q) == 1 ? dym : (cy(q) == -1 ? dyp : 0u);
+            const uint32_t rz = cz(q) == 1 ? dzm : (cz(q) == -1 ? dzp : 0u);
+            const T *row = src + (r0 + ry + rz + a.qoff[q]);
             const V v = P::ld(row + x0);
             if (cx(q) == 0) {
                 rv[q] = v;
@@ -625,13 +638,13 @@ __global__ void __launch_bounds__(128) k_psc_step2(const StepArgs a) {
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) rv[q] = P::ld(src + (size_t)q * nc + cell0);
+        for (int q = 0; q < Q; ++q) rv[q] = P::ld(src + (cell0 + a.qoff[q]));
     }
     float2 aux[5] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(a.omega0)};
     if (SMAG == LBDEM_SMAG_REFERENCE && inb) {
         const T *ax = (const T *)a.aux;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) aux[k] = P::adec(P::ld(ax + k * nc + cell0));
+        for (int k = 0; k < 5; ++k) aux[k] = P::adec(P::ld(ax + (cell0 + a.qoff[k])));
     }
     uint2 key = make_uint2(0u, 0u);
     if (a.key != nullptr && inb) key = *reinterpret_cast<const uint2 *>(a.key + cell0);
@@ -645,8 +658,8 @@ __global__ void __launch_bounds__(128) k_psc_step2(const StepArgs a) {
     if (GATHER && ((la | lb) & 0x7FFFEu)) {
 #pragma unroll
         for (int q = 1; q < Q; ++q) {
-            const T lo = (la & LINK_BB(q)) ? Store<T>::ld(src + (size_t)qinv(q) * nc + cell0) : P::lo(rv[q]);
-            const T hi = (lb & LINK_BB(q)) ? Store<T>::ld(src + (size_t)qinv(q) * nc + cell0 + 1) : P::hi(rv[q]);
+            const T lo = (la & LINK_BB(q)) ? Store<T>::ld(src + (cell0 + a.qoff[qinv(q)])) : P::lo(rv[q]);
+            const T hi = (lb & LINK_BB(q)) ? Store<T>::ld(src + (cell0 + 1 + a.qoff[qinv(q)])) : P::hi(rv[q]);
             rv[q] = P::make(lo, hi);
         }
     }
@@ -663,26 +676,26 @@ __global__ void __launch_bounds__(128) k_psc_step2(const StepArgs a) {
     T *dst = (T *)a.dst;
     if (acta && actb) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) P::st(dst + (size_t)q * nc + cell0, P::enc(d[q], a.enc / wq(q)));
+        for (int q = 0; q < Q; ++q) P::st(dst + (cell0 + a.qoff[q]), P::enc(d[q], a.enc / wq(q)));
         if (SMAG == LBDEM_SMAG_REFERENCE) {
             T *ax = (T *)a.aux;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) P::st(ax + k * nc + cell0, P::aenc(aux[k]));
+            for (int k = 0; k < 5; ++k) P::st(ax + (cell0 + a.qoff[k]), P::aenc(aux[k]));
         }
     } else if (acta || actb) {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const V v = P::enc(d[q], a.enc / wq(q));
-            if (acta) dst[(size_t)q * nc + cell0] = P::lo(v);
-            if (actb) dst[(size_t)q * nc + cell0 + 1] = P::hi(v);
+            if (acta) dst[cell0 + a.qoff[q]] = P::lo(v);
+            if (actb) dst[cell0 + 1 + a.qoff[q]] = P::hi(v);
         }
         if (SMAG == LBDEM_SMAG_REFERENCE) {
             T *ax = (T *)a.aux;
 #pragma unroll
             for (int k = 0; k < 5; ++k) {
                 const V v = P::aenc(aux[k]);
-                if (acta) ax[k * nc + cell0] = P::lo(v);
-                if (actb) ax[k * nc + cell0 + 1] = P::hi(v);
+                if (acta) ax[cell0 + a.qoff[k]] = P::lo(v);
+                if (actb) ax[cell0 + 1 + a.qoff[k]] = P::hi(v);
             }
         }
     }
@@ -1051,13 +1064,15 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
         set_error("invalid lattice descriptor");
         return LBDEM_ERR_ARG;
     }
-    if ((size_t)L->nx * L->ny * L->nz >= (1ull << 32)) {
-        set_error("lattice has %zu cells; at most 2^32-1 supported", (size_t)L->nx * L->ny * L->nz);
+    if ((size_t)L->nx * L->ny * L->nz * Q >= (1ull << 32)) {
+        set_error("lattice has %zu cells; element offsets are 32-bit, so at most %llu cells are supported",
+                  (size_t)L->nx * L->ny * L->nz, (unsigned long long)((1ull << 32) / Q - 1));
         return LBDEM_ERR_ARG;
     }
     memset(&a, 0, sizeof(a));
     a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
     a.nc = (size_t)L->nx * L->ny * L->nz;
+    for (int q = 0; q < Q; ++q) a.qoff[q] = (uint32_t)(q * a.nc);
     a.omega0 = L->omega0;
     a.inv_omega0 = 1.f / L->omega0;
     a.smag_c2 = L->smag_cs * L->smag_cs;
