@@ -11,12 +11,18 @@
  *    detected on the host).  Numerical/capacity faults found on the device are
  *    OR-ed into a caller-provided int32 status word (LBDEM_ST_* bits) that the
  *    caller reads at a synchronisation point of its choice.
- *  - Lattice arrays are structure-of-arrays, x fastest: cell (x, y, z) ->
- *    (z*Ny + y)*Nx + x; population q of a cell at q*Ncells + cell.
+ *  - Per-cell arrays (rho, vel, links, keys, ...) are x fastest: cell
+ *    (x, y, z) -> (z*Ny + y)*Nx + x, vector fields as SoA planes of Ncells.
  *    (The reference's Taichi fields are indexed [i, j, k] = [x, y, z].)
- *  - Populations are stored as deviations from the lattice weights,
- *    d_q = f_q - w_q (FP32 form), or h_q = (f_q - w_q) * scale16 / w_q
- *    (FP16 / BF16 forms); arithmetic is FP32 in every form.
+ *  - Populations are blocked by 32 cells along x: with NB = ceil(Nx/32),
+ *    population q of cell (x, y, z) is element
+ *        ((z*Ny + y)*NB + x/32)*19*32 + q*32 + x%32
+ *    (buffer of 19*32*NB*Ny*Nz elements; lanes x >= Nx of the last block are
+ *    padding).  The lagged Smagorinsky state uses the same blocking with 5
+ *    values per cell.
+ *  - Populations are stored as scaled deviations from the lattice weights,
+ *    h_q = (f_q - w_q) * S / w_q with S = 1 (FP32) or scale16 (FP16 / BF16);
+ *    arithmetic is FP32 in every form.
  *  - Particle (DEM) state is FP64, array-of-structures (n, 3) like the
  *    reference's Grain fields.
  *
@@ -96,10 +102,10 @@ typedef struct lbdem_lattice {
     int32_t force_on;      /* 1: add w_q rho (c_q . F)/cs^2 to post-collision populations */
     float force[3];        /* body force, lattice units */
     float scale16;         /* storage scale of the 16-bit forms */
-    void *f[2];            /* population buffers, 19*Ncells elements of the storage type */
+    void *f[2];            /* population buffers, 19*32*NB*Ny*Nz elements of the storage type (blocked) */
     float *rho;            /* Ncells, FP32 (moments; also the initial state) */
     float *vel;            /* 3*Ncells, FP32 SoA (ux | uy | uz) */
-    void *aux;             /* LBDEM_SMAG_REFERENCE: 5*Ncells of the storage type, else NULL */
+    void *aux;             /* LBDEM_SMAG_REFERENCE: 5*32*NB*Ny*Nz of the storage type (blocked), else NULL */
     const uint32_t *links; /* per-cell link mask from lbdem_build_links */
     const uint8_t *row_simple; /* per (y,z) row: 1 = row and its 8 neighbour rows all plain FLUID */
     int32_t *status;       /* device status word */

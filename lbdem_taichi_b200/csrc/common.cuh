@@ -30,6 +30,10 @@ __host__ __device__ constexpr float wq(int q) {
     return q == 0 ? 1.0f / 3.0f : (q <= 6 ? 1.0f / 18.0f : 1.0f / 36.0f);
 }
 constexpr float CS2 = 1.0f / 3.0f;
+// Blocked population layout: 32 cells per x-block, QB elements per block of
+// populations, AB per block of the 5 lagged Smagorinsky values.
+constexpr uint32_t QB = Q * 32;
+constexpr uint32_t AB = 5 * 32;
 
 // Per-cell link mask (built once from CellType by lbdem_build_links)
 constexpr uint32_t LINK_SKIP = 1u << 19;   // cell is not updated (OBSTACLE / VEL_LADD / FREE_SLIP [/ INLET])
@@ -37,23 +41,31 @@ constexpr uint32_t LINK_FLUID = 1u << 20;  // FLUID: moments are recomputed
 constexpr uint32_t LINK_MAP_SKIP = 1u << 21;  // PSC map skips the cell
 __host__ __device__ constexpr uint32_t LINK_BB(int q) { return 1u << q; }  // neighbour x-c_q is OBSTACLE
 
-// Storage forms.  FP32 stores d = f - w; 16-bit forms store
-// h = (f - w) * scale / w (scale = scale16), decoded as d = h * w / scale.
+// Storage forms.  Every form stores the scaled deviation
+// h = (f - w) * S / w (S = 1 for FP32, scale16 for the 16-bit forms): the
+// step computes in h directly (widen/narrow), the auxiliary kernels decode
+// d = f - w = h * w / S (dec) and encode h = d * S / w (enc).
 template <typename T> struct Store;
 template <> struct Store<float> {
     static constexpr int kind = LBDEM_F32;
-    __device__ __forceinline__ static float dec(float v, float /*wscale*/) { return v; }
-    __device__ __forceinline__ static float enc(float d, float /*inv_wscale*/) { return d; }
+    __device__ __forceinline__ static float widen(float v) { return v; }
+    __device__ __forceinline__ static float narrow(float h) { return h; }
+    __device__ __forceinline__ static float dec(float v, float wscale) { return v * wscale; }
+    __device__ __forceinline__ static float enc(float d, float inv_wscale) { return d * inv_wscale; }
     __device__ __forceinline__ static float ld(const float *p) { return __ldg(p); }
 };
 template <> struct Store<__half> {
     static constexpr int kind = LBDEM_F16;
+    __device__ __forceinline__ static float widen(__half v) { return __half2float(v); }
+    __device__ __forceinline__ static __half narrow(float h) { return __float2half_rn(h); }
     __device__ __forceinline__ static float dec(__half v, float wscale) { return __half2float(v) * wscale; }
     __device__ __forceinline__ static __half enc(float d, float inv_wscale) { return __float2half_rn(d * inv_wscale); }
     __device__ __forceinline__ static __half ld(const __half *p) { return __ldg(p); }
 };
 template <> struct Store<__nv_bfloat16> {
     static constexpr int kind = LBDEM_BF16;
+    __device__ __forceinline__ static float widen(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ __forceinline__ static __nv_bfloat16 narrow(float h) { return __float2bfloat16_rn(h); }
     __device__ __forceinline__ static float dec(__nv_bfloat16 v, float wscale) { return __bfloat162float(v) * wscale; }
     __device__ __forceinline__ static __nv_bfloat16 enc(float d, float inv_wscale) {
         return __float2bfloat16_rn(d * inv_wscale);

@@ -1,12 +1,17 @@
 // Lattice kernels: the fused PSC collide-stream step and its helpers.
 //
-// Data layout (HBM): populations are structure-of-arrays, x fastest,
-// population q of cell c at q*Ncells + c, in two buffers (pull scheme: the
-// step reads post-collision populations of the previous step from f[src],
-// streams them by gathering from the 18 upwind neighbours, collides, and
-// writes post-collision populations of this step to f[dst]).  One thread per
-// cell, 32 consecutive x per warp, so every direction is one coalesced
-// 128 B (FP32) / 64 B (16-bit) access per warp (+1 element shift for c_x != 0).
+// Data layout (HBM): populations are blocked by 32 cells along x ("AoSoA"):
+// row r = z*Ny + y holds ceil(Nx/32) x-blocks, each block 19 populations x
+// 32 lanes, so population q of cell (x, y, z) is element
+//   (r * NB + x/32) * 19*32 + q*32 + x%32,   NB = ceil(Nx/32),
+// in two buffers (pull scheme: the step reads post-collision populations of
+// the previous step from f[src], streams them by gathering from the 18 upwind
+// neighbours, collides, and writes post-collision populations of this step to
+// f[dst]).  One thread per cell, a warp is one x-block, so every direction is
+// one coalesced 128 B (FP32) / 64 B (16-bit) access per warp (+1 element
+// shift for c_x != 0), and all 19 populations of a cell sit at compile-time
+// offsets q*32 from one address.  The lagged Smagorinsky state (5 values per
+// cell) uses the same blocking with 5 instead of 19.
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -38,11 +43,12 @@ int check_launch(const char *what) {
 struct StepArgs {
     int nx, ny, nz;
     size_t nc;
-    float omega0, inv_omega0, smag_c2;
-    int force_on;
-    float f3x, f3y, f3z;   // 3 * body force (1/cs^2 folded in)
-    float dec;             // w_q * dec = decode factor of population q (16-bit forms)
-    float enc;             // enc / w_q = encode factor
+    float omega0, inv_omega0, smag_k;   // smag_k = 4.5 Cs^2 (strain-rate factor folded)
+    float S;                            // storage scale: h = (f - w) S / w
+    float W0, W1, W2;                   // lattice weights / S (moments from h)
+    float g3x, g3y, g3z;                // 3 S F: body force in h units per unit density
+    float dec;                          // 1/S  (f - w = h w dec; auxiliary kernels)
+    float enc;                          // S
     const void *src;
     void *dst;
     void *aux;
@@ -54,8 +60,9 @@ struct StepArgs {
     double *force_fluid, *moment_fluid;
     float *hydro_out;
     int32_t *status;
-    int kernel_choice;         // LBDEM_STEP_KERNEL: 0 default, 1 one cell/thread, 2 two cells/thread, 3 staged rows
-    uint32_t qoff[Q];          // q * Ncells: element offset of population q (kernel-parameter constants)
+    uint32_t nb;               // x-blocks per row, ceil(Nx / 32)
+    uint32_t rs;               // population elements per row, nb * 19 * 32
+    uint32_t ars;              // auxiliary elements per row, nb * 5 * 32
 };
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
@@ -65,811 +72,389 @@ __device__ __forceinline__ unsigned lane_id() {
     return (threadIdx.y * blockDim.x + threadIdx.x) & 31u;
 }
 
+// Hardware reciprocal and square root (PTX rcp.approx / sqrt.approx, at most
+// one ulp from the rounded result): the step uses them for 1/rho, the
+// Smagorinsky relaxation frequency and the PSC weight, where an ulp is far
+// below the FP32 tolerance of the whole step.
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_fast(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // ---------------------------------------------------------------------------
-// fused step: per-cell collision (shared by the 1- and 2-cell kernels)
+// Lane-generic arithmetic: the collision is written over a value type V with
+// Lanes<V> (cells per value) so that a packed form can reuse it; the step
+// instantiates it for V = float, one cell per thread.
 // ---------------------------------------------------------------------------
-// d[]: deviations f - w of the streamed populations, overwritten with the
-// post-collision deviations.  aux[5]: previous (drho, ux, uy, uz, omega) in,
-// current out (reference Smagorinsky mode).  key: PSC owner key of the cell.
-// Outputs gid (-1 if no solid) and the cell's hydrodynamic force h and torque
-// arm product t (lattice units).
-template <int SMAG>
-__device__ __forceinline__ void collide_cell(const StepArgs &a, float d[Q], bool act, uint32_t cell, int x, int y,
-                                             int z, float aux[5], uint32_t key, int &gid, float &hx, float &hy,
-                                             float &hz, float &tx, float &ty, float &tz) {
-    // D3Q19 directions come in opposite pairs (q, q+1) for odd q (c_{q+1} = -c_q):
-    // symmetric sums sp = d_q + d_{q+1} and antisymmetric sums am = d_q - d_{q+1}
-    // carry every moment needed below.
-    float sp[9], am[9];
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+
+template <class V> struct Lanes;
+template <> struct Lanes<float> {
+    static constexpr int N = 1;
+    __device__ __forceinline__ static float splat(float s) { return s; }
+    __device__ __forceinline__ static float get(float v, int) { return v; }
+    __device__ __forceinline__ static void set(float &v, int, float s) { v = s; }
+    __device__ __forceinline__ static float rcp(float v) { return rcp_fast(v); }
+    __device__ __forceinline__ static float sqrt(float v) { return sqrt_fast(v); }
+};
+// c_q . (x, y, z) for odd q (whose first non-zero component is +1), with the
+// zero components dropped at compile time (q is a constant after unrolling;
+// 0 * v is not foldable under IEEE rules).
+template <class V>
+__device__ __forceinline__ V cdot(int q, V x, V y, V z) {
+    V r = x;
+    bool first = true;
+    if (cx(q)) { r = x; first = false; }
+    if (cy(q)) { r = first ? y : (cy(q) > 0 ? r + y : r - y); first = false; }
+    if (cz(q)) { r = first ? z : (cz(q) > 0 ? r + z : r - z); }
+    return r;
+}
+
+// Per-cell results of the collision needed by the force reduction.
+struct CellForce {
+    int gid;                       // owner particle, -1 if none
+    float hx, hy, hz, tx, ty, tz;  // hydrodynamic force and torque (lattice units)
+};
+
+// PSC quantities of one cell owned by a particle (psclattice3d.py:144-182;
+// B from the current omega as hybridlattice.py:236-245): weight B, 3 u_s,
+// and the cell's force B (j - rho u_s) with its torque about the centre.
+__device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float om, float rho, float jx, float jy,
+                                          float jz, int x, int y, int z, float &s3x, float &s3y, float &s3z,
+                                          CellForce &cf) {
+    cf.gid = (int)key_gid(key);
+    const float eps = (key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f);
+    const float taum = rcp_fast(om) - 0.5f;
+    const float Bw = eps * taum * rcp_fast((1.f - eps) + taum);
+    const float4 t0 = a.table[4 * cf.gid + 0], t1 = a.table[4 * cf.gid + 1];
+    const float4 t2 = a.table[4 * cf.gid + 2], t3 = a.table[4 * cf.gid + 3];
+    const float rx = ((float)x - t0.x) - t1.x;
+    const float ry = ((float)y - t0.y) - t1.y;
+    const float rz = ((float)z - t0.z) - t1.z;
+    const float sx = t2.x + (t3.y * rz - t3.z * ry);
+    const float sy = t2.y + (t3.z * rx - t3.x * rz);
+    const float sz = t2.z + (t3.x * ry - t3.y * rx);
+    s3x = 3.f * sx; s3y = 3.f * sy; s3z = 3.f * sz;
+    cf.hx = Bw * fmaf(-rho, sx, jx);
+    cf.hy = Bw * fmaf(-rho, sy, jy);
+    cf.hz = Bw * fmaf(-rho, sz, jz);
+    cf.tx = ry * cf.hz - rz * cf.hy;
+    cf.ty = rz * cf.hx - rx * cf.hz;
+    cf.tz = rx * cf.hy - ry * cf.hx;
+    return Bw;
+}
+
+// ---------------------------------------------------------------------------
+// fused step: collision in scaled-deviation ("h") form
+// ---------------------------------------------------------------------------
+// Populations are carried as h_q = (f_q - w_q) S / w_q.  Because w_q = w_qbar,
+// the BGK, PSC and body-force updates of the reference are w-free in h:
+//   feq_h = S (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2))      (compute_feq)
+//   g_h   = 3 S rho (c.F)                          (ForcedLattice3D, added last)
+// and the weights only enter the moments (W_k = w_k / S).  h[] holds the
+// streamed populations; every post-collision population goes to out(q, h_q)
+// as soon as it is known (registers are the occupancy limit).  aux[5]:
+// previous (drho, ux, uy, uz, omega); the current ones go to aux_out(k, v)
+// (reference Smagorinsky mode).  psc: the warp holds at least one owned cell (warp-
+// uniform), so every cell takes the PSC form, fluid cells with B = 0.
+template <class V, int SMAG, class Out, class AuxOut>
+__device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const bool act[], const int xs[], int y,
+                                        int z, const V aux[5], bool psc, const uint32_t key[], CellForce cf[], Out &&out,
+                                        AuxOut &&aux_out) {
+    using L = Lanes<V>;
+    // Opposite pairs (q, q+1), q odd: sp = h_q + h_{q+1}, am = h_q - h_{q+1}.
+    // Pair p = (q-1)/2 has direction c_q: p0 (1,0,0), p1 (0,1,0), p2 (0,0,1),
+    // p3 (1,1,0), p4 (1,-1,0), p5 (1,0,1), p6 (1,0,-1), p7 (0,1,1), p8 (0,1,-1).
+    V sp[9], am[9];
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
-        sp[p] = d[2 * p + 1] + d[2 * p + 2];
-        am[p] = d[2 * p + 1] - d[2 * p + 2];
+        sp[p] = h[2 * p + 1] + h[2 * p + 2];
+        am[p] = h[2 * p + 1] - h[2 * p + 2];
     }
-    // moments (compute_rho_vel, lbm_solver3d.py:276-303), deviation form
-    float drho = d[0];
+    // moments (compute_rho_vel, lbm_solver3d.py:276-303)
+    const V W1 = L::splat(a.W1), W2 = L::splat(a.W2);
+    const V pxy = sp[3] + sp[4], pxz = sp[5] + sp[6], pyz = sp[7] + sp[8];
+    const V drho = vfma(L::splat(a.W0), h[0], vfma(W1, (sp[0] + sp[1]) + sp[2], W2 * ((pxy + pxz) + pyz)));
+    const V jx = vfma(W1, am[0], W2 * ((am[3] + am[4]) + (am[5] + am[6])));
+    const V jy = vfma(W1, am[1], W2 * ((am[3] - am[4]) + (am[7] + am[8])));
+    const V jz = vfma(W1, am[2], W2 * ((am[5] - am[6]) + (am[7] - am[8])));
+    const V rho = L::splat(1.f) + drho;
+    const V irho = L::rcp(rho);
+    const V i3 = L::splat(3.f) * irho;
+    const V u3x = jx * i3, u3y = jy * i3, u3z = jz * i3;                         // 3u
+    const V nU = vfma(u3x, u3x, vfma(u3y, u3y, u3z * u3z)) * L::splat(-1.f / 3.f);   // -3 u^2
 #pragma unroll
-    for (int p = 0; p < 9; ++p) drho += sp[p];
-    float jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-    for (int p = 0; p < 9; ++p) {
-        const int q = 2 * p + 1;
-        if (cx(q)) jx += cx(q) * am[p];
-        if (cy(q)) jy += cy(q) * am[p];
-        if (cz(q)) jz += cz(q) * am[p];
-    }
-    const float rho = 1.f + drho;
-    const float irho = 1.f / rho;
-    const float ux = jx * irho, uy = jy * irho, uz = jz * irho;
-    const float usq = ux * ux + uy * uy + uz * uz;
-    if (act) {
-        uint32_t bad = 0;
-        if (!isfinite(rho) || !isfinite(usq)) bad |= LBDEM_ST_NAN;
-        if (rho <= 0.f) bad |= LBDEM_ST_RHO;
-        if (usq >= 2.f / 3.f) bad |= LBDEM_ST_VELMAX;
-        if (bad) atomicOr(a.status, (int)bad);
+    for (int i = 0; i < L::N; ++i) {
+        const float r = L::get(rho, i), U = -L::get(nU, i);
+        if (act[i] && !(r > 0.f && r < 3.0e38f && U < 2.f)) {
+            uint32_t bad = 0;
+            if (!isfinite(r) || !isfinite(U)) bad |= LBDEM_ST_NAN;
+            if (r <= 0.f) bad |= LBDEM_ST_RHO;
+            if (U >= 2.f) bad |= LBDEM_ST_VELMAX;
+            atomicOr(a.status, (int)(bad ? bad : LBDEM_ST_NAN));
+        }
     }
 
-    // Smagorinsky relaxation frequency (computeOmega, lbm_solver3d.py:460-513)
-    float om = a.omega0;
+    // Smagorinsky relaxation frequency (computeOmega, lbm_solver3d.py:460-513):
+    // Pi = sum c c (f - feq_lagged); omega = 1 / (1/omega0 + 3 Cs^2 rate),
+    // rate = omega_prev / (2 cs^2 rho) sqrt(2 Pi:Pi)
+    V om = L::splat(a.omega0);
     if (SMAG != LBDEM_SMAG_OFF) {
-        float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
-#pragma unroll
-        for (int p = 0; p < 9; ++p) {
-            const int q = 2 * p + 1;
-            if (cx(q)) sxx += sp[p];
-            if (cy(q)) syy += sp[p];
-            if (cz(q)) szz += sp[p];
-            if (cx(q) * cy(q)) sxy += cx(q) * cy(q) * sp[p];
-            if (cx(q) * cz(q)) sxz += cx(q) * cz(q) * sp[p];
-            if (cy(q) * cz(q)) syz += cy(q) * cz(q) * sp[p];
-        }
-        // second moment of the equilibrium: rho cs^2 delta + rho u u
-        float er, eux, euy, euz, pref;
+        const V sxx = vfma(W1, sp[0], W2 * (pxy + pxz));
+        const V syy = vfma(W1, sp[1], W2 * (pxy + pyz));
+        const V szz = vfma(W1, sp[2], W2 * (pxz + pyz));
+        const V sxy = W2 * (sp[3] - sp[4]);
+        const V sxz = W2 * (sp[5] - sp[6]);
+        const V syz = W2 * (sp[7] - sp[8]);
+        // second moment of the equilibrium deviation: drho cs^2 delta + rho u u
+        const V third = L::splat(1.f / 3.f);
+        V er, eux, euy, euz, pref;
         if (SMAG == LBDEM_SMAG_REFERENCE) {
             er = aux[0]; eux = aux[1]; euy = aux[2]; euz = aux[3]; pref = aux[4];
         } else {
-            er = drho; eux = ux; euy = uy; euz = uz;
-            pref = a.omega0;
+            er = drho; eux = u3x * third; euy = u3y * third; euz = u3z * third;
+            pref = L::splat(a.omega0);
         }
-        const float erho = 1.f + er;
-        const float pxx = sxx - (er * CS2 + erho * eux * eux);
-        const float pyy = syy - (er * CS2 + erho * euy * euy);
-        const float pzz = szz - (er * CS2 + erho * euz * euz);
-        const float pxy = sxy - erho * eux * euy;
-        const float pxz = sxz - erho * eux * euz;
-        const float pyz = syz - erho * euy * euz;
-        const float pi = sqrtf(2.f * (pxx * pxx + pyy * pyy + pzz * pzz + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz)));
-        const float rate = pref * (0.5f / CS2) * irho * pi;
-        const float nut = a.smag_c2 * rate;
-        om = 1.f / (a.inv_omega0 + nut * (1.f / CS2));
-        aux[0] = drho; aux[1] = ux; aux[2] = uy; aux[3] = uz; aux[4] = om;
-    }
-
-    // Collision, one opposite pair (q, q+1) at a time, in place in d[].
-    // Equilibrium deviations feq - w (compute_feq, lbm_solver3d.py:255-271):
-    // fe_q = A + B, fe_{q+1} = A - B with A = w (drho + rho (4.5 cu^2 - 1.5 u^2)),
-    // B = 3 w rho cu.  Body force w rho (c . F)/cs^2 (lbm_foecelover.py:150-164)
-    // is odd in c: +g on q, -g on q+1 (g = 0 when no force is set).
-    const float base = -1.5f * usq;
-    const float gx = rho * a.f3x, gy = rho * a.f3y, gz = rho * a.f3z;
-
-    gid = -1;
-    hx = hy = hz = tx = ty = tz = 0.f;
-    if (key) {
-        // PSC weighted collision (psclattice3d.py:240-261; B from the current
-        // omega as hybridlattice.py:236-245; solid velocity :160-182):
-        // fpc = f + B Os + (1-B) Of, Os_q = f_{qbar} - feq_{qbar} + feqs_q - f_q,
-        // Of = -omega (f - feq), hydroforce -= B Os_q c_q
-        gid = (int)key_gid(key);
-        const float eps = (key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f);
-        const float taum = 1.f / om - 0.5f;
-        const float Bw = eps * taum / ((1.f - eps) + taum);
-        const float Bf = (1.f - Bw) * om;
-        const float4 t0 = a.table[4 * gid + 0], t1 = a.table[4 * gid + 1];
-        const float4 t2 = a.table[4 * gid + 2], t3 = a.table[4 * gid + 3];
-        const float rx = ((float)x - t0.x) - t1.x;
-        const float ry = ((float)y - t0.y) - t1.y;
-        const float rz = ((float)z - t0.z) - t1.z;
-        const float sx = t2.x + (t3.y * rz - t3.z * ry);
-        const float sy = t2.y + (t3.z * rx - t3.x * rz);
-        const float sz = t2.z + (t3.x * ry - t3.y * rx);
-        const float sbase = -1.5f * (sx * sx + sy * sy + sz * sz);
-        {
-            const float fe0 = wq(0) * (drho + rho * base);
-            const float fs0 = wq(0) * (drho + rho * sbase);
-            d[0] = d[0] + Bw * (fs0 - fe0) - Bf * (d[0] - fe0);
-        }
-#pragma unroll
-        for (int p = 0; p < 9; ++p) {
-            const int q = 2 * p + 1;
-            const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
-            const float A = wq(q) * (drho + rho * (4.5f * cu * cu + base));
-            const float B = wq(q) * 3.f * rho * cu;
-            const float cus = cx(q) * sx + cy(q) * sy + cz(q) * sz;
-            const float As = wq(q) * (drho + rho * (4.5f * cus * cus + sbase));
-            const float Bs = wq(q) * 3.f * rho * cus;
-            const float dq = d[q], db = d[q + 1];
-            const float osq = db - (A - B) + (As + Bs) - dq;
-            const float osb = dq - (A + B) + (As - Bs) - db;
-            const float g = wq(q) * (cx(q) * gx + cy(q) * gy + cz(q) * gz);
-            d[q] = dq + Bw * osq - Bf * (dq - (A + B)) + g;
-            d[q + 1] = db + Bw * osb - Bf * (db - (A - B)) - g;
-            const float m = Bw * (osq - osb);   // B Os_q c_q + B Os_{q+1} c_{q+1}
-            if (cx(q)) hx -= cx(q) * m;
-            if (cy(q)) hy -= cy(q) * m;
-            if (cz(q)) hz -= cz(q) * m;
-        }
-        tx = ry * hz - rz * hy;
-        ty = rz * hx - rx * hz;
-        tz = rx * hy - ry * hx;
-        if (a.hydro_out) {
-            a.hydro_out[cell] = hx;
-            a.hydro_out[a.nc + cell] = hy;
-            a.hydro_out[2 * a.nc + cell] = hz;
-        }
-    } else {
-        d[0] = d[0] + om * (wq(0) * (drho + rho * base) - d[0]);
-#pragma unroll
-        for (int p = 0; p < 9; ++p) {
-            const int q = 2 * p + 1;
-            const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
-            const float A = wq(q) * (drho + rho * (4.5f * cu * cu + base));
-            const float B = wq(q) * 3.f * rho * cu;
-            const float g = wq(q) * (cx(q) * gx + cy(q) * gy + cz(q) * gz);
-            d[q] = d[q] + om * ((A + B) - d[q]) + g;
-            d[q + 1] = d[q + 1] + om * ((A - B) - d[q + 1]) - g;
+        const V erho = L::splat(1.f) + er;
+        const V ecs = er * third;
+        const V qx = erho * eux, qy = erho * euy;
+        const V Pxx = sxx - vfma(qx, eux, ecs);
+        const V Pyy = syy - vfma(qy, euy, ecs);
+        const V Pzz = szz - vfma(erho * euz, euz, ecs);
+        const V Pxy = sxy - qx * euy;
+        const V Pxz = sxz - qx * euz;
+        const V Pyz = syz - qy * euz;
+        const V diag = vfma(Pxx, Pxx, vfma(Pyy, Pyy, Pzz * Pzz));
+        const V offd = vfma(Pxy, Pxy, vfma(Pxz, Pxz, Pyz * Pyz));
+        const V pi = L::sqrt(vfma(L::splat(4.f), offd, L::splat(2.f) * diag));
+        om = L::rcp(vfma(L::splat(a.smag_k) * pref, irho * pi, L::splat(a.inv_omega0)));
+        if (SMAG == LBDEM_SMAG_REFERENCE) {
+            aux_out(0, drho);
+            aux_out(1, u3x * third);
+            aux_out(2, u3y * third);
+            aux_out(3, u3z * third);
+            aux_out(4, om);
         }
     }
 
+    const V S = L::splat(a.S);
+    const V SR = S * rho;
+    const V rg3x = rho * L::splat(a.g3x), rg3y = rho * L::splat(a.g3y), rg3z = rho * L::splat(a.g3z);
+#pragma unroll
+    for (int i = 0; i < L::N; ++i) {
+        cf[i].gid = -1;
+        cf[i].hx = cf[i].hy = cf[i].hz = cf[i].tx = cf[i].ty = cf[i].tz = 0.f;
+    }
+    if (!psc) {
+        // BGK: h' = (1-om) h + om feq_h + g_h, one opposite pair at a time.
+        // om feq_h = k0 + k2 (v^2 - U) +/- om S rho v, v = c.(3u); the odd part
+        // and the body force combine into c.V, V = om S rho 3u + 3 S rho F.
+        const V k0 = om * S * drho;
+        const V k2 = L::splat(0.5f) * om * SR;
+        const V omc = L::splat(1.f) - om;
+        const V ks = om * SR;
+        const V Vx = vfma(ks, u3x, rg3x), Vy = vfma(ks, u3y, rg3y), Vz = vfma(ks, u3z, rg3z);
+        out(0, vfma(omc, h[0], vfma(k2, nU, k0)));
+#pragma unroll
+        for (int p = 0; p < 9; ++p) {
+            const int q = 2 * p + 1;
+            const V v = cdot(q, u3x, u3y, u3z);
+            const V cv = cdot(q, Vx, Vy, Vz);
+            const V e = vfma(k2, vfma(v, v, nU), k0);
+            out(q, vfma(omc, h[q], e + cv));
+            out(q + 1, vfma(omc, h[q + 1], e - cv));
+        }
+        return;
+    }
+    // PSC weighted collision (psclattice3d.py:240-261):
+    //   fpc = f + B Os + (1-B) Of,  Os_q = f_qbar - feq_qbar + feqs_q - f_q,
+    //   Of = -om (f - feq),  hydroforce -= B sum_q Os_q c_q.
+    // Per pair, with Bf = (1-B) om, c1 = 1 - B - Bf, feq = A +/- Bo,
+    // feqs = As +/- Bso (solid velocity u_s, same rho):
+    //   h_q'    = c1 h_q + B h_qbar + E + O,  h_qbar' = c1 h_qbar + B h_q + E - O,
+    //   E = Bf A + B (As - A),  O = (B + Bf) Bo + B Bso + g_h.
+    // sum_q Os_q c_q = rho (u_s - u) exactly for this equilibrium, so the
+    // cell's force is B (j - rho u_s) (psc_cell).
+    V Bw = L::splat(0.f), s3x = Bw, s3y = Bw, s3z = Bw;
+#pragma unroll
+    for (int i = 0; i < L::N; ++i) {
+        if (key[i]) {
+            float sx, sy, sz;
+            L::set(Bw, i, psc_cell(a, key[i], L::get(om, i), L::get(rho, i), L::get(jx, i), L::get(jy, i),
+                                   L::get(jz, i), xs[i], y, z, sx, sy, sz, cf[i]));
+            L::set(s3x, i, sx); L::set(s3y, i, sy); L::set(s3z, i, sz);
+        }
+    }
+    const V Bf = (L::splat(1.f) - Bw) * om;
+    const V nUs = vfma(s3x, s3x, vfma(s3y, s3y, s3z * s3z)) * L::splat(-1.f / 3.f);
+    const V k2 = L::splat(0.5f) * SR;
+    const V eA = k2 * (Bf - Bw), eS = k2 * Bw, e0 = Bf * (S * drho);
+    const V c1 = (L::splat(1.f) - Bf) - Bw;
+    const V ca = L::splat(0.5f) * (c1 + Bw);   // (c1 + B)/2
+    const V cb = L::splat(0.5f) * (c1 - Bw);   // (c1 - B)/2
+    const V kb = (Bw + Bf) * SR, ks = Bw * SR;
+    const V Vx = vfma(kb, u3x, vfma(ks, s3x, rg3x));
+    const V Vy = vfma(kb, u3y, vfma(ks, s3y, rg3y));
+    const V Vz = vfma(kb, u3z, vfma(ks, s3z, rg3z));
+    // q = 0: h0' = (c1 + B) h0 + Bf A0 + B (As0 - A0), A0 = S drho - k2 U
+    out(0, vfma(c1 + Bw, h[0], vfma(eA, nU, vfma(eS, nUs, e0))));
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        const int q = 2 * p + 1;
+        const V v = cdot(q, u3x, u3y, u3z);
+        const V vs = cdot(q, s3x, s3y, s3z);
+        const V O = cdot(q, Vx, Vy, Vz);
+        const V E = vfma(eA, vfma(v, v, nU), vfma(eS, vfma(vs, vs, nUs), e0));
+        const V SE = vfma(ca, sp[p], E);
+        const V AO = vfma(cb, am[p], O);
+        out(q, SE + AO);
+        out(q + 1, SE - AO);
+    }
 }
 
 // Warp-segmented sum of (h, t) over runs of equal owner id, one FP64 atomic
 // per run and component (lattice2grains, psclattice3d.py:316-358).
-__device__ __forceinline__ void reduce_forces(const StepArgs &a, int gid, float hx, float hy, float hz, float tx,
-                                              float ty, float tz) {
-    if (!__any_sync(0xffffffffu, gid >= 0)) return;
+__device__ __forceinline__ void reduce_forces(const StepArgs &a, CellForce c) {
     const unsigned lane = lane_id();
+    const int gid = c.gid;
     const int gnext = __shfl_down_sync(0xffffffffu, gid, 1);
     const int gprev = __shfl_up_sync(0xffffffffu, gid, 1);
     const unsigned tails = __ballot_sync(0xffffffffu, lane == 31 || gnext != gid);
     const unsigned mytail = (unsigned)(__ffs(tails >> lane) - 1) + lane;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const float vx = __shfl_down_sync(0xffffffffu, hx, o);
-        const float vy = __shfl_down_sync(0xffffffffu, hy, o);
-        const float vz = __shfl_down_sync(0xffffffffu, hz, o);
-        const float wx = __shfl_down_sync(0xffffffffu, tx, o);
-        const float wy = __shfl_down_sync(0xffffffffu, ty, o);
-        const float wz = __shfl_down_sync(0xffffffffu, tz, o);
+        const float vx = __shfl_down_sync(0xffffffffu, c.hx, o);
+        const float vy = __shfl_down_sync(0xffffffffu, c.hy, o);
+        const float vz = __shfl_down_sync(0xffffffffu, c.hz, o);
+        const float wx = __shfl_down_sync(0xffffffffu, c.tx, o);
+        const float wy = __shfl_down_sync(0xffffffffu, c.ty, o);
+        const float wz = __shfl_down_sync(0xffffffffu, c.tz, o);
         if (lane + o <= mytail) {
-            hx += vx; hy += vy; hz += vz;
-            tx += wx; ty += wy; tz += wz;
+            c.hx += vx; c.hy += vy; c.hz += vz;
+            c.tx += wx; c.ty += wy; c.tz += wz;
         }
     }
     const bool head = lane == 0 || gprev != gid;
     if (head && gid >= 0) {
         double *F = a.force_fluid + 3 * (size_t)gid;
         double *M = a.moment_fluid + 3 * (size_t)gid;
-        atomicAdd(F + 0, (double)hx * a.fscale);
-        atomicAdd(F + 1, (double)hy * a.fscale);
-        atomicAdd(F + 2, (double)hz * a.fscale);
-        atomicAdd(M + 0, (double)tx * a.tscale);
-        atomicAdd(M + 1, (double)ty * a.tscale);
-        atomicAdd(M + 2, (double)tz * a.tscale);
+        atomicAdd(F + 0, (double)c.hx * a.fscale);
+        atomicAdd(F + 1, (double)c.hy * a.fscale);
+        atomicAdd(F + 2, (double)c.hz * a.fscale);
+        atomicAdd(M + 0, (double)c.tx * a.tscale);
+        atomicAdd(M + 1, (double)c.ty * a.tscale);
+        atomicAdd(M + 2, (double)c.tz * a.tscale);
     }
 }
 
 // ---------------------------------------------------------------------------
-// packed FP32x2 arithmetic (sm_100 FFMA2/FADD2/FMUL2): two cells per thread,
-// cell A in .x and cell B in .y, every operation IEEE round-to-nearest per lane
+// fused step, one cell per thread
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 f2(float s) { return make_float2(s, s); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
-    // packed subtract (PTX sub.rn.f32x2, sm_100+)
-    unsigned long long ra = *reinterpret_cast<unsigned long long *>(&a);
-    unsigned long long rb = *reinterpret_cast<unsigned long long *>(&b), rd;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
-    return *reinterpret_cast<float2 *>(&rd);
-}
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 dot3_2(int ax, int ay, int az, float2 x, float2 y, float2 z) {
-    // c . v with c in {-1, 0, 1}^3 folded at compile time
-    float2 r = f2(0.f);
-    bool first = true;
-    if (ax) { r = ax > 0 ? x : make_float2(-x.x, -x.y); first = false; }
-    if (ay) { r = first ? (ay > 0 ? y : make_float2(-y.x, -y.y)) : (ay > 0 ? add2(r, y) : sub2(r, y)); first = false; }
-    if (az) { r = first ? (az > 0 ? z : make_float2(-z.x, -z.y)) : (az > 0 ? add2(r, z) : sub2(r, z)); }
-    return r;
+#ifndef ONE_THREADS
+#define ONE_THREADS 256
+#endif
+#ifndef ONE_MIN_BLOCKS
+#define ONE_MIN_BLOCKS 4
+#endif
+// Element offset, within its row, of cell x's block slot (lane x % 32 of
+// x-block x / 32; the population or auxiliary index adds q * 32).
+__device__ __forceinline__ uint32_t xslot(uint32_t x, uint32_t per_block) {
+    return (x >> 5) * per_block + (x & 31u);
 }
 
-// Same semantics as collide_cell, on two cells at once.  Lanes whose cell is
-// not updated (act false) carry zeros and their results are discarded.  When
-// either cell is owned by a particle the PSC form is evaluated for both, with
-// weight B = 0 on a fluid cell, which reduces it exactly to BGK.
-template <int SMAG>
-__device__ __forceinline__ void collide_pair(const StepArgs &a, float2 d[Q], bool acta, bool actb, int x0, int y,
-                                             int z, uint32_t cell0, float2 aux[5], uint32_t keya, uint32_t keyb,
-                                             int &ga, int &gb, float ha[6], float hb[6]) {
-    float2 sp[9], am[9];
-#pragma unroll
-    for (int p = 0; p < 9; ++p) {
-        sp[p] = add2(d[2 * p + 1], d[2 * p + 2]);
-        am[p] = sub2(d[2 * p + 1], d[2 * p + 2]);
-    }
-    float2 drho = d[0];
-#pragma unroll
-    for (int p = 0; p < 9; ++p) drho = add2(drho, sp[p]);
-    float2 jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
-#pragma unroll
-    for (int p = 0; p < 9; ++p) {
-        const int q = 2 * p + 1;
-        if (cx(q)) jx = cx(q) > 0 ? add2(jx, am[p]) : sub2(jx, am[p]);
-        if (cy(q)) jy = cy(q) > 0 ? add2(jy, am[p]) : sub2(jy, am[p]);
-        if (cz(q)) jz = cz(q) > 0 ? add2(jz, am[p]) : sub2(jz, am[p]);
-    }
-    const float2 rho = add2(f2(1.f), drho);
-    const float2 irho = make_float2(1.f / rho.x, 1.f / rho.y);
-    const float2 ux = mul2(jx, irho), uy = mul2(jy, irho), uz = mul2(jz, irho);
-    const float2 usq = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
-    {
-        uint32_t bad = 0;
-        if (acta) {
-            if (!isfinite(rho.x) || !isfinite(usq.x)) bad |= LBDEM_ST_NAN;
-            if (rho.x <= 0.f) bad |= LBDEM_ST_RHO;
-            if (usq.x >= 2.f / 3.f) bad |= LBDEM_ST_VELMAX;
-        }
-        if (actb) {
-            if (!isfinite(rho.y) || !isfinite(usq.y)) bad |= LBDEM_ST_NAN;
-            if (rho.y <= 0.f) bad |= LBDEM_ST_RHO;
-            if (usq.y >= 2.f / 3.f) bad |= LBDEM_ST_VELMAX;
-        }
-        if (bad) atomicOr(a.status, (int)bad);
-    }
-    float2 om = f2(a.omega0);
-    if (SMAG != LBDEM_SMAG_OFF) {
-        float2 sxx = f2(0.f), syy = f2(0.f), szz = f2(0.f), sxy = f2(0.f), sxz = f2(0.f), syz = f2(0.f);
-#pragma unroll
-        for (int p = 0; p < 9; ++p) {
-            const int q = 2 * p + 1;
-            if (cx(q)) sxx = add2(sxx, sp[p]);
-            if (cy(q)) syy = add2(syy, sp[p]);
-            if (cz(q)) szz = add2(szz, sp[p]);
-            if (cx(q) * cy(q)) sxy = cx(q) * cy(q) > 0 ? add2(sxy, sp[p]) : sub2(sxy, sp[p]);
-            if (cx(q) * cz(q)) sxz = cx(q) * cz(q) > 0 ? add2(sxz, sp[p]) : sub2(sxz, sp[p]);
-            if (cy(q) * cz(q)) syz = cy(q) * cz(q) > 0 ? add2(syz, sp[p]) : sub2(syz, sp[p]);
-        }
-        float2 er, eux, euy, euz, pref;
-        if (SMAG == LBDEM_SMAG_REFERENCE) {
-            er = aux[0]; eux = aux[1]; euy = aux[2]; euz = aux[3]; pref = aux[4];
-        } else {
-            er = drho; eux = ux; euy = uy; euz = uz;
-            pref = f2(a.omega0);
-        }
-        const float2 erho = add2(f2(1.f), er);
-        const float2 ecs = mul2(er, f2(CS2));
-        const float2 pxx = sub2(sxx, fma2(mul2(erho, eux), eux, ecs));
-        const float2 pyy = sub2(syy, fma2(mul2(erho, euy), euy, ecs));
-        const float2 pzz = sub2(szz, fma2(mul2(erho, euz), euz, ecs));
-        const float2 pxy = sub2(sxy, mul2(mul2(erho, eux), euy));
-        const float2 pxz = sub2(sxz, mul2(mul2(erho, eux), euz));
-        const float2 pyz = sub2(syz, mul2(mul2(erho, euy), euz));
-        const float2 off = fma2(pxy, pxy, fma2(pxz, pxz, mul2(pyz, pyz)));
-        const float2 dia = fma2(pxx, pxx, fma2(pyy, pyy, mul2(pzz, pzz)));
-        const float2 pi2 = mul2(f2(2.f), fma2(f2(2.f), off, dia));
-        const float2 pi = make_float2(sqrtf(pi2.x), sqrtf(pi2.y));
-        const float2 rate = mul2(mul2(pref, f2(0.5f / CS2)), mul2(irho, pi));
-        const float2 den = fma2(mul2(f2(a.smag_c2), rate), f2(1.f / CS2), f2(a.inv_omega0));
-        om = make_float2(1.f / den.x, 1.f / den.y);
-        aux[0] = drho; aux[1] = ux; aux[2] = uy; aux[3] = uz; aux[4] = om;
-    }
-    const float2 base = mul2(f2(-1.5f), usq);
-    const float2 gx = mul2(rho, f2(a.f3x)), gy = mul2(rho, f2(a.f3y)), gz = mul2(rho, f2(a.f3z));
-    ga = gb = -1;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) ha[k] = hb[k] = 0.f;
-    if (keya | keyb) {
-        float2 Bw = f2(0.f), sx = f2(0.f), sy = f2(0.f), sz = f2(0.f);
-        float rxa = 0.f, rya = 0.f, rza = 0.f, rxb = 0.f, ryb = 0.f, rzb = 0.f;
-        if (keya) {
-            ga = (int)key_gid(keya);
-            const float eps = (keya & KEY_FULL) ? 1.f : (float)key_count(keya) * (1.f / 125.f);
-            const float taum = 1.f / om.x - 0.5f;
-            Bw.x = eps * taum / ((1.f - eps) + taum);
-            const float4 t0 = a.table[4 * ga + 0], t1 = a.table[4 * ga + 1];
-            const float4 t2 = a.table[4 * ga + 2], t3 = a.table[4 * ga + 3];
-            rxa = ((float)x0 - t0.x) - t1.x; rya = ((float)y - t0.y) - t1.y; rza = ((float)z - t0.z) - t1.z;
-            sx.x = t2.x + (t3.y * rza - t3.z * rya);
-            sy.x = t2.y + (t3.z * rxa - t3.x * rza);
-            sz.x = t2.z + (t3.x * rya - t3.y * rxa);
-        }
-        if (keyb) {
-            gb = (int)key_gid(keyb);
-            const float eps = (keyb & KEY_FULL) ? 1.f : (float)key_count(keyb) * (1.f / 125.f);
-            const float taum = 1.f / om.y - 0.5f;
-            Bw.y = eps * taum / ((1.f - eps) + taum);
-            const float4 t0 = a.table[4 * gb + 0], t1 = a.table[4 * gb + 1];
-            const float4 t2 = a.table[4 * gb + 2], t3 = a.table[4 * gb + 3];
-            rxb = ((float)(x0 + 1) - t0.x) - t1.x; ryb = ((float)y - t0.y) - t1.y; rzb = ((float)z - t0.z) - t1.z;
-            sx.y = t2.x + (t3.y * rzb - t3.z * ryb);
-            sy.y = t2.y + (t3.z * rxb - t3.x * rzb);
-            sz.y = t2.z + (t3.x * ryb - t3.y * rxb);
-        }
-        const float2 Bf = mul2(sub2(f2(1.f), Bw), om);
-        const float2 sbase = mul2(f2(-1.5f), fma2(sx, sx, fma2(sy, sy, mul2(sz, sz))));
-        float2 hx = f2(0.f), hy = f2(0.f), hz = f2(0.f);
-        {
-            const float2 fe0 = mul2(f2(wq(0)), fma2(rho, base, drho));
-            const float2 fs0 = mul2(f2(wq(0)), fma2(rho, sbase, drho));
-            d[0] = sub2(fma2(Bw, sub2(fs0, fe0), d[0]), mul2(Bf, sub2(d[0], fe0)));
-        }
-#pragma unroll
-        for (int p = 0; p < 9; ++p) {
-            const int q = 2 * p + 1;
-            const float2 cu = dot3_2(cx(q), cy(q), cz(q), ux, uy, uz);
-            const float2 A = mul2(f2(wq(q)), fma2(rho, fma2(mul2(f2(4.5f), cu), cu, base), drho));
-            const float2 B = mul2(mul2(f2(3.f * wq(q)), rho), cu);
-            const float2 cus = dot3_2(cx(q), cy(q), cz(q), sx, sy, sz);
-            const float2 As = mul2(f2(wq(q)), fma2(rho, fma2(mul2(f2(4.5f), cus), cus, sbase), drho));
-            const float2 Bs = mul2(mul2(f2(3.f * wq(q)), rho), cus);
-            const float2 dq = d[q], db = d[q + 1];
-            const float2 feq = add2(A, B), feb = sub2(A, B);
-            const float2 osq = sub2(add2(sub2(db, feb), add2(As, Bs)), dq);
-            const float2 osb = sub2(add2(sub2(dq, feq), sub2(As, Bs)), db);
-            const float2 g = mul2(f2(wq(q)), dot3_2(cx(q), cy(q), cz(q), gx, gy, gz));
-            d[q] = add2(sub2(fma2(Bw, osq, dq), mul2(Bf, sub2(dq, feq))), g);
-            d[q + 1] = sub2(sub2(fma2(Bw, osb, db), mul2(Bf, sub2(db, feb))), g);
-            const float2 m = mul2(Bw, sub2(osq, osb));
-            if (cx(q)) hx = cx(q) > 0 ? sub2(hx, m) : add2(hx, m);
-            if (cy(q)) hy = cy(q) > 0 ? sub2(hy, m) : add2(hy, m);
-            if (cz(q)) hz = cz(q) > 0 ? sub2(hz, m) : add2(hz, m);
-        }
-        if (keya) {
-            ha[0] = hx.x; ha[1] = hy.x; ha[2] = hz.x;
-            ha[3] = rya * hz.x - rza * hy.x; ha[4] = rza * hx.x - rxa * hz.x; ha[5] = rxa * hy.x - rya * hx.x;
-            if (a.hydro_out) {
-                a.hydro_out[cell0] = hx.x; a.hydro_out[a.nc + cell0] = hy.x; a.hydro_out[2 * a.nc + cell0] = hz.x;
-            }
-        }
-        if (keyb) {
-            hb[0] = hx.y; hb[1] = hy.y; hb[2] = hz.y;
-            hb[3] = ryb * hz.y - rzb * hy.y; hb[4] = rzb * hx.y - rxb * hz.y; hb[5] = rxb * hy.y - ryb * hx.y;
-            if (a.hydro_out) {
-                const uint32_t c1 = cell0 + 1;
-                a.hydro_out[c1] = hx.y; a.hydro_out[a.nc + c1] = hy.y; a.hydro_out[2 * a.nc + c1] = hz.y;
-            }
-        }
-    } else {
-        d[0] = fma2(om, sub2(mul2(f2(wq(0)), fma2(rho, base, drho)), d[0]), d[0]);
-#pragma unroll
-        for (int p = 0; p < 9; ++p) {
-            const int q = 2 * p + 1;
-            const float2 cu = dot3_2(cx(q), cy(q), cz(q), ux, uy, uz);
-            const float2 A = mul2(f2(wq(q)), fma2(rho, fma2(mul2(f2(4.5f), cu), cu, base), drho));
-            const float2 B = mul2(mul2(f2(3.f * wq(q)), rho), cu);
-            const float2 g = mul2(f2(wq(q)), dot3_2(cx(q), cy(q), cz(q), gx, gy, gz));
-            d[q] = add2(fma2(om, sub2(add2(A, B), d[q]), d[q]), g);
-            d[q + 1] = sub2(fma2(om, sub2(sub2(A, B), d[q + 1]), d[q + 1]), g);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// fused step, one cell per thread (any lattice size)
-// ---------------------------------------------------------------------------
 template <typename T, bool GATHER, int SMAG>
-__global__ void __launch_bounds__(256) k_psc_step(const StepArgs a) {
+__global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const size_t nc = a.nc;
     const bool inb = (x < nx) && (y < ny);
-    const uint32_t cell = inb ? (uint32_t)(z * ny + y) * (uint32_t)nx + (uint32_t)x : 0u;
+    const int xc_ = inb ? x : 0, yc_ = inb ? y : 0;
+    const uint32_t row = (uint32_t)(z * ny + yc_);
+    const uint32_t cell = row * (uint32_t)nx + (uint32_t)xc_;
+    const uint32_t rs = a.rs;                         // elements per row of populations
+    const uint32_t r0 = row * rs;
+    const uint32_t own = r0 + xslot((uint32_t)xc_, QB);
     // Issue the 19 gather loads first (their addresses never depend on the
     // link mask), then resolve the link mask and re-fetch bounce-back
-    // directions on the few cells next to an obstacle.  Element indices are
-    // 32-bit: the source cell of direction q is a wrapped row base (9 per
-    // thread) plus a wrapped x offset, plus q*Ncells from the parameters.
-    const int xc_ = inb ? x : 0, yc_ = inb ? y : 0;
-    const uint32_t cellc = inb ? cell : 0u;
-    const uint32_t unx = (uint32_t)nx, nxy = (uint32_t)nx * (uint32_t)ny;
-    const T *__restrict__ src = (const T *)a.src;
+    // directions on the few cells next to an obstacle.  One pointer per
+    // upwind (row, x) slot; the direction index is an immediate offset.
+    const T *__restrict__ src = static_cast<const T *>(a.src);
     T raw[Q];
     if (GATHER) {
-        const uint32_t r0 = (uint32_t)(z * ny + yc_) * unx;
-        const uint32_t dym = yc_ == 0 ? (uint32_t)(ny - 1) * unx : (uint32_t)(-(int)nx);
-        const uint32_t dyp = yc_ == ny - 1 ? (uint32_t)(-(int)((ny - 1) * nx)) : unx;
-        const uint32_t dzm = z == 0 ? (uint32_t)(nz - 1) * nxy : (uint32_t)(-(int)nxy);
-        const uint32_t dzp = z == nz - 1 ? (uint32_t)(-(int)((nz - 1) * nxy)) : nxy;
-        const uint32_t xm = xc_ == 0 ? (uint32_t)(nx - 1) : (uint32_t)(xc_ - 1);
-        const uint32_t xp = xc_ == nx - 1 ? 0u : (uint32_t)(xc_ + 1);
+        const uint32_t dym = yc_ == 0 ? (uint32_t)(ny - 1) * rs : (uint32_t)(-(int)rs);
+        const uint32_t dyp = yc_ == ny - 1 ? (uint32_t)(-(int)((ny - 1) * rs)) : rs;
+        const uint32_t zs = (uint32_t)ny * rs;
+        const uint32_t dzm = z == 0 ? (uint32_t)(nz - 1) * zs : (uint32_t)(-(int)zs);
+        const uint32_t dzp = z == nz - 1 ? (uint32_t)(-(int)((nz - 1) * zs)) : zs;
+        const uint32_t sx0 = xslot((uint32_t)xc_, QB);
+        const uint32_t sxm = xslot(xc_ == 0 ? (uint32_t)(nx - 1) : (uint32_t)(xc_ - 1), QB);
+        const uint32_t sxp = xslot(xc_ == nx - 1 ? 0u : (uint32_t)(xc_ + 1), QB);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const uint32_t ry = cy(q) == 1 ? dym : (cy(q) == -1 ? dyp : 0u);
             const uint32_t rz = cz(q) == 1 ? dzm : (cz(q) == -1 ? dzp : 0u);
-            const uint32_t xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : (uint32_t)xc_);
-            raw[q] = Store<T>::ld(src + (r0 + ry + rz + xs + a.qoff[q]));
+            const uint32_t xs = cx(q) == 1 ? sxm : (cx(q) == -1 ? sxp : sx0);
+            const T *p = src + (r0 + ry + rz + xs);
+            raw[q] = Store<T>::ld(p + q * 32);
         }
     } else {
+        const T *p = src + own;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) raw[q] = Store<T>::ld(src + (cellc + a.qoff[q]));
+        for (int q = 0; q < Q; ++q) raw[q] = Store<T>::ld(p + q * 32);
     }
     float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
-    if (SMAG == LBDEM_SMAG_REFERENCE && inb) {
-        const T *ax = (const T *)a.aux;
+    const uint32_t aown = row * a.ars + xslot((uint32_t)xc_, AB);
+    if (SMAG == LBDEM_SMAG_REFERENCE) {
+        const T *ap = static_cast<const T *>(a.aux) + aown;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ax[cell + a.qoff[k]]);
+        for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ap[k * 32]);
     }
-    const uint32_t key = (a.key != nullptr && inb) ? a.key[cell] : 0u;
+    uint32_t key = (a.key != nullptr) ? a.key[cell] : 0u;
     uint32_t lk = LINK_FLUID;
-    if (inb && !a.row_simple[z * ny + y]) lk = a.links[cell];
+    if (!a.row_simple[row]) lk = a.links[cell];
     const bool act = inb && !(lk & LINK_SKIP);
+    if (!act) key = 0u;
     if (GATHER && (lk & 0x7FFFEu)) {
+        const T *p = src + own;
 #pragma unroll
         for (int q = 1; q < Q; ++q)
-            if (lk & LINK_BB(q)) raw[q] = Store<T>::ld(src + (cellc + a.qoff[qinv(q)]));
+            if (lk & LINK_BB(q)) raw[q] = Store<T>::ld(p + qinv(q) * 32);
     }
-    float d[Q];
+    float h[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) d[q] = act ? Store<T>::dec(raw[q], wq(q) * a.dec) : 0.f;
-    int gid;
-    float hx, hy, hz, tx, ty, tz;
-    collide_cell<SMAG>(a, d, act, cell, x, y, z, aux, act ? key : 0u, gid, hx, hy, hz, tx, ty, tz);
+    for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(raw[q]);
+    const bool psc = a.key != nullptr && __any_sync(0xffffffffu, key != 0u);
+    CellForce cf[1];
+    const bool acts[1] = {act};
+    const int xs[1] = {x};
+    const uint32_t keys[1] = {key};
+    // post-collision values overwrite h[] and aux[] and are stored together
+    collide<float, SMAG>(
+        a, h, acts, xs, y, z, aux, psc, keys, cf, [&](int q, float v) { h[q] = v; },
+        [&](int k, float v) { aux[k] = v; });
     if (act) {
-        T *dst = (T *)a.dst;
+        T *d = static_cast<T *>(a.dst) + own;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) dst[cell + a.qoff[q]] = Store<T>::enc(d[q], a.enc / wq(q));
+        for (int q = 0; q < Q; ++q) d[q * 32] = Store<T>::narrow(h[q]);
         if (SMAG == LBDEM_SMAG_REFERENCE) {
-            T *ax = (T *)a.aux;
+            T *ap = static_cast<T *>(a.aux) + aown;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) ax[cell + a.qoff[k]] = aux_enc<T>(aux[k]);
+            for (int k = 0; k < 5; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+        }
+        if (a.hydro_out) {
+            a.hydro_out[cell] = cf[0].hx;
+            a.hydro_out[a.nc + cell] = cf[0].hy;
+            a.hydro_out[2 * a.nc + cell] = cf[0].hz;
         }
     }
-    if (a.key != nullptr) reduce_forces(a, gid, hx, hy, hz, tx, ty, tz);
-}
-
-// ---------------------------------------------------------------------------
-// fused step, two x-neighbouring cells per thread (Nx % 64 == 0): pair loads
-// and stores (8 B FP32 / 4 B 16-bit); a warp covers 64 cells of one row, so
-// the x-shifted directions come from the aligned pair loads of the
-// neighbouring lane (one shuffle) plus one extra element at the warp edge.
-// ---------------------------------------------------------------------------
-template <typename T> struct Pair;
-template <> struct Pair<float> {
-    using V = float2;
-    __device__ __forceinline__ static V ld(const float *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
-    __device__ __forceinline__ static void st(float *p, V v) { *reinterpret_cast<float2 *>(p) = v; }
-    __device__ __forceinline__ static float lo(V v) { return v.x; }
-    __device__ __forceinline__ static float hi(V v) { return v.y; }
-    __device__ __forceinline__ static V make(float a, float b) { return make_float2(a, b); }
-    __device__ __forceinline__ static float2 dec(V v, float) { return v; }
-    __device__ __forceinline__ static V enc(float2 d, float) { return d; }
-    __device__ __forceinline__ static float2 adec(V v) { return v; }
-    __device__ __forceinline__ static V aenc(float2 d) { return d; }
-    __device__ __forceinline__ static float shup(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
-    __device__ __forceinline__ static float shdn(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
-};
-template <> struct Pair<__half> {
-    using V = __half2;
-    __device__ __forceinline__ static V ld(const __half *p) { return __ldg(reinterpret_cast<const __half2 *>(p)); }
-    __device__ __forceinline__ static void st(__half *p, V v) { *reinterpret_cast<__half2 *>(p) = v; }
-    __device__ __forceinline__ static __half lo(V v) { return __low2half(v); }
-    __device__ __forceinline__ static __half hi(V v) { return __high2half(v); }
-    __device__ __forceinline__ static V make(__half a, __half b) { return __halves2half2(a, b); }
-    __device__ __forceinline__ static float2 dec(V v, float s) { return mul2(__half22float2(v), f2(s)); }
-    __device__ __forceinline__ static V enc(float2 d, float s) { return __float22half2_rn(mul2(d, f2(s))); }
-    __device__ __forceinline__ static float2 adec(V v) { return __half22float2(v); }
-    __device__ __forceinline__ static V aenc(float2 d) { return __float22half2_rn(d); }
-    __device__ __forceinline__ static __half shup(__half v) {
-        return __ushort_as_half((unsigned short)__shfl_up_sync(0xffffffffu, (unsigned)__half_as_ushort(v), 1));
-    }
-    __device__ __forceinline__ static __half shdn(__half v) {
-        return __ushort_as_half((unsigned short)__shfl_down_sync(0xffffffffu, (unsigned)__half_as_ushort(v), 1));
-    }
-};
-template <> struct Pair<__nv_bfloat16> {
-    using V = __nv_bfloat162;
-    __device__ __forceinline__ static V ld(const __nv_bfloat16 *p) {
-        return __ldg(reinterpret_cast<const __nv_bfloat162 *>(p));
-    }
-    __device__ __forceinline__ static void st(__nv_bfloat16 *p, V v) { *reinterpret_cast<__nv_bfloat162 *>(p) = v; }
-    __device__ __forceinline__ static __nv_bfloat16 lo(V v) { return __low2bfloat16(v); }
-    __device__ __forceinline__ static __nv_bfloat16 hi(V v) { return __high2bfloat16(v); }
-    __device__ __forceinline__ static V make(__nv_bfloat16 a, __nv_bfloat16 b) { return __halves2bfloat162(a, b); }
-    __device__ __forceinline__ static float2 dec(V v, float s) { return mul2(__bfloat1622float2(v), f2(s)); }
-    __device__ __forceinline__ static V enc(float2 d, float s) { return __float22bfloat162_rn(mul2(d, f2(s))); }
-    __device__ __forceinline__ static float2 adec(V v) { return __bfloat1622float2(v); }
-    __device__ __forceinline__ static V aenc(float2 d) { return __float22bfloat162_rn(d); }
-    __device__ __forceinline__ static __nv_bfloat16 shup(__nv_bfloat16 v) {
-        return __ushort_as_bfloat16((unsigned short)__shfl_up_sync(0xffffffffu, (unsigned)__bfloat16_as_ushort(v), 1));
-    }
-    __device__ __forceinline__ static __nv_bfloat16 shdn(__nv_bfloat16 v) {
-        return __ushort_as_bfloat16((unsigned short)__shfl_down_sync(0xffffffffu, (unsigned)__bfloat16_as_ushort(v), 1));
-    }
-};
-
-template <typename T, bool GATHER, int SMAG>
-__global__ void __launch_bounds__(128) k_psc_step2(const StepArgs a) {
-    using P = Pair<T>;
-    using V = typename P::V;
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int tx2 = blockIdx.x * blockDim.x + threadIdx.x;   // pair index along x
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    const size_t nc = a.nc;
-    const bool inb = y < ny;                                  // x always in range (Nx % 64 == 0)
-    const int x0 = 2 * tx2;
-    const int yc_ = inb ? y : 0;
-    const uint32_t cell0 = (uint32_t)(z * ny + yc_) * (uint32_t)nx + (uint32_t)x0;
-    const unsigned lane = lane_id();
-    const T *__restrict__ src = (const T *)a.src;
-    V rv[Q];   // streamed populations of cells (x0, x0+1)
-    const uint32_t unx = (uint32_t)nx, nxy = (uint32_t)nx * (uint32_t)ny;
-    if (GATHER) {
-        const uint32_t r0 = (uint32_t)(z * ny + yc_) * unx;
-        const uint32_t dym = yc_ == 0 ? (uint32_t)(ny - 1) * unx : (uint32_t)(-(int)nx);
-        const uint32_t dyp = yc_ == ny - 1 ? (uint32_t)(-(int)((ny - 1) * nx)) : unx;
-        const uint32_t dzm = z == 0 ? (uint32_t)(nz - 1) * nxy : (uint32_t)(-(int)nxy);
-        const uint32_t dzp = z == nz - 1 ? (uint32_t)(-(int)((nz - 1) * nxy)) : nxy;
-        // x of the element just left of this warp's 64 cells, and just right of them
-        const int wx0 = x0 - 2 * (int)lane;
-        const uint32_t xl = wx0 == 0 ? (uint32_t)(nx - 1) : (uint32_t)(wx0 - 1);
-        const uint32_t xr = wx0 + 64 == nx ? 0u : (uint32_t)(wx0 + 64);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const uint32_t ry = cy(q) == 1 ? dym : (cy(q) == -1 ? dyp : 0u);
-            const uint32_t rz = cz(q) == 1 ? dzm : (cz(q) == -1 ? dzp : 0u);
-            const T *row = src + (r0 + ry + rz + a.qoff[q]);
-            const V v = P::ld(row + x0);
-            if (cx(q) == 0) {
-                rv[q] = v;
-            } else if (cx(q) == 1) {        // source x-1: (x0-1, x0)
-                T left = P::shup(P::hi(v));
-                if (lane == 0) left = Store<T>::ld(row + xl);
-                rv[q] = P::make(left, P::lo(v));
-            } else {                        // source x+1: (x0+1, x0+2)
-                T right = P::shdn(P::lo(v));
-                if (lane == 31) right = Store<T>::ld(row + xr);
-                rv[q] = P::make(P::hi(v), right);
-            }
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) rv[q] = P::ld(src + (cell0 + a.qoff[q]));
-    }
-    float2 aux[5] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(a.omega0)};
-    if (SMAG == LBDEM_SMAG_REFERENCE && inb) {
-        const T *ax = (const T *)a.aux;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) aux[k] = P::adec(P::ld(ax + (cell0 + a.qoff[k])));
-    }
-    uint2 key = make_uint2(0u, 0u);
-    if (a.key != nullptr && inb) key = *reinterpret_cast<const uint2 *>(a.key + cell0);
-    uint32_t la = LINK_FLUID, lb = LINK_FLUID;
-    if (inb && !a.row_simple[z * ny + y]) {
-        const uint2 l = *reinterpret_cast<const uint2 *>(a.links + cell0);
-        la = l.x;
-        lb = l.y;
-    }
-    const bool acta = inb && !(la & LINK_SKIP), actb = inb && !(lb & LINK_SKIP);
-    if (GATHER && ((la | lb) & 0x7FFFEu)) {
-#pragma unroll
-        for (int q = 1; q < Q; ++q) {
-            const T lo = (la & LINK_BB(q)) ? Store<T>::ld(src + (cell0 + a.qoff[qinv(q)])) : P::lo(rv[q]);
-            const T hi = (lb & LINK_BB(q)) ? Store<T>::ld(src + (cell0 + 1 + a.qoff[qinv(q)])) : P::hi(rv[q]);
-            rv[q] = P::make(lo, hi);
-        }
-    }
-    float2 d[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        d[q] = P::dec(rv[q], wq(q) * a.dec);
-        if (!acta) d[q].x = 0.f;
-        if (!actb) d[q].y = 0.f;
-    }
-    int ga, gb;
-    float ha[6], hb[6];
-    collide_pair<SMAG>(a, d, acta, actb, x0, y, z, cell0, aux, acta ? key.x : 0u, actb ? key.y : 0u, ga, gb, ha, hb);
-    T *dst = (T *)a.dst;
-    if (acta && actb) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) P::st(dst + (cell0 + a.qoff[q]), P::enc(d[q], a.enc / wq(q)));
-        if (SMAG == LBDEM_SMAG_REFERENCE) {
-            T *ax = (T *)a.aux;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) P::st(ax + (cell0 + a.qoff[k]), P::aenc(aux[k]));
-        }
-    } else if (acta || actb) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const V v = P::enc(d[q], a.enc / wq(q));
-            if (acta) dst[cell0 + a.qoff[q]] = P::lo(v);
-            if (actb) dst[cell0 + 1 + a.qoff[q]] = P::hi(v);
-        }
-        if (SMAG == LBDEM_SMAG_REFERENCE) {
-            T *ax = (T *)a.aux;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                const V v = P::aenc(aux[k]);
-                if (acta) ax[cell0 + a.qoff[k]] = P::lo(v);
-                if (actb) ax[cell0 + 1 + a.qoff[k]] = P::hi(v);
-            }
-        }
-    }
-    if (a.key != nullptr) {
-        reduce_forces(a, ga, ha[0], ha[1], ha[2], ha[3], ha[4], ha[5]);
-        reduce_forces(a, gb, hb[0], hb[1], hb[2], hb[3], hb[4], hb[5]);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// fused step with rows staged in shared memory by asynchronous bulk copies
-// (cp.async.bulk on the TMA engine, completion counted on an mbarrier).
-// A block owns whole lattice rows (fixed y, z; all x) and walks them
-// persistently with a two-stage ring: while the threads collide row k from
-// one stage, the copies of row k+1 land in the other.  Per row and stage:
-// for each direction q the source row (y - c_qy, z - c_qz), periodic in y and
-// z through the row index, plus the Smagorinsky state and the owner keys of
-// the row itself.  x +/- 1 neighbours (periodic in x) are read from shared
-// memory.  Requires Nx * sizeof(T) % 16 == 0 and Nx % blockDim.x == 0.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait: gives up after ~2^22 polls (each poll may suspend the thread
-// for a short while), flags LBDEM_ST_WAIT_TIMEOUT and reports failure.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int32_t *status) {
-    for (int it = 0; it < (1 << 22); ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    atomicOr(status, (int)LBDEM_ST_WAIT_TIMEOUT);
-    return false;
-}
-
-template <typename T, int SMAG>
-struct RowStage {
-    // element offsets of each staged row inside one stage
-    static __host__ __device__ size_t pop(int q, int nx) { return (size_t)q * nx; }
-    static __host__ __device__ size_t aux(int k, int nx) { return (size_t)(Q + k) * nx; }
-    static __host__ __device__ int rows() { return Q + (SMAG == LBDEM_SMAG_REFERENCE ? 5 : 0); }
-    static __host__ __device__ size_t bytes(int nx, bool keys) {
-        return (size_t)rows() * nx * sizeof(T) + (keys ? (size_t)nx * sizeof(uint32_t) : 0);
-    }
-};
-
-template <typename T, int SMAG>
-__global__ void __launch_bounds__(256, 3) k_psc_step_rows(const StepArgs a) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bars[2];
-    using RS = RowStage<T, SMAG>;
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const size_t nc = a.nc;
-    const int nrows = ny * nz;
-    const bool keys = a.key != nullptr;
-    const size_t stage_bytes = RS::bytes(nx, keys);
-    const uint32_t row_bytes = (uint32_t)(nx * sizeof(T));
-    const T *__restrict__ src = (const T *)a.src;
-    T *dst = (T *)a.dst;
-
-    auto stage_ptr = [&](int s) { return reinterpret_cast<T *>(smem + (size_t)s * stage_bytes); };
-    auto key_ptr = [&](int s) {
-        return reinterpret_cast<uint32_t *>(smem + (size_t)s * stage_bytes + (size_t)RS::rows() * nx * sizeof(T));
-    };
-    // one elected thread fills a stage with the rows needed by lattice row r
-    auto issue = [&](int r, int s) {
-        const int z = r / ny, y = r - z * ny;
-        const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
-        const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
-        T *st = stage_ptr(s);
-        mbar_expect_tx(&bars[s], (uint32_t)stage_bytes);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int ys = cy(q) == 1 ? ym : (cy(q) == -1 ? yp : y);
-            const int zs = cz(q) == 1 ? zm : (cz(q) == -1 ? zp : z);
-            bulk_g2s(st + RS::pop(q, nx), src + (size_t)q * nc + (size_t)(zs * ny + ys) * nx, row_bytes, &bars[s]);
-        }
-        if (SMAG == LBDEM_SMAG_REFERENCE) {
-            const T *ax = (const T *)a.aux;
-#pragma unroll
-            for (int k = 0; k < 5; ++k)
-                bulk_g2s(st + RS::aux(k, nx), ax + (size_t)k * nc + (size_t)r * nx, row_bytes, &bars[s]);
-        }
-        if (keys) bulk_g2s(key_ptr(s), a.key + (size_t)r * nx, (uint32_t)(nx * sizeof(uint32_t)), &bars[s]);
-    };
-
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    int r = blockIdx.x;
-    if (threadIdx.x == 0 && r < nrows) issue(r, 0);
-    bool ok = true;
-    int kfail = -1, rnfail = nrows;
-    for (int k = 0; r < nrows; ++k, r += gridDim.x) {
-        const int s = k & 1;
-        const int rn = r + gridDim.x;
-        if (threadIdx.x == 0 && rn < nrows) {
-            // the stage about to be refilled was last read before the
-            // __syncthreads that closed the previous iteration
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(rn, s ^ 1);
-        }
-        ok = mbar_wait_bounded(&bars[s], (uint32_t)((k >> 1) & 1), a.status);
-        if (!__syncthreads_and(ok)) {
-            kfail = k;
-            rnfail = rn;
-            break;
-        }
-        const int z = r / ny, y = r - z * ny;
-        const bool simple = a.row_simple[r] != 0;
-        const T *st = stage_ptr(s);
-        for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-            const uint32_t cell = (uint32_t)r * (uint32_t)nx + (uint32_t)x;
-            const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
-            const uint32_t lk = simple ? LINK_FLUID : a.links[cell];
-            const bool act = !(lk & LINK_SKIP);
-            float d[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : x);
-                T v = st[RS::pop(q, nx) + xs];
-                if (q != 0 && (lk & LINK_BB(q))) v = Store<T>::ld(src + (size_t)qinv(q) * nc + cell);
-                d[q] = act ? Store<T>::dec(v, wq(q) * a.dec) : 0.f;
-            }
-            float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
-            if (SMAG == LBDEM_SMAG_REFERENCE) {
-#pragma unroll
-                for (int kk = 0; kk < 5; ++kk) aux[kk] = aux_dec<T>(st[RS::aux(kk, nx) + x]);
-            }
-            const uint32_t key = (keys && act) ? key_ptr(s)[x] : 0u;
-            int gid;
-            float hx, hy, hz, tx, ty, tz;
-            collide_cell<SMAG>(a, d, act, cell, x, y, z, aux, key, gid, hx, hy, hz, tx, ty, tz);
-            if (act) {
-#pragma unroll
-                for (int q = 0; q < Q; ++q) dst[(size_t)q * nc + cell] = Store<T>::enc(d[q], a.enc / wq(q));
-                if (SMAG == LBDEM_SMAG_REFERENCE) {
-                    T *ax = (T *)a.aux;
-#pragma unroll
-                    for (int kk = 0; kk < 5; ++kk) ax[(size_t)kk * nc + cell] = aux_enc<T>(aux[kk]);
-                }
-            }
-            if (keys) reduce_forces(a, gid, hx, hy, hz, tx, ty, tz);
-        }
-        __syncthreads();
-    }
-    // after a timeout, wait (bounded again) for this block's copies still in
-    // flight before its shared memory is released
-    if (kfail >= 0 && threadIdx.x == 0) {
-        mbar_wait_bounded(&bars[kfail & 1], (uint32_t)((kfail >> 1) & 1), a.status);
-        if (rnfail < nrows) mbar_wait_bounded(&bars[(kfail + 1) & 1], (uint32_t)(((kfail + 1) >> 1) & 1), a.status);
-    }
+    if (psc) reduce_forces(a, cf[0]);
 }
 
 // stream only: move post-collision populations to their cells and compute
@@ -882,28 +467,31 @@ __global__ void __launch_bounds__(256) k_stream_moments(const StepArgs a, float 
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t nc = a.nc;
     if (x >= nx || y >= ny) return;
-    const uint32_t cell = (uint32_t)(z * ny + y) * (uint32_t)nx + (uint32_t)x;
+    const uint32_t row = (uint32_t)(z * ny + y);
+    const uint32_t cell = row * (uint32_t)nx + (uint32_t)x;
     uint32_t lk = LINK_FLUID;
-    if (!a.row_simple[z * ny + y]) lk = a.links[cell];
+    if (!a.row_simple[row]) lk = a.links[cell];
     if (lk & LINK_SKIP) return;
-    const T *src = (const T *)a.src;
-    T *dst = (T *)a.dst;
+    const T *src = static_cast<const T *>(a.src);
+    T *dst = static_cast<T *>(a.dst);
+    const uint32_t rs = a.rs;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
     const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+    const uint32_t own = row * rs + xslot((uint32_t)x, QB);
     float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         T v;
         if (q != 0 && (lk & LINK_BB(q))) {
-            v = src[(size_t)qinv(q) * nc + cell];
+            v = src[own + qinv(q) * 32];
         } else {
             const int xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : x);
             const int ys = cy(q) == 1 ? ym : (cy(q) == -1 ? yp : y);
             const int zs = cz(q) == 1 ? zm : (cz(q) == -1 ? zp : z);
-            v = src[(size_t)q * nc + ((uint32_t)(zs * ny + ys) * (uint32_t)nx + xs)];
+            v = src[(uint32_t)(zs * ny + ys) * rs + xslot((uint32_t)xs, QB) + q * 32];
         }
-        dst[(size_t)q * nc + cell] = v;
+        dst[own + q * 32] = v;
         const float dq = Store<T>::dec(v, wq(q) * a.dec);
         drho += dq;
         jx += cx(q) * dq;
@@ -922,10 +510,14 @@ __global__ void __launch_bounds__(256) k_stream_moments(const StepArgs a, float 
 // f = feq(rho, u) (initialize, psclattice3d.py:60-75)
 template <typename T>
 __global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_in, int smag_ref) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
     const size_t nc = a.nc;
-    const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    T *dst = (T *)a.dst;
+    const uint32_t row = (uint32_t)(z * a.ny + y);
+    const uint32_t c = row * (uint32_t)a.nx + (uint32_t)x;
+    T *dst = static_cast<T *>(a.dst) + (row * a.rs + xslot((uint32_t)x, QB));
     const bool skip = (a.links[c] & LINK_SKIP) != 0;
     const float rho = skip ? 1.f : rho_in[c];
     const float ux = skip ? 0.f : vel_in[c], uy = skip ? 0.f : vel_in[nc + c], uz = skip ? 0.f : vel_in[2 * nc + c];
@@ -935,15 +527,15 @@ __global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_i
     for (int q = 0; q < Q; ++q) {
         const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
         const float fe = wq(q) * (drho + rho * (3.f * cu + 4.5f * cu * cu - 1.5f * usq));
-        dst[(size_t)q * nc + c] = Store<T>::enc(fe, a.enc / wq(q));
+        dst[q * 32] = Store<T>::enc(fe, a.enc / wq(q));
     }
     if (smag_ref) {
-        T *ax = (T *)a.aux;
-        ax[c] = aux_enc<T>(drho);
-        ax[nc + c] = aux_enc<T>(ux);
-        ax[2 * nc + c] = aux_enc<T>(uy);
-        ax[3 * nc + c] = aux_enc<T>(uz);
-        ax[4 * nc + c] = aux_enc<T>(a.omega0);
+        T *ax = static_cast<T *>(a.aux) + (row * a.ars + xslot((uint32_t)x, AB));
+        ax[0] = aux_enc<T>(drho);
+        ax[32] = aux_enc<T>(ux);
+        ax[64] = aux_enc<T>(uy);
+        ax[96] = aux_enc<T>(uz);
+        ax[128] = aux_enc<T>(a.omega0);
     }
 }
 
@@ -1007,7 +599,9 @@ __global__ void k_decode(const StepArgs a, int smag_ref, int32_t *id, float *vol
     const int x = (int)(c % a.nx), y = (int)((c / a.nx) % a.ny), z = (int)(c / ((size_t)a.nx * a.ny));
     const int gid = (int)key_gid(key);
     const float eps = (key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f);
-    const float om = smag_ref ? aux_dec<T>(((const T *)a.aux)[4 * nc + c]) : a.omega0;
+    const uint32_t row = (uint32_t)(c / (size_t)a.nx), xx = (uint32_t)(c % (size_t)a.nx);
+    const float om = smag_ref ? aux_dec<T>(static_cast<const T *>(a.aux)[row * a.ars + xslot(xx, AB) + 4 * 32])
+                              : a.omega0;
     const float taum = 1.f / om - 0.5f;
     id[c] = gid;
     volfrac[c] = eps;
@@ -1025,13 +619,15 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_sums(const StepArgs a, double *partials) {
     const size_t nc = a.nc;
     double m = 0, px = 0, py = 0, pz = 0;
-    const T *f = (const T *)a.src;
+    const T *f = static_cast<const T *>(a.src);
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
         if (a.links[c] & LINK_SKIP) continue;
+        const uint32_t row = (uint32_t)(c / (size_t)a.nx), x = (uint32_t)(c % (size_t)a.nx);
+        const T *p = f + (row * a.rs + xslot(x, QB));
         float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const float dq = Store<T>::dec(f[(size_t)q * nc + c], wq(q) * a.dec);
+            const float dq = Store<T>::dec(p[q * 32], wq(q) * a.dec);
             dr += dq; jx += cx(q) * dq; jy += cy(q) * dq; jz += cz(q) * dq;
         }
         m += 1.0 + (double)dr;
@@ -1064,40 +660,45 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
         set_error("invalid lattice descriptor");
         return LBDEM_ERR_ARG;
     }
-    if ((size_t)L->nx * L->ny * L->nz * Q >= (1ull << 32)) {
-        set_error("lattice has %zu cells; element offsets are 32-bit, so at most %llu cells are supported",
-                  (size_t)L->nx * L->ny * L->nz, (unsigned long long)((1ull << 32) / Q - 1));
+    const size_t nb = ((size_t)L->nx + 31) / 32;
+    if (nb * 32 * L->ny * L->nz * Q >= (1ull << 32)) {
+        set_error("lattice has %zu cells (%zu with x padded to 32); element offsets are 32-bit, so at most %llu "
+                  "padded cells are supported",
+                  (size_t)L->nx * L->ny * L->nz, nb * 32 * L->ny * L->nz, (unsigned long long)((1ull << 32) / Q - 1));
         return LBDEM_ERR_ARG;
     }
     memset(&a, 0, sizeof(a));
     a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
     a.nc = (size_t)L->nx * L->ny * L->nz;
-    for (int q = 0; q < Q; ++q) a.qoff[q] = (uint32_t)(q * a.nc);
+    a.nb = (uint32_t)nb;
+    a.rs = (uint32_t)nb * QB;
+    a.ars = (uint32_t)nb * AB;
     a.omega0 = L->omega0;
     a.inv_omega0 = 1.f / L->omega0;
-    a.smag_c2 = L->smag_cs * L->smag_cs;
-    a.force_on = L->force_on;
-    a.f3x = 3.f * L->force[0]; a.f3y = 3.f * L->force[1]; a.f3z = 3.f * L->force[2];
-    if (L->storage == LBDEM_F32) {
-        a.dec = 1.f; a.enc = 1.f;
-    } else {
+    a.smag_k = 4.5f * L->smag_cs * L->smag_cs;
+    float S = 1.f;
+    if (L->storage != LBDEM_F32) {
         if (!(L->scale16 > 0.f)) {
             set_error("scale16 must be positive for 16-bit storage");
             return LBDEM_ERR_ARG;
         }
-        a.dec = 1.f / L->scale16;
-        a.enc = L->scale16;
+        S = L->scale16;
+    }
+    a.S = S;
+    a.dec = 1.f / S;
+    a.enc = S;
+    a.W0 = (1.f / 3.f) / S;
+    a.W1 = (1.f / 18.f) / S;
+    a.W2 = (1.f / 36.f) / S;
+    if (L->force_on) {
+        a.g3x = 3.f * S * L->force[0];
+        a.g3y = 3.f * S * L->force[1];
+        a.g3z = 3.f * S * L->force[2];
     }
     a.aux = L->aux;
     a.links = L->links;
     a.row_simple = L->row_simple;
     a.status = L->status;
-    {
-        const char *k = getenv("LBDEM_STEP_KERNEL");
-        a.kernel_choice = (k && strcmp(k, "one") == 0) ? 1
-                          : (k && strcmp(k, "pair") == 0) ? 2
-                          : (k && strcmp(k, "rows") == 0) ? 3 : 0;
-    }
     if (!a.links || !a.row_simple || !a.status) {
         set_error("links, row_simple and status are required");
         return LBDEM_ERR_ARG;
@@ -1109,10 +710,10 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
     return LBDEM_OK;
 }
 
-static void step_geometry(const lbdem_lattice *L, dim3 &grid, dim3 &block) {
+static void step_geometry(const lbdem_lattice *L, dim3 &grid, dim3 &block, int nthreads = 256) {
     int bx = ((L->nx + 31) / 32) * 32;
-    if (bx > 256) bx = 256;
-    int by = 256 / bx;
+    if (bx > nthreads) bx = nthreads;
+    int by = nthreads / bx;
     if (by > L->ny) by = L->ny;
     block = dim3(bx, by, 1);
     grid = dim3((L->nx + bx - 1) / bx, (L->ny + by - 1) / by, L->nz);
@@ -1143,61 +744,9 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
         a.moment_fluid = G->moment_fluid;
         a.hydro_out = P->hydro_out;
     }
-    // Rows staged in shared memory by bulk copies (opt-in: measured slower
-    // than the register-gather kernels on 256^3, see the design notes).
-    if (gather && a.kernel_choice == 3 && (L->nx % 32) == 0) {
-        const bool keys = a.key != nullptr;
-        size_t stage = 0;
-        void (*kern)(StepArgs) = nullptr;
-        if (L->smag_mode == LBDEM_SMAG_OFF) {
-            kern = k_psc_step_rows<T, LBDEM_SMAG_OFF>;
-            stage = RowStage<T, LBDEM_SMAG_OFF>::bytes(L->nx, keys);
-        } else if (L->smag_mode == LBDEM_SMAG_REFERENCE) {
-            kern = k_psc_step_rows<T, LBDEM_SMAG_REFERENCE>;
-            stage = RowStage<T, LBDEM_SMAG_REFERENCE>::bytes(L->nx, keys);
-        } else {
-            kern = k_psc_step_rows<T, LBDEM_SMAG_LOCAL>;
-            stage = RowStage<T, LBDEM_SMAG_LOCAL>::bytes(L->nx, keys);
-        }
-        const size_t smem = 2 * stage;
-        if (smem <= 200 * 1024) {
-            const int nt = L->nx < 256 ? L->nx : 256;
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess) {
-                int per_sm = 0, dev = 0, nsm = 0;
-                cudaGetDevice(&dev);
-                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem) == cudaSuccess && per_sm > 0) {
-                    const int nrows = L->ny * L->nz;
-                    int nb = per_sm * nsm;
-                    if (nb > nrows) nb = nrows;
-                    kern<<<nb, nt, smem, st>>>(a);
-                    return check_launch("psc_step (rows)");
-                }
-            }
-            cudaGetLastError();
-        }
-    }
     dim3 grid, block;
-    // Two cells per thread with packed FP32x2 arithmetic pays off where the
-    // step is issue-bound (16-bit storage); the FP32 form is memory-bound and
-    // runs fastest one cell per thread.  Needs Nx % 64 == 0.
-    const bool pairs = (L->nx % 64) == 0 &&
-                       (a.kernel_choice == 2 || (a.kernel_choice == 0 && L->storage != LBDEM_F32));
-    if (pairs) {
-        int bx = L->nx / 2;
-        if (bx > 128) bx = 128;
-        int by = 128 / bx;
-        if (by > L->ny) by = L->ny;
-        block = dim3(bx, by, 1);
-        grid = dim3(L->nx / 2 / bx, (L->ny + by - 1) / by, L->nz);
-    } else {
-        step_geometry(L, grid, block);
-    }
-#define LBDEM_STEP_CASE(G_, S_)                                            \
-    do {                                                                   \
-        if (pairs) k_psc_step2<T, G_, S_><<<grid, block, 0, st>>>(a);      \
-        else k_psc_step<T, G_, S_><<<grid, block, 0, st>>>(a);             \
-    } while (0)
+    step_geometry(L, grid, block, ONE_THREADS);
+#define LBDEM_STEP_CASE(G_, S_) k_psc_step<T, G_, S_><<<grid, block, 0, st>>>(a)
     if (gather) {
         if (L->smag_mode == LBDEM_SMAG_OFF) LBDEM_STEP_CASE(true, LBDEM_SMAG_OFF);
         else if (L->smag_mode == LBDEM_SMAG_REFERENCE) LBDEM_STEP_CASE(true, LBDEM_SMAG_REFERENCE);
@@ -1238,8 +787,9 @@ static int launch_init(const lbdem_lattice *L, int buf, cudaStream_t st) {
         return LBDEM_ERR_ARG;
     }
     a.dst = L->f[buf];
-    const unsigned nb = (unsigned)((a.nc + 255) / 256);
-    k_init<T><<<nb, 256, 0, st>>>(a, L->rho, L->vel, L->smag_mode == LBDEM_SMAG_REFERENCE);
+    dim3 grid, block;
+    step_geometry(L, grid, block);
+    k_init<T><<<grid, block, 0, st>>>(a, L->rho, L->vel, L->smag_mode == LBDEM_SMAG_REFERENCE);
     return check_launch("lattice_init");
 }
 

@@ -139,10 +139,14 @@ class LatticeEngine:
         nc = self.Nx * self.Ny * self.Nz
         self.ncells = nc
         dev = "cuda"
-        self._f = [torch.zeros((19, nc), dtype=tdtype, device=dev) for _ in range(2)]
+        # populations and lagged Smagorinsky state are blocked by 32 cells
+        # along x: [z][y][x // 32][q][x % 32] (x padded to a multiple of 32)
+        self._nb = (self.Nx + 31) // 32
+        nblk = self.Nz * self.Ny * self._nb
+        self._f = [torch.zeros((nblk, 19, 32), dtype=tdtype, device=dev) for _ in range(2)]
         self._rho = torch.ones(nc, dtype=torch.float32, device=dev)
         self._vel = torch.zeros((3, nc), dtype=torch.float32, device=dev)
-        self._aux = (torch.zeros((5, nc), dtype=tdtype, device=dev)
+        self._aux = (torch.zeros((nblk, 5, 32), dtype=tdtype, device=dev)
                      if smagorinsky == "reference" else None)
         self._links = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._rows = torch.zeros(self.Ny * self.Nz, dtype=torch.uint8, device=dev)
@@ -218,10 +222,15 @@ class LatticeEngine:
 
     # ------------------------------------------------------------ populations
     def _decode(self, buf):
-        d = self._f[buf].float().cpu().numpy().astype(np.float64)
-        if self._kind != N.F32:
-            d = d * (W[:, None] / self._scale)
-        return d + W[:, None]
+        # every storage form holds h = (f - w) S / w
+        h = self._unblock(self._f[buf], 19)
+        return h * (W[:, None] / self._scale) + W[:, None]
+
+    def _unblock(self, t, k):
+        """(k, Ncells) FP64 host copy of a blocked [z][y][x//32][k][x%32] buffer."""
+        a = t.float().cpu().numpy().astype(np.float64).reshape(self.Nz, self.Ny, self._nb, k, 32)
+        a = a.transpose(3, 0, 1, 2, 4).reshape(k, self.Nz, self.Ny, self._nb * 32)[..., :self.Nx]
+        return a.reshape(k, -1)
 
     def _materialize(self):
         """Bring the lattice to the reference's post-stream state on the device."""
@@ -255,7 +264,7 @@ class LatticeEngine:
     def _pull_omega(self):
         if self._aux is None:
             return np.full((self.Nx, self.Ny, self.Nz), self.omega0)
-        om = self._aux[4].float().cpu().numpy().astype(np.float64).reshape(self.Nz, self.Ny, self.Nx)
+        om = self._unblock(self._aux, 5)[4].reshape(self.Nz, self.Ny, self.Nx)
         ct = self._host_ct
         out = to_ref(om)
         skip = (ct & (CellType.OBSTACLE | CellType.VEL_LADD | CellType.FREE_SLIP | CellType.VEL_INLET_LADD)) != 0

@@ -261,35 +261,6 @@ def test_default_max_coordinate_number_flags_overflow():
         dem.check_status()
 
 
-@pytest.mark.parametrize("kernel", ["pair", "rows"])
-@pytest.mark.parametrize("storage,atol", [("f32", 1e-6), ("f16", 2e-5), ("bf16", 2e-4)])
-def test_step_kernel_variants_match_one_cell_kernel(kernel, storage, atol, monkeypatch):
-    """The two-cells-per-thread kernel (packed FP32x2 arithmetic, Nx % 64 == 0)
-    and the one-cell kernel agree: same formulas, rounding may differ by an
-    ulp, so populations within `atol` (a few storage ulps) after six steps."""
-    rng = np.random.default_rng(12)
-    nx, ny, nz = 128, 24, 20
-    pos, rad = rsa_spheres(rng, 12, (nx, ny, nz), 6.0, 9.0, gap=1.0, margin=1.0)
-    vel = rng.normal(0, 2e-3, (12, 3))
-    omg = rng.normal(0, 2e-3, (12, 3))
-    u0 = 0.02 * rng.uniform(-1, 1, (nx, ny, nz, 3))
-    out = []
-    for kern in (kernel, "one"):
-        monkeypatch.setenv("LBDEM_STEP_KERNEL", kern)
-        lat, dem, *_ = _pair(nx, ny, nz, pos, rad, vel, omg, force=(1e-5, 0, -2e-6), storage=storage)
-        lat.vel.from_numpy(u0)
-        lat.initialize()
-        for _ in range(6):
-            lat.collide()
-            lat.stream()
-        out.append((lat.f.to_numpy(), dem.gf.force_fluid.to_numpy(), lat.omega.to_numpy()))
-    monkeypatch.delenv("LBDEM_STEP_KERNEL", raising=False)
-    fl = _ct_zwalls(nx, ny, nz) == FLUID
-    assert np.abs(out[0][0] - out[1][0])[fl].max() < atol
-    assert np.abs(out[0][2] - out[1][2]).max() < 1e-4
-    assert relmax(out[0][1], out[1][1]) < 1e-3
-
-
 def test_dem_cluster_kernel_matches_split_kernels(monkeypatch):
     """The single-launch cluster DEM path and the two-launches-per-sub-step
     path give the same contact sets and states (FP64; only the order of the
