@@ -11,6 +11,7 @@ collide-stream with force reduction -> 10 DEM sub-steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16]
     python bench.py --impl reference     # FP64 CPU restatement of the reference path
+    python bench.py --adjoint [--adjoint-fd K]   # drag gradient on the frozen-bed channel (below)
 
 Prints ONE JSON line (rank 0).  Multi-GPU: independent replicas (the path is
 one GPU per the workload definition), aggregate throughput, weak scaling.
@@ -334,6 +335,101 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Differentiation workload: 128^3 channel (OBSTACLE walls at z = 0 and 127,
+# periodic x/y), 500 frozen spheres of diameter 10 placed by seeded random
+# sequential addition in z < 64 (0.2 lu gap), body force g_x = 2e-6, tau 0.6,
+# Smagorinsky off, FP32, smooth solid fraction; loss = total x-drag on the bed
+# after step 500; gradient w.r.t. g_x and every sphere centre by the adjoint
+# with checkpoints every 50 steps.  --adjoint-fd K adds FP64 central finite
+# differences (h = 1e-4 relative) of the oracle's forward for g_x and the K-1
+# largest position components.
+# ---------------------------------------------------------------------------
+ADJ_N, ADJ_NP, ADJ_STEPS, ADJ_EVERY, ADJ_G = 128, 500, 500, 50, 2e-6
+
+
+def adjoint_workload(seed=2024):
+    from tests.gpu_util import rsa_spheres
+    rng = np.random.default_rng(seed)
+    pos, rad = rsa_spheres(rng, ADJ_NP, (ADJ_N, ADJ_N, ADJ_N), 10.0, 10.0, gap=0.2, zmax=ADJ_N / 2, margin=1.0)
+    ct = np.full((ADJ_N,) * 3, 1, np.int32)
+    ct[:, :, 0] = ct[:, :, -1] = 8
+    return pos, rad, ct
+
+
+def run_adjoint(args):
+    import torch
+
+    from lbdem_taichi_b200 import _native as Nat
+    from lbdem_taichi_b200.dem3d.demconfig import HertzContactConfig
+    from lbdem_taichi_b200.lbdem.adjoint import FrozenBedDrag
+    from lbdem_taichi_b200.lbdem.psclattice3d import PSCLattice3D
+    from tests.gpu_util import make_dem
+    pos, rad, ct = adjoint_workload()
+    n = len(rad)
+    mass = 2.0 * 4.0 / 3.0 * np.pi * rad ** 3
+    dem = make_dem((0.0, ADJ_N, 0.0, ADJ_N, 0.0, ADJ_N), 0.1, (0, 0, 0),
+                   HertzContactConfig(pp_friction=0.3, pw_friction=0.3, pp_restitution=0.9, pw_restitution=0.9),
+                   rad, mass, pos, np.zeros((n, 3)), periodic=(True, True, False), freeze=np.ones(n, np.int32))
+    lat = PSCLattice3D(ADJ_N, ADJ_N, ADJ_N, 1.0 / TAU, 1.0, 1.0, 1.0, dem, body_force=(ADJ_G, 0.0, 0.0),
+                       solid_fraction="smooth")
+    lat.CT.from_numpy(ct)
+    prob = FrozenBedDrag(lat, ADJ_STEPS, direction=(1.0, 0.0, 0.0), checkpoint_every=ADJ_EVERY)
+    prob.forward()
+    prob.backward()
+    reps = max(1, min(args.steps, 5))
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    fwd, bwd = [], []
+    Nat.reset_launch_count()
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        e0.record()
+        L = prob.forward()
+        e1.record()
+        gF, gP = prob.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        fwd.append(e0.elapsed_time(e1))
+        bwd.append(e1.elapsed_time(e2))
+    launches = Nat.launch_count() // reps
+    cells = ADJ_N ** 3
+    out = {"metric": "C4 drag gradient: forward + adjoint wall time (checkpointed)", "value": round(
+        statistics.median(fwd) + statistics.median(bwd), 2), "unit": "ms", "higher_is_better": False,
+        "n_gpus": 1, "steps": ADJ_STEPS, "reps": reps, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "128^3 channel, 500 frozen spheres d=10 (RSA, z<64), g_x=2e-6, tau=0.6, "
+                               "500 steps, checkpoints every 50, smooth solid fraction"},
+        "forward_ms": round(statistics.median(fwd), 2), "backward_ms": round(statistics.median(bwd), 2),
+        "forward_mlups": round(cells * ADJ_STEPS / statistics.median(fwd) / 1e3, 1),
+        "gpu_launches": launches, "peak_mem_gb": round(torch.cuda.max_memory_allocated() / 1e9, 2),
+        "loss": L, "dL_dgx": float(gF[0]), "dL_dpos_absmax": float(np.abs(gP).max())}
+    if args.adjoint_fd > 0:
+        from oracle.oracle import frozen_bed_drag
+        F = np.array([ADJ_G, 0.0, 0.0])
+        shape = (ADJ_N,) * 3
+
+        def L64(Fv, P):
+            return frozen_bed_drag(shape, 1.0 / TAU, ct, rad, P, Fv, ADJ_STEPS)
+        t0 = time.perf_counter()
+        checks = []
+        h = 1e-4 * ADJ_G
+        fd = (L64(F + [h, 0, 0], pos) - L64(F - [h, 0, 0], pos)) / (2 * h)
+        checks.append({"param": "g_x", "adjoint": float(gF[0]), "fd64": fd, "rel": abs(gF[0] - fd) / abs(fd)})
+        order = np.argsort(-np.abs(gP).ravel())[: args.adjoint_fd - 1]
+        for flat in order:
+            i, k = divmod(int(flat), 3)
+            hp = 1e-4 * abs(pos[i, k])
+            pp, pm = pos.copy(), pos.copy()
+            pp[i, k] += hp
+            pm[i, k] -= hp
+            fdp = (L64(F, pp) - L64(F, pm)) / (2 * hp)
+            checks.append({"param": f"pos[{i},{'xyz'[k]}]", "adjoint": float(gP[i, k]), "fd64": fdp,
+                           "rel": abs(gP[i, k] - fdp) / abs(fdp)})
+        out["fd_check"] = {"h": "1e-4 relative, central, FP64 oracle forward", "cpu_seconds":
+                           round(time.perf_counter() - t0, 1), "cores": os.cpu_count(), "params": checks,
+                           "max_rel": max(c["rel"] for c in checks)}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,7 +441,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=256, help="cube edge; non-default only for profiling")
     ap.add_argument("--particles", type=int, default=2000, help="non-default only for profiling")
+    ap.add_argument("--adjoint", action="store_true", help="drag-gradient workload instead of the step")
+    ap.add_argument("--adjoint-fd", type=int, default=0, help="FP64 finite-difference checks (count)")
     args = ap.parse_args()
+    if args.adjoint:
+        run_adjoint(args)
+        return
     global NX, NY, NZ, NP
     NX = NY = NZ = args.size
     NP = args.particles

@@ -45,6 +45,13 @@
  *  lbdem_build_links      <- CellType dispatch in BasicLattice3D.stream
  *                            src/lbm3d/lbm_solver3d.py:203-236
  *  lbdem_global_sums_f64  <- (no counterpart; FP64 conservation totals)
+ *  lbdem_psc_map_smooth,
+ *  lbdem_psc_step_adjoint_f32,
+ *  lbdem_psc_force_adjoint <- (no counterpart; the reference has no gradients:
+ *                            reverse mode of PSCLattice3D.collide + stream +
+ *                            lattice2grains, psclattice3d.py:187-358,
+ *                            lbm_solver3d.py:197-240, lbm_foecelover.py:52-68,
+ *                            on a frozen bed with a smooth solid fraction)
  */
 #ifndef LBDEM_H
 #define LBDEM_H
@@ -130,6 +137,8 @@ typedef struct lbdem_psc {
     double *prev;              /* 4*n: lattice centre and mapping radius of the previous map */
     int32_t have_prev;         /* 1: prev holds a map to clear */
     float *hydro_out;          /* optional per-cell hydrodynamic force (3*Ncells) or NULL */
+    float *eps;                /* smooth solid fraction per cell (lbdem_psc_map_smooth), or NULL:
+                                  the step then takes the exact 5^3 count from the key */
 } lbdem_psc;
 
 typedef struct lbdem_dem {
@@ -196,6 +205,43 @@ int lbdem_stream_moments(const lbdem_lattice *L, int32_t src, int32_t dst, void 
 /* Expand the owner keys into the reference's per-cell PSC fields. */
 int lbdem_psc_decode(const lbdem_lattice *L, const lbdem_psc *P, int32_t *id, float *volfrac,
                      float *weight, float *velsolid, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Differentiable drag on a frozen particle bed (reverse mode).
+ *
+ * The reference's solid fraction is a count of 5^3 sub-points, piecewise
+ * constant in the particle position; for gradients the map can instead use a
+ * smooth fraction of the same effective radius r = R/dx - 1/2:
+ *     t = clamp(r - d + 1/2, 0, 1),  eps = t^2 (3 - 2t)      (d: centre distance)
+ * owner = the particle of largest eps (ties: lowest id), other cells free.
+ * Model differentiated: FP32 storage, Smagorinsky off, constant omega, frozen
+ * particles (u_s = 0), uniform body force F on every updated cell.  Loss:
+ *     L = e . sum_particles force_fluid   after the step-N kernel
+ * (e: 3 doubles, physical units of force_fluid).
+ * ------------------------------------------------------------------------- */
+
+/* Smooth map: fills P->key and P->eps (both Ncells), the particle table and
+ * zeroes the force accumulators.  scratch: Ncells uint64 (caller-owned). */
+int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G, uint64_t *scratch,
+                         void *stream);
+
+/* Reverse of one lbdem_psc_step_f32 (step n) on the lattice L (P->eps set).
+ *  f_prev  populations the forward step n read (blocked, as L->f)
+ *  lam_in  dL/d(post-collision populations of step n), blocked FP32 in units
+ *          of f (ignored when seed = 1: step n is the last step)
+ *  lam_out dL/d(f_prev), blocked FP32, written when gather = 1 (step n
+ *          streamed f_prev; gather = 0 for the first step after initialize)
+ *  bbar    Ncells FP32, dL/dB of every cell's PSC weight, accumulated (+=)
+ *  gbar    3 doubles, dL/dF accumulated (+=), F in lattice units
+ *  loss_dir 3 doubles, e of the loss */
+int lbdem_psc_step_adjoint_f32(const lbdem_lattice *L, const lbdem_psc *P, const void *f_prev, const float *lam_in,
+                               float *lam_out, float *bbar, double *gbar, const double *loss_dir, int32_t gather,
+                               int32_t seed, void *stream);
+
+/* Position gradient from dL/dB: pos_bar (n,3 doubles, physical units) +=
+ * sum over each particle's owned cells of bbar dB/deps deps/dpos. */
+int lbdem_psc_force_adjoint(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, const float *bbar,
+                            double *pos_bar, void *stream);
 
 int lbdem_dem_bin(lbdem_dem *D, void *stream);
 int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream);

@@ -52,7 +52,7 @@ class Psc(C.Structure):
     _fields_ = [("dx", C.c_double), ("dt", C.c_double), ("rho_unit", C.c_double),
                 ("xmin", C.c_double), ("ymin", C.c_double), ("zmin", C.c_double),
                 ("skip_inlet", C.c_int32), ("key", vp), ("table", vp), ("prev", vp),
-                ("have_prev", C.c_int32), ("hydro_out", vp)]
+                ("have_prev", C.c_int32), ("hydro_out", vp), ("eps", vp)]
 
 
 _DEM_PTRS = ("pos", "vel", "acc", "force", "quat", "omega", "omega_dot", "moment", "inertia", "mass", "radius",
@@ -88,6 +88,9 @@ EXPORTS = {
     "lbdem_dem_substeps": ([vp, C.c_int32, vp], C.c_int),
     "lbdem_global_sums_f64": ([vp, C.c_int32, vp, vp, vp], C.c_int),
     "lbdem_global_sums_f64_noalloc": ([vp, C.c_int32, vp, vp], C.c_int),
+    "lbdem_psc_map_smooth": ([vp, vp, vp, vp, vp], C.c_int),
+    "lbdem_psc_step_adjoint_f32": ([vp, vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp], C.c_int),
+    "lbdem_psc_force_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
 }
 
 _lib = None
@@ -96,7 +99,8 @@ _lib = None
 KERNELS_PER_CALL = {"lbdem_build_links": 2, "lbdem_lattice_init": 1, "lbdem_psc_map": 2,
                     "lbdem_psc_step_f32": 1, "lbdem_psc_step_f16": 1, "lbdem_psc_step_bf16": 1,
                     "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
-                    "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2}
+                    "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2,
+                    "lbdem_psc_map_smooth": 3, "lbdem_psc_step_adjoint_f32": 1, "lbdem_psc_force_adjoint": 1}
 _launches = [0]
 
 

@@ -6,6 +6,7 @@ Each translation unit is compiled separately:
   lbm.cu      fused PSC collide-stream and lattice helpers (FMA contraction on)
   psc_map.cu  particle -> lattice mapping, FP64, -fmad=false (bit-exact counts)
   dem.cu      DEM sub-step, FP64, -fmad=false (reference operation order)
+  adjoint.cu  reverse mode of the step on a frozen bed (drag gradients)
 and linked into one shared library with a static CUDA runtime.
 """
 from __future__ import annotations
@@ -26,6 +27,7 @@ UNITS = {
     "lbm.cu": [],
     "psc_map.cu": ["-fmad=false"],
     "dem.cu": ["-fmad=false"],
+    "adjoint.cu": [],
 }
 
 

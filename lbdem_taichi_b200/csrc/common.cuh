@@ -34,6 +34,11 @@ constexpr float CS2 = 1.0f / 3.0f;
 // populations, AB per block of the 5 lagged Smagorinsky values.
 constexpr uint32_t QB = Q * 32;
 constexpr uint32_t AB = 5 * 32;
+// Element offset, within its row, of cell x's block slot (lane x % 32 of
+// x-block x / 32; the population or auxiliary index adds q * 32).
+__host__ __device__ inline uint32_t xslot(uint32_t x, uint32_t per_block) {
+    return (x >> 5) * per_block + (x & 31u);
+}
 
 // Per-cell link mask (built once from CellType by lbdem_build_links)
 constexpr uint32_t LINK_SKIP = 1u << 19;   // cell is not updated (OBSTACLE / VEL_LADD / FREE_SLIP [/ INLET])

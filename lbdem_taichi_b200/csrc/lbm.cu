@@ -55,6 +55,7 @@ struct StepArgs {
     const uint32_t *links;
     const uint8_t *row_simple;
     const uint32_t *key;
+    const float *eps;          // smooth solid fraction per cell, or NULL (exact count in the key)
     const float4 *table;
     double fscale, tscale;
     double *force_fluid, *moment_fluid;
@@ -125,11 +126,11 @@ struct CellForce {
 // PSC quantities of one cell owned by a particle (psclattice3d.py:144-182;
 // B from the current omega as hybridlattice.py:236-245): weight B, 3 u_s,
 // and the cell's force B (j - rho u_s) with its torque about the centre.
-__device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float om, float rho, float jx, float jy,
-                                          float jz, int x, int y, int z, float &s3x, float &s3y, float &s3z,
-                                          CellForce &cf) {
+__device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float eps_smooth, float om, float rho,
+                                          float jx, float jy, float jz, int x, int y, int z, float &s3x, float &s3y,
+                                          float &s3z, CellForce &cf) {
     cf.gid = (int)key_gid(key);
-    const float eps = (key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f);
+    const float eps = a.eps ? eps_smooth : ((key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f));
     const float taum = rcp_fast(om) - 0.5f;
     const float Bw = eps * taum * rcp_fast((1.f - eps) + taum);
     const float4 t0 = a.table[4 * cf.gid + 0], t1 = a.table[4 * cf.gid + 1];
@@ -165,8 +166,8 @@ __device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float
 // uniform), so every cell takes the PSC form, fluid cells with B = 0.
 template <class V, int SMAG, class Out, class AuxOut>
 __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const bool act[], const int xs[], int y,
-                                        int z, const V aux[5], bool psc, const uint32_t key[], CellForce cf[], Out &&out,
-                                        AuxOut &&aux_out) {
+                                        int z, const V aux[5], bool psc, const uint32_t key[], const float eps[],
+                                        CellForce cf[], Out &&out, AuxOut &&aux_out) {
     using L = Lanes<V>;
     // Opposite pairs (q, q+1), q odd: sp = h_q + h_{q+1}, am = h_q - h_{q+1}.
     // Pair p = (q-1)/2 has direction c_q: p0 (1,0,0), p1 (0,1,0), p2 (0,0,1),
@@ -286,7 +287,7 @@ __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const b
     for (int i = 0; i < L::N; ++i) {
         if (key[i]) {
             float sx, sy, sz;
-            L::set(Bw, i, psc_cell(a, key[i], L::get(om, i), L::get(rho, i), L::get(jx, i), L::get(jy, i),
+            L::set(Bw, i, psc_cell(a, key[i], eps[i], L::get(om, i), L::get(rho, i), L::get(jx, i), L::get(jy, i),
                                    L::get(jz, i), xs[i], y, z, sx, sy, sz, cf[i]));
             L::set(s3x, i, sx); L::set(s3y, i, sy); L::set(s3z, i, sz);
         }
@@ -362,11 +363,6 @@ __device__ __forceinline__ void reduce_forces(const StepArgs &a, CellForce c) {
 #ifndef ONE_MIN_BLOCKS
 #define ONE_MIN_BLOCKS 4
 #endif
-// Element offset, within its row, of cell x's block slot (lane x % 32 of
-// x-block x / 32; the population or auxiliary index adds q * 32).
-__device__ __forceinline__ uint32_t xslot(uint32_t x, uint32_t per_block) {
-    return (x >> 5) * per_block + (x & 31u);
-}
 
 template <typename T, bool GATHER, int SMAG>
 __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
@@ -435,9 +431,10 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     const bool acts[1] = {act};
     const int xs[1] = {x};
     const uint32_t keys[1] = {key};
+    const float epss[1] = {(a.eps != nullptr && key) ? a.eps[cell] : 0.f};
     // post-collision values overwrite h[] and aux[] and are stored together
     collide<float, SMAG>(
-        a, h, acts, xs, y, z, aux, psc, keys, cf, [&](int q, float v) { h[q] = v; },
+        a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { h[q] = v; },
         [&](int k, float v) { aux[k] = v; });
     if (act) {
         T *d = static_cast<T *>(a.dst) + own;
@@ -598,7 +595,7 @@ __global__ void k_decode(const StepArgs a, int smag_ref, int32_t *id, float *vol
     }
     const int x = (int)(c % a.nx), y = (int)((c / a.nx) % a.ny), z = (int)(c / ((size_t)a.nx * a.ny));
     const int gid = (int)key_gid(key);
-    const float eps = (key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f);
+    const float eps = a.eps ? a.eps[c] : ((key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f));
     const uint32_t row = (uint32_t)(c / (size_t)a.nx), xx = (uint32_t)(c % (size_t)a.nx);
     const float om = smag_ref ? aux_dec<T>(static_cast<const T *>(a.aux)[row * a.ars + xslot(xx, AB) + 4 * 32])
                               : a.omega0;
@@ -737,6 +734,7 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
             return LBDEM_ERR_ARG;
         }
         a.key = P->key;
+        a.eps = P->eps;
         a.table = (const float4 *)P->table;
         a.fscale = P->rho_unit * (P->dx * P->dx * P->dx * P->dx) / (P->dt * P->dt);
         a.tscale = a.fscale * P->dx;
@@ -801,6 +799,7 @@ static int launch_decode(const lbdem_lattice *L, const lbdem_psc *P, int32_t *id
     if (rc) return rc;
     if (P) {
         a.key = P->key;
+        a.eps = P->eps;
         a.table = (const float4 *)P->table;
     }
     const unsigned nb = (unsigned)((a.nc + 255) / 256);

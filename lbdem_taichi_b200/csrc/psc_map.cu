@@ -207,7 +207,101 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Smooth solid fraction (differentiable stand-in for the 5^3 count): the same
+// effective radius r = R/dx - 1/2 (psclattice3d.py:105), a C1 ramp of one
+// lattice spacing across the surface,
+//     t = clamp(r - d + 1/2, 0, 1),  eps = t^2 (3 - 2t),
+// owner = largest eps (ties: lowest id) through atomicMax on
+// (float bits of eps) << 32 | (0xFFFFFFFF - id); no periodic images, and
+// map-skipped cells stay free, as in the reference mapping.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_map_smooth(const MapArgs a, unsigned long long *scratch) {
+    const int g = blockIdx.x;
+    double xc, yc, zc, r;
+    particle_lattice(a, g, xc, yc, zc, r);
+    const double lim = r + 0.5;
+    if (!(lim > 0.0)) return;
+    const int x0 = max(0, (int)floor(xc - lim)), x1 = min(a.nx - 1, (int)ceil(xc + lim));
+    const int y0 = max(0, (int)floor(yc - lim)), y1 = min(a.ny - 1, (int)ceil(yc + lim));
+    const int z0 = max(0, (int)floor(zc - lim)), z1 = min(a.nz - 1, (int)ceil(zc + lim));
+    const int ex = x1 - x0 + 1, ey = y1 - y0 + 1, ez = z1 - z0 + 1;
+    if (ex <= 0 || ey <= 0 || ez <= 0) return;
+    const unsigned exy = (unsigned)ex * (unsigned)ey, tot = exy * (unsigned)ez;
+    for (unsigned t = threadIdx.x; t < tot; t += blockDim.x) {
+        const unsigned kz = t / exy, rem = t - kz * exy, jy = rem / (unsigned)ex;
+        const int i = x0 + (int)(rem - jy * (unsigned)ex), j = y0 + (int)jy, k = z0 + (int)kz;
+        const size_t c = ((size_t)k * a.ny + j) * a.nx + i;
+        if (a.links[c] & LINK_MAP_SKIP) continue;
+        const double dxv = xc - i, dyv = yc - j, dzv = zc - k;
+        const double d = sqrt(dxv * dxv + dyv * dyv + dzv * dzv);
+        double tt = r - d + 0.5;
+        if (tt <= 0.0) continue;
+        if (tt > 1.0) tt = 1.0;
+        const float e = (float)(tt * tt * (3.0 - 2.0 * tt));
+        if (!(e > 0.f)) continue;
+        const unsigned long long kk =
+            ((unsigned long long)__float_as_uint(e) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)g);
+        atomicMax(scratch + c, kk);
+    }
+}
+
+__global__ void k_map_smooth_decode(size_t nc, const unsigned long long *scratch, uint32_t *key, float *eps) {
+    const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const unsigned long long kk = scratch[c];
+    if (!kk) {
+        key[c] = 0u;
+        eps[c] = 0.f;
+        return;
+    }
+    const unsigned g = 0xFFFFFFFFu - (unsigned)(kk & 0xFFFFFFFFull);
+    const float e = __uint_as_float((unsigned)(kk >> 32));
+    key[c] = (e >= 1.f ? KEY_FULL : 0u) | (0xFFFFFFu - g);
+    eps[c] = e;
+}
+
 }  // namespace lbdem
+
+extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G,
+                                    uint64_t *scratch, void *stream) {
+    using namespace lbdem;
+    if (!L || !P || !G || !P->key || !P->eps || !P->table || !L->links || !scratch) {
+        set_error("psc_map_smooth: bad arguments (key, eps, table, links and scratch are required)");
+        return LBDEM_ERR_ARG;
+    }
+    if (G->n > 0xFFFFFF) {
+        set_error("psc_map_smooth: %d particles exceed the 2^24-1 owner-key range", G->n);
+        return LBDEM_ERR_ARG;
+    }
+    if (!(P->dx > 0.0) || !(P->dt > 0.0)) {
+        set_error("psc_map_smooth: dx and dt must be positive");
+        return LBDEM_ERR_ARG;
+    }
+    const size_t nc = (size_t)L->nx * L->ny * L->nz;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(scratch, 0, nc * sizeof(uint64_t), st) != cudaSuccess) return check_launch("psc_map_smooth");
+    if (G->n > 0) {
+        MapArgs a;
+        a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
+        a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;
+        a.pos = G->pos; a.radius = G->radius; a.vel = G->vel; a.omega = G->omega;
+        a.links = L->links;
+        a.key = P->key;
+        a.table = (float4 *)P->table;
+        a.prev = P->prev;
+        a.have_prev = 0;
+        a.ff = G->force_fluid; a.mf = G->moment_fluid;
+        a.status = L->status;
+        k_map_clear<<<G->n, 128, 0, st>>>(a);
+        k_map_smooth<<<G->n, 256, 0, st>>>(a, reinterpret_cast<unsigned long long *>(scratch));
+    }
+    k_map_smooth_decode<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(
+        nc, reinterpret_cast<const unsigned long long *>(scratch), P->key, P->eps);
+    P->have_prev = 0;   // every key is rewritten; a later exact map must not rely on a clear shell
+    return check_launch("psc_map_smooth");
+}
 
 using namespace lbdem;
 

@@ -15,6 +15,10 @@ reference PSC lattice exactly):
   body_force   lattice-unit body force added as in ForcedLattice3D (default none)
   storage      "f32" | "f16" | "bf16" population storage (FP32 arithmetic)
   keep_hydroforce  also store the per-cell hydrodynamic force field
+  solid_fraction   "exact" (the reference's 5^3 sub-sample count) or "smooth"
+               (a C1 ramp of one lattice spacing across the same effective
+               surface, differentiable in the particle positions; used by
+               lbdem_taichi_b200.lbdem.adjoint)
 """
 from __future__ import annotations
 
@@ -31,10 +35,14 @@ from ..lbm3d.lbmutils import CellType
 
 class PSCLattice3D(LatticeEngine):
     def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, demslover: DEMSolver, *, smagorinsky="off",
-                 body_force=None, storage="f32", keep_hydroforce=False, skip_inlet=False):
+                 body_force=None, storage="f32", keep_hydroforce=False, skip_inlet=False,
+                 solid_fraction="exact"):
         super().__init__(Nx, Ny, Nz, omega, dx, dt, rho, smagorinsky=smagorinsky, body_force=body_force,
                          storage=storage, skip_inlet=skip_inlet)
+        if solid_fraction not in ("exact", "smooth"):
+            raise ValueError('solid_fraction must be "exact" or "smooth"')
         self.dem = demslover
+        self.solid_fraction = solid_fraction
         nc = self.ncells
         dev = "cuda"
         n = max(demslover.n, 1)
@@ -51,6 +59,13 @@ class PSCLattice3D(LatticeEngine):
         p.key, p.table, p.prev = N.ptr(self._key), N.ptr(self._table), N.ptr(self._prev)
         p.have_prev = 0
         p.hydro_out = N.ptr(self._hydro)
+        if solid_fraction == "smooth":
+            self._eps = torch.zeros(nc, dtype=torch.float32, device=dev)
+            self._map_scratch = torch.zeros(nc, dtype=torch.int64, device=dev)
+            p.eps = N.ptr(self._eps)
+        else:
+            self._eps = None
+            p.eps = None
         self._grains = N.Grains()
         g, t = self._grains, demslover._t
         g.n = demslover.n
@@ -102,7 +117,12 @@ class PSCLattice3D(LatticeEngine):
         if self.dem.n == 0:
             return
         self._sync_inputs()
-        N.call("lbdem_psc_map", C.byref(self._lat), C.byref(self._psc), C.byref(self._grains), N.stream_handle())
+        if self.solid_fraction == "smooth":
+            N.call("lbdem_psc_map_smooth", C.byref(self._lat), C.byref(self._psc), C.byref(self._grains),
+                   N.ptr(self._map_scratch), N.stream_handle())
+        else:
+            N.call("lbdem_psc_map", C.byref(self._lat), C.byref(self._psc), C.byref(self._grains),
+                   N.stream_handle())
         self._decoded = None
 
     def initialize(self):

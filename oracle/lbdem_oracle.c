@@ -335,6 +335,173 @@ void orc_global_sums(const orc_lat *L, double *out4) {
     out4[0] = m; out4[1] = px; out4[2] = py; out4[3] = pz;
 }
 
+
+/* ======================================================================== */
+/* Reverse mode on a frozen bed (no reference counterpart: the reference has */
+/* no gradients).  FP64 restatement of the adjoint that the CUDA library     */
+/* implements, written against the forward functions above (orc_collide with */
+/* psc = 1, smag = 0, frozen grains; orc_stream; orc_lattice2grains), with   */
+/* the smooth solid fraction of orc_map_smooth in place of the 5^3 count.    */
+/* ======================================================================== */
+
+/* Smooth solid fraction: t = clamp(r - d + 1/2, 0, 1), eps = t^2 (3 - 2t),
+ * r = R/dx - 1/2 as psclattice3d.py:105; owner = largest eps, ties to the
+ * lowest id; no periodic images; skipped cells stay free. */
+void orc_map_smooth(orc_lat *L, const orc_grains *G) {
+    long nc = (long)L->nx * L->ny * L->nz;
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < nc; c++) {
+        int i = (int)(c / ((long)L->ny * L->nz));
+        int j = (int)((c / L->nz) % L->ny);
+        int k = (int)(c % L->nz);
+        L->id[c] = -1;
+        L->volfrac[c] = 0.0;
+        L->weight[c] = 0.0;
+        L->velsolid[3 * c] = L->velsolid[3 * c + 1] = L->velsolid[3 * c + 2] = 0.0;
+        if (skip_cell(L, L->ct[c])) continue;
+        for (int g = 0; g < G->n; g++) {
+            double xc = (G->pos[3 * g + 0] - L->xmin + 0.5 * L->dx) / L->dx;
+            double yc = (G->pos[3 * g + 1] - L->ymin + 0.5 * L->dx) / L->dx;
+            double zc = (G->pos[3 * g + 2] - L->zmin + 0.5 * L->dx) / L->dx;
+            double r = (G->radius[g] - 0.5 * L->dx) / L->dx;
+            double dxv = xc - i, dyv = yc - j, dzv = zc - k;
+            double d = sqrt(dxv * dxv + dyv * dyv + dzv * dzv);
+            double t = r - d + 0.5;
+            if (t <= 0.0) continue;
+            if (t > 1.0) t = 1.0;
+            double eps = t * t * (3.0 - 2.0 * t);
+            if (eps > L->volfrac[c]) {
+                L->id[c] = g;
+                L->volfrac[c] = eps;
+                solid_vel(L, G, c, i, j, k, g, xc, yc, zc);
+            }
+        }
+    }
+}
+
+/* Adjoint of one orc_collide on L->f (the streamed populations of that step):
+ * lam = dL/dfpc (Q per cell) -> sbar = dL/df; bbar[c] += dL/dB,
+ * gbar[3] += dL/dF.  seed: this is the last step, whose hydrodynamic force
+ * enters L = fscale e . sum hydro (e = loss_dir). */
+void orc_adjoint_collide(const orc_lat *L, const double *lam, double *sbar, double *bbar, double *gbar,
+                         const double *loss_dir, int seed) {
+    long nc = (long)L->nx * L->ny * L->nz;
+    double fscale = (L->rho_unit * (L->dx * L->dx * L->dx * L->dx)) / (L->dt * L->dt);
+    double e[3] = {fscale * loss_dir[0], fscale * loss_dir[1], fscale * loss_dir[2]};
+    double F[3] = {0, 0, 0};
+    if (L->force_on) { F[0] = L->force[0]; F[1] = L->force[1]; F[2] = L->force[2]; }
+    double g0 = 0, g1 = 0, g2 = 0;
+#pragma omp parallel for schedule(static) reduction(+ : g0, g1, g2)
+    for (long c = 0; c < nc; c++) {
+        double *sb = sbar + Q * c;
+        for (int q = 0; q < Q; q++) sb[q] = 0.0;
+        if (skip_cell(L, L->ct[c])) continue;
+        const double *s = L->f + Q * c;
+        const double *la = lam ? lam + Q * c : NULL;
+        double om = L->omega0;
+        double B = 0.0;
+        if (L->psc && L->volfrac[c] > 0) {
+            double eps = L->volfrac[c], taum = 1.0 / om - 0.5;
+            B = (eps * taum) / ((1.0 - eps) + taum);
+        }
+        double rho = 0, j[3] = {0, 0, 0};
+        for (int q = 0; q < Q; q++) {
+            rho += s[q];
+            j[0] += CX[q] * s[q]; j[1] += CY[q] * s[q]; j[2] += CZ[q] * s[q];
+        }
+        double jj = j[0] * j[0] + j[1] * j[1] + j[2] * j[2];
+        double feq[Q];
+        for (int q = 0; q < Q; q++) {
+            double cj = CX[q] * j[0] + CY[q] * j[1] + CZ[q] * j[2];
+            feq[q] = W[q] * (rho + 3.0 * cj + (4.5 * cj * cj - 1.5 * jj) / rho);
+        }
+        double D = 0, G[3] = {0, 0, 0}, bb = 0;
+        for (int q = 0; q < Q; q++) {
+            double lq = la ? la[q] : 0.0, lqb = la ? la[QINV[q]] : 0.0;
+            double cj = CX[q] * j[0] + CY[q] * j[1] + CZ[q] * j[2];
+            double A = (1.0 - B) * om * lq - B * lqb;
+            D += A * W[q] * (1.0 - (4.5 * cj * cj - 1.5 * jj) / (rho * rho));
+            double k = A * W[q] / rho;
+            G[0] += A * W[q] * 3.0 * CX[q] + k * (9.0 * cj * CX[q] - 3.0 * j[0]);
+            G[1] += A * W[q] * 3.0 * CY[q] + k * (9.0 * cj * CY[q] - 3.0 * j[1]);
+            G[2] += A * W[q] * 3.0 * CZ[q] + k * (9.0 * cj * CZ[q] - 3.0 * j[2]);
+            double cf = CX[q] * F[0] + CY[q] * F[1] + CZ[q] * F[2];
+            D += lq * W[q] * (B + cf / CSSQ);
+            bb += lq * ((s[QINV[q]] - feq[QINV[q]] + W[q] * rho - s[q]) + om * (s[q] - feq[q]));
+            g0 += lq * W[q] * rho * CX[q] / CSSQ;
+            g1 += lq * W[q] * rho * CY[q] / CSSQ;
+            g2 += lq * W[q] * rho * CZ[q] / CSSQ;
+        }
+        double c1 = 1.0 - B - (1.0 - B) * om;
+        for (int p = 0; p < Q; p++) {
+            double lp = la ? la[p] : 0.0, lpb = la ? la[QINV[p]] : 0.0;
+            sb[p] = lp * c1 + B * lpb + D + CX[p] * G[0] + CY[p] * G[1] + CZ[p] * G[2];
+            if (seed) sb[p] += B * (CX[p] * e[0] + CY[p] * e[1] + CZ[p] * e[2]);
+        }
+        if (seed) bb += e[0] * j[0] + e[1] * j[1] + e[2] * j[2];
+        bbar[c] += bb;
+    }
+    gbar[0] += g0; gbar[1] += g1; gbar[2] += g2;
+}
+
+/* Transpose of orc_stream for FLUID / OBSTACLE neighbours:
+ * lam_prev = dL/dfpc of the previous step from sbar = dL/df. */
+void orc_adjoint_stream(const orc_lat *L, const double *sbar, double *lam_prev) {
+    int nx = L->nx, ny = L->ny, nz = L->nz;
+    long nc = (long)nx * ny * nz;
+    int32_t stream_skip = CT_OBSTACLE | CT_VEL_LADD | CT_FREE_SLIP | CT_VEL_INLET_LADD;
+    int32_t prop = CT_FLUID | CT_VEL_ZOUHE | CT_VEL_EXIT | CT_PRE_ZOUHE;
+    memset(lam_prev, 0, sizeof(double) * Q * nc);
+    /* serial: every target is written once, but keep it simple and exact */
+    for (long c = 0; c < nc; c++) {
+        int i = (int)(c / ((long)ny * nz));
+        int j = (int)((c / nz) % ny);
+        int k = (int)(c % nz);
+        if (L->ct[c] & stream_skip) continue;
+        const double *sb = sbar + Q * c;
+        lam_prev[Q * c] += sb[0];
+        for (int q = 1; q < Q; q++) {
+            int in = (int)(i - CX[q]), jn = (int)(j - CY[q]), kn = (int)(k - CZ[q]);
+            if (in >= nx) in = 0; else if (in < 0) in = nx - 1;
+            if (jn >= ny) jn = 0; else if (jn < 0) jn = ny - 1;
+            if (kn >= nz) kn = 0; else if (kn < 0) kn = nz - 1;
+            long n = cidx(L, in, jn, kn);
+            int32_t ctn = L->ct[n];
+            if (ctn & prop) lam_prev[Q * n + q] += sb[q];
+            else if (ctn & CT_OBSTACLE) lam_prev[Q * c + QINV[q]] += sb[q];
+        }
+    }
+}
+
+/* Chain rule from bbar = dL/dB to the grain centres (physical units). */
+void orc_pos_adjoint(const orc_lat *L, const orc_grains *G, const double *bbar, double *pos_bar) {
+    long nc = (long)L->nx * L->ny * L->nz;
+    double taum = 1.0 / L->omega0 - 0.5;
+    for (long c = 0; c < nc; c++) {
+        int g = L->id[c];
+        double eps = L->volfrac[c];
+        if (g < 0 || !(eps > 0.0 && eps < 1.0)) continue;
+        int i = (int)(c / ((long)L->ny * L->nz));
+        int j = (int)((c / L->nz) % L->ny);
+        int k = (int)(c % L->nz);
+        double xc = (G->pos[3 * g + 0] - L->xmin + 0.5 * L->dx) / L->dx;
+        double yc = (G->pos[3 * g + 1] - L->ymin + 0.5 * L->dx) / L->dx;
+        double zc = (G->pos[3 * g + 2] - L->zmin + 0.5 * L->dx) / L->dx;
+        double r = (G->radius[g] - 0.5 * L->dx) / L->dx;
+        double rx = i - xc, ry = j - yc, rz = k - zc;
+        double d = sqrt(rx * rx + ry * ry + rz * rz);
+        double t = r - d + 0.5;
+        if (!(t > 0.0 && t < 1.0) || d <= 0.0) continue;
+        double de_dt = 6.0 * t * (1.0 - t);
+        double den = (1.0 - eps) + taum;
+        double dB_de = taum * (1.0 + taum) / (den * den);
+        double sc = bbar[c] * dB_de * de_dt / (d * L->dx);
+        pos_bar[3 * g] += sc * rx;
+        pos_bar[3 * g + 1] += sc * ry;
+        pos_bar[3 * g + 2] += sc * rz;
+    }
+}
+
 /* ======================================================================== */
 /* DEM                                                                       */
 /* ======================================================================== */

@@ -47,6 +47,10 @@ def lib():
         _lib.orc_dem_run_simulation.argtypes = [C.c_void_p]
         _lib.orc_dem_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         _lib.orc_dem_candidates.restype = C.c_int
+        _lib.orc_map_smooth.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.orc_adjoint_collide.argtypes = [C.c_void_p] + [C.c_void_p] * 5 + [C.c_int]
+        _lib.orc_adjoint_stream.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_pos_adjoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     return _lib
 
 
@@ -135,6 +139,20 @@ class OracleLattice:
         out = np.zeros(4)
         lib().orc_global_sums(self._bind(), _p(out))
         return out
+
+    # reverse mode on a frozen bed (smooth solid fraction)
+    def map_smooth(self, g: "OracleGrains"):
+        lib().orc_map_smooth(self._bind(), g._bind())
+
+    def adjoint_collide(self, lam, sbar, bbar, gbar, loss_dir, seed):
+        d = np.ascontiguousarray(loss_dir, np.float64)
+        lib().orc_adjoint_collide(self._bind(), _p(lam), _p(sbar), _p(bbar), _p(gbar), _p(d), int(seed))
+
+    def adjoint_stream(self, sbar, lam_prev):
+        lib().orc_adjoint_stream(self._bind(), _p(sbar), _p(lam_prev))
+
+    def pos_adjoint(self, g: "OracleGrains", bbar, pos_bar):
+        lib().orc_pos_adjoint(self._bind(), g._bind(), _p(bbar), _p(pos_bar))
 
 
 class OracleGrains:
@@ -299,3 +317,46 @@ class OracleDEM:
                 if self.cf_active[s]:
                     res[(int(self.cf_i[s]), int(self.cf_j[s]))] = self.cf_shear[s].copy()
         return res
+
+
+def frozen_bed_drag(shape, omega0, ct, radius, pos, force, n_steps, loss_dir=(1.0, 0.0, 0.0), grad=False,
+                    dx=1.0, dt=1.0, rho_unit=1.0, dom_min=(0.0, 0.0, 0.0)):
+    """FP64 drag on a frozen bed after ``n_steps`` PSC steps with the smooth
+    solid fraction: L = e . sum_particles force_fluid after the last collide
+    (the forward of lbdem_taichi_b200.lbdem.adjoint, restated with the
+    reference's own collide / stream / lattice2grains in this file).
+
+    Returns L, or (L, dL/dF (3,), dL/dpos (n, 3)) with ``grad`` (FP64 adjoint;
+    every streamed state is kept, so use small lattices)."""
+    nx, ny, nz = shape
+    lat = OracleLattice(nx, ny, nz, omega0, dx=dx, dt=dt, rho_unit=rho_unit, psc=True, force=force,
+                        dom_min=dom_min)
+    lat.ct[...] = ct
+    n = len(radius)
+    g = OracleGrains(pos, radius, np.zeros((n, 3)), np.zeros((n, 3)))
+    lat.map_smooth(g)
+    lat.initialize()
+    e = np.asarray(loss_dir, np.float64)
+    states = []
+    for step in range(1, n_steps + 1):
+        if grad:
+            states.append(lat.f.copy())
+        lat.collide()
+        lat.lattice2grains(g)
+        if step < n_steps:
+            lat.stream()
+    L = float((g.force_fluid.sum(axis=0) * e).sum())
+    if not grad:
+        return L
+    lam = np.zeros_like(lat.f)
+    sbar = np.zeros_like(lat.f)
+    bbar = np.zeros(shape)
+    gbar = np.zeros(3)
+    for step in range(n_steps, 0, -1):
+        lat.f[...] = states[step - 1]
+        lat.adjoint_collide(None if step == n_steps else lam, sbar, bbar, gbar, e, step == n_steps)
+        if step > 1:
+            lat.adjoint_stream(sbar, lam)
+    pos_bar = np.zeros((n, 3))
+    lat.pos_adjoint(g, bbar, pos_bar)
+    return L, gbar, pos_bar
