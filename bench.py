@@ -1,15 +1,17 @@
 """Benchmark of the resolved LBM-DEM (PSC) time step.
 
-Workload (dense suspension, seeded synthetic input): 256^3 D3Q19 lattice,
-periodic in x, y and z; 2000 spheres with diameters uniform in [8, 12] lattice
-units placed by random sequential addition (1 lu gap); Gaussian velocities
-(sigma 1e-3); density ratio 2.0; Hertz-Mindlin contacts (E=1e5, nu=0.3,
-restitution 0.9, friction 0.3); uniform body force 1e-6 (x) on fluid and
-particles; tau=0.6 with Smagorinsky Cs=0.1 (reference lagged form); DEM
-sub-cycled 10x per lattice step.  A step = map particles -> fused PSC
+Default workload (dense suspension, seeded synthetic input): 256^3 D3Q19
+lattice, periodic in x, y and z; 2000 spheres with diameters uniform in
+[8, 12] lattice units placed by random sequential addition (1 lu gap);
+Gaussian velocities (sigma 1e-3); density ratio 2.0; Hertz-Mindlin contacts
+(E=1e5, nu=0.3, restitution 0.9, friction 0.3); uniform body force 1e-6 (x) on
+fluid and particles; tau=0.6 with Smagorinsky Cs=0.1 (reference lagged form);
+DEM sub-cycled 10x per lattice step.  A step = map particles -> fused PSC
 collide-stream with force reduction -> 10 DEM sub-steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16]
+    python bench.py --workload c5        # 512x512x256 channel, 20000 spheres, LES
+    python bench.py --workload c1        # single sphere settling, 64x64x128
     python bench.py --impl reference     # FP64 CPU restatement of the reference path
     python bench.py --adjoint [--adjoint-fd K]   # drag gradient on the frozen-bed channel (below)
 
@@ -33,13 +35,36 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MLUPS & HBM-roofline % for D3Q19 PSC step, FP16-store vs FP32 at ≤1e-3 drag err"
-NX = NY = NZ = 256
-NP = 2000       # overridable (--size/--particles) only for small profiling cases
-SUB = 10
-TAU = 0.6
-CS = 0.1
-GBODY = 1e-6
 BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}   # 19 reads + 19 writes of the storage type
+# DRAM read + write per cell of the step kernel, from the ncu capture of the
+# 128^3 case (see profiles/k_psc_step_128cube_full.md), scaled by the cells of a launch
+TRAFFIC_PER_CELL = {"f32": 177.4, "f16": 85.7, "bf16": 85.7}
+
+# Workloads (lattice units).  c2 is the headline configuration; c5 and c1 are
+# the large channel and the single settling sphere.  Parameters the workload
+# descriptions leave open are fixed here and used identically by the oracle.
+WORKLOADS = {
+    "c2": dict(desc="dense suspension 256^3 periodic, 2000 spheres d~U[8,12], Hertz e=0.9, body force 1e-6, "
+                    "tau=0.6, Smagorinsky Cs=0.1 (lagged), 10 DEM sub-steps",
+               shape=(256, 256, 256), n=2000, dmin=8.0, dmax=12.0, gap=1.0, walls_z=False, tau=0.6, cs=0.1,
+               fluid_force=(1e-6, 0.0, 0.0), gravity=(1e-6, 0.0, 0.0), rho_p=2.0, vel_sigma=1e-3, sub=10),
+    "c5": dict(desc="large channel 512x512x256, periodic x/y, no-slip walls at z=0,255, 20000 spheres "
+                    "d~U[6,10], Hertz e=0.9, body force 1e-6, tau=0.51, Smagorinsky Cs=0.12 (lagged), "
+                    "10 DEM sub-steps",
+               shape=(512, 512, 256), n=20000, dmin=6.0, dmax=10.0, gap=0.5, walls_z=True, tau=0.51, cs=0.12,
+               fluid_force=(1e-6, 0.0, 0.0), gravity=(1e-6, 0.0, 0.0), rho_p=2.0, vel_sigma=1e-3, sub=10),
+    "c1": dict(desc="single sphere d=12 settling in 64x64x128, periodic x/y, no-slip walls at z=0,127, density "
+                    "ratio 2.5, gravity 1e-5 (-z, buoyancy-reduced on the particle), tau=0.6, Smagorinsky Cs=0.1 "
+                    "(lagged), Hertz with the bottom wall, 10 DEM sub-steps",
+               shape=(64, 64, 128), n=1, dmin=12.0, dmax=12.0, gap=0.0, walls_z=True, tau=0.6, cs=0.1,
+               fluid_force=None, gravity=(0.0, 0.0, -1e-5 * (1.0 - 1.0 / 2.5)), rho_p=2.5, vel_sigma=0.0, sub=10),
+}
+W = dict(WORKLOADS["c2"], key="c2")
+NX, NY, NZ = W["shape"]
+NP = W["n"]
+SUB = W["sub"]
+TAU = W["tau"]
+CS = W["cs"]
 
 
 def peaks():
@@ -52,13 +77,27 @@ def peaks():
 
 
 def workload(seed=2024):
-    """Seeded C2 inputs (lattice units)."""
-    from tests.gpu_util import rsa_spheres   # pure numpy helper
+    """Seeded inputs of the selected workload (lattice units)."""
+    from tests.gpu_util import rsa_spheres_grid   # pure numpy helper
     rng = np.random.default_rng(seed)
-    pos, rad = rsa_spheres(rng, NP, (NX, NY, NZ), 8.0, 12.0, gap=1.0, margin=0.5)
-    vel = rng.normal(0.0, 1e-3, (NP, 3))
-    mass = 2.0 * 4.0 / 3.0 * np.pi * rad ** 3
+    if W["key"] == "c1":
+        pos = np.array([[NX / 2 + rng.uniform(-0.5, 0.5), NY / 2 + rng.uniform(-0.5, 0.5), NZ - 18.0]])
+        rad = np.array([0.5 * W["dmin"]])
+    else:
+        zlo = 1.0 if W["walls_z"] else None
+        zhi = NZ - 1.0 if W["walls_z"] else None
+        pos, rad = rsa_spheres_grid(rng, NP, (NX, NY, NZ), W["dmin"], W["dmax"], gap=W["gap"], zmin=zlo, zmax=zhi,
+                                    margin=0.5)
+    vel = rng.normal(0.0, W["vel_sigma"], (NP, 3)) if W["vel_sigma"] > 0 else np.zeros((NP, 3))
+    mass = W["rho_p"] * 4.0 / 3.0 * np.pi * rad ** 3
     return pos, rad, vel, mass
+
+
+def cell_types():
+    ct = np.full((NX, NY, NZ), 1, np.int32)
+    if W["walls_z"]:
+        ct[:, :, 0] = ct[:, :, -1] = 8
+    return ct
 
 
 def build_gpu(storage, pos, rad, vel, mass):
@@ -67,16 +106,19 @@ def build_gpu(storage, pos, rad, vel, mass):
     from lbdem_taichi_b200.dem3d.demsolver import DEMSolver
     from lbdem_taichi_b200.lbdem.psclattice3d import PSCLattice3D
     domain = (0.0, float(NX), 0.0, float(NY), 0.0, float(NZ))
-    cfg = DEMSolverConfig(DomainBounds(*domain), 1.0 / SUB, Vector3(GBODY, 0, 0),
+    cfg = DEMSolverConfig(DomainBounds(*domain), 1.0 / SUB, Vector3(*W["gravity"]),
                           HertzContactConfig(pp_friction=0.3, pw_friction=0.3, pp_restitution=0.9, pw_restitution=0.9))
     cfg.set_particle_properties(elastic_modulus=1e5, poisson_ratio=0.3, max_coordinate_number=16)
     cfg.set_wall_properties(elastic_modulus=1e5, poisson_ratio=0.3)
-    cfg.set_periodic_boundaries(True, True, True)
+    cfg.set_periodic_boundaries(True, True, not W["walls_z"])
     dem = DEMSolver(cfg)
     dem.init_particle_arrays(rad, mass, pos, vel, Vector3(0, 0, 0), Vector3(NX, NY, NZ))
     dem.set_contact_model("hertz")
     lat = PSCLattice3D(NX, NY, NZ, 1.0 / TAU, 1.0, 1.0, 1.0, dem, smagorinsky="reference",
-                       body_force=(GBODY, 0.0, 0.0), storage=storage)
+                       body_force=W["fluid_force"], storage=storage)
+    lat.SmagorinskyConstant = CS
+    if W["walls_z"]:
+        lat.CT.from_numpy(cell_types())
     lat.initialize()
     return lat, dem
 
@@ -158,8 +200,12 @@ def run_gpu(args):
     lat.check_status()
     dem.check_status()
 
-    # ---- device-resident throughput (inputs already in HBM); the populations
-    # (1.27 GB FP32) exceed L2, so no flush is needed between steps
+    # ---- device-resident throughput (inputs already in HBM).  When the
+    # populations do not exceed L2 several times over, a 256 MB buffer is
+    # rewritten between steps (outside the per-step events) to flush L2.
+    cells = NX * NY * NZ
+    pop_gb = 2 * 19 * cells * (4 if args.storage == "f32" else 2) / 1e9
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda") if pop_gb <= 0.5 else None
     mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     ev_step = [(mk(), mk()) for _ in range(args.steps)]
     ev_phase = [(mk(), mk(), mk()) for _ in range(args.steps)]   # before map, after step kernel, after DEM
@@ -173,6 +219,8 @@ def run_gpu(args):
     with Clocks(local) as clk:
         t0.record(st)
         for k in range(args.steps):
+            if flush is not None:
+                flush.fill_(float(k))
             lat._kernel_events = ev_step[k]
             ev_phase[k][0].record(st)
             lat.collide()
@@ -186,7 +234,8 @@ def run_gpu(args):
     lat._kernel_events = None
     launches = Nat.launch_count()
     barrier()
-    ms = t0.elapsed_time(t1)
+    # with a flush the step time is the sum of the per-step events (map to end of DEM)
+    ms = t0.elapsed_time(t1) if flush is None else sum(a.elapsed_time(c) for a, _, c in ev_phase)
     ms_t = torch.tensor([ms], device="cuda")
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -232,25 +281,26 @@ def run_gpu(args):
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_ms = float(e2e_t.item())
 
-    cells = NX * NY * NZ
     value = world * cells * args.steps / (ms * 1e-3) / 1e6
     e2e_value = world * cells * e_steps / (e2e_ms * 1e-3) / 1e6
     peak, peak_kind = peaks()
     bpc = BYTES_PER_CELL[args.storage]
+    l2_note = (f"inputs larger than L2 (populations {pop_gb:.2f} GB); no flush" if flush is None else
+               f"populations {pop_gb:.2f} GB; L2 flushed between steps (256 MB rewrite outside the step events)")
     achieved = bpc * cells / (kern_ms * 1e-3) / 1e9
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
-        "config": {"workload": "dense suspension 256^3 periodic, 2000 spheres d~U[8,12], Hertz e=0.9, "
-                               "body force 1e-6, tau=0.6, Smagorinsky Cs=0.1 (lagged), 10 DEM sub-steps",
+        "config": {"workload": W["desc"], "name": W["key"],
                    "lattice": [NX, NY, NZ], "particles": NP, "dem_subcycles": SUB, "storage": args.storage,
-                   "l2": "inputs larger than L2 (populations 1.27 GB FP32 / 0.64 GB 16-bit); no flush",
-                   "parallelism": f"replicas x{world}"},
+                   "l2": l2_note, "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "kernel": f"lbdem_psc_step_{args.storage}", "kernel_ms": round(kern_ms, 4),
-                     "bytes_per_cell": bpc, "traffic": None},
+                     "bytes_per_cell": bpc,
+                     "traffic": round(TRAFFIC_PER_CELL[args.storage] * cells / 1e9, 4),
+                     "traffic_unit": "GB per launch (DRAM read+write per cell from the 128^3 ncu capture x cells)"},
         "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 2 * NP * 3 * 8,
                 "d2h_bytes_per_step": 4 * NP * 3 * 8},
         "gpu_launches": launches,
@@ -267,16 +317,21 @@ def run_gpu(args):
         print(json.dumps(out), flush=True)
 
 
-def cpu_sample(pos, rad, vel, mass, nz_slab=8):
+def slab_depth():
+    """z-depth of the CPU sample: the oracle maps by probing every particle for
+    every cell, so the slab keeps cells x particles near 2e8 per step."""
+    return int(max(1, min(NZ, 8, 2e8 // max(1, NX * NY * NP))))
+
+
+def cpu_sample(pos, rad, vel, mass, nz_slab):
     """Oracle (FP64 C restatement of the reference) on a z-slab of the workload
     carrying every particle: same per-cell work (grains2lattice probes all
-    particles for every cell), 256x256x`nz_slab` cells."""
+    particles for every cell), NX x NY x `nz_slab` cells."""
     from oracle.oracle import OracleDEM, OracleGrains, OracleLattice
-    lat = OracleLattice(NX, NY, nz_slab, 1.0 / TAU, smag=True, psc=True, force=(GBODY, 0.0, 0.0),
-                        smag_cs=CS)
-    dem = OracleDEM(pos, vel, rad, mass, dt=1.0 / SUB, gravity=(GBODY, 0, 0), domain=(0, NX, 0, NY, 0, NZ),
-                    periodic=(True, True, True), E=1e5, nu=0.3, wall_E=1e5, wall_nu=0.3, pp_mu=0.3, pw_mu=0.3,
-                    pp_e=0.9, pw_e=0.9, max_coord=16)
+    lat = OracleLattice(NX, NY, nz_slab, 1.0 / TAU, smag=True, psc=True, force=W["fluid_force"], smag_cs=CS)
+    dem = OracleDEM(pos, vel, rad, mass, dt=1.0 / SUB, gravity=W["gravity"], domain=(0, NX, 0, NY, 0, NZ),
+                    periodic=(True, True, not W["walls_z"]), E=1e5, nu=0.3, wall_E=1e5, wall_nu=0.3, pp_mu=0.3,
+                    pw_mu=0.3, pp_e=0.9, pw_e=0.9, max_coord=16)
     g = OracleGrains(dem.pos, dem.radius, dem.vel, dem.omega)
     g.force_fluid, g.moment_fluid = dem.force_fluid, dem.moment_fluid
     lat.initialize()
@@ -293,7 +348,7 @@ def cpu_step(lat, dem, g):
 
 
 def cpu_baseline(pos, rad, vel, mass, budget_s=20.0):
-    nz_slab = 8
+    nz_slab = slab_depth()
     lat, dem, g = cpu_sample(pos, rad, vel, mass, nz_slab)
     t0 = time.perf_counter()
     steps = 0
@@ -305,7 +360,7 @@ def cpu_baseline(pos, rad, vel, mass, budget_s=20.0):
     dt = time.perf_counter() - t0
     cells = NX * NY * nz_slab
     return {"value": round(cells * steps / dt / 1e6, 4), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{steps} full steps (map, collide, force reduction, stream, 10 DEM sub-steps) on a "
+            "sample": f"{steps} full steps (map, collide, force reduction, stream, {SUB} DEM sub-steps) on a "
                       f"{NX}x{NY}x{nz_slab} slab of the workload carrying all {NP} particles; FP64 C "
                       f"restatement, OpenMP {os.cpu_count()} threads"}
 
@@ -315,22 +370,23 @@ def run_reference(args):
     if rank != 0:
         return
     pos, rad, vel, mass = workload()
-    lat, dem, g = cpu_sample(pos, rad, vel, mass)
+    nz_slab = slab_depth()
+    lat, dem, g = cpu_sample(pos, rad, vel, mass, nz_slab)
     for _ in range(args.warmup_ref):
         cpu_step(lat, dem, g)
     t0 = time.perf_counter()
     for _ in range(args.steps_ref):
         cpu_step(lat, dem, g)
     dt = time.perf_counter() - t0
-    cells = NX * NY * 8
+    cells = NX * NY * nz_slab
     v = cells * args.steps_ref / dt / 1e6
+    sample = f"{NX}x{NY}x{nz_slab} slab of the workload with all {NP} particles per step"
     out = {"metric": METRIC, "value": round(v, 4), "unit": "MLUPS", "impl": "reference", "n_gpus": 0,
            "steps": args.steps_ref, "warmup": args.warmup_ref, "ms_per_step": round(dt * 1e3 / args.steps_ref, 2),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "dense suspension 256^3 periodic, 2000 spheres d~U[8,12] (per-step sample: "
-                                  "256x256x8 slab with all particles)"},
+           "config": {"workload": W["desc"] + f" (per-step sample: {sample})"},
            "cpu_baseline": {"value": round(v, 4), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
-                            "sample": "256x256x8 slab of the workload with all 2000 particles per step"},
+                            "sample": sample},
            "e2e": {"value": round(v, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -439,17 +495,23 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--size", type=int, default=256, help="cube edge; non-default only for profiling")
-    ap.add_argument("--particles", type=int, default=2000, help="non-default only for profiling")
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--size", type=int, default=0, help="cube edge override; only for small profiling cases")
+    ap.add_argument("--particles", type=int, default=0, help="particle count override; only for profiling")
     ap.add_argument("--adjoint", action="store_true", help="drag-gradient workload instead of the step")
     ap.add_argument("--adjoint-fd", type=int, default=0, help="FP64 finite-difference checks (count)")
     args = ap.parse_args()
+    global W, NX, NY, NZ, NP, SUB, TAU, CS
+    W = dict(WORKLOADS[args.workload], key=args.workload)
+    NX, NY, NZ = W["shape"]
+    NP, SUB, TAU, CS = W["n"], W["sub"], W["tau"], W["cs"]
+    if args.size:
+        NX = NY = NZ = args.size
+    if args.particles:
+        NP = args.particles
     if args.adjoint:
         run_adjoint(args)
         return
-    global NX, NY, NZ, NP
-    NX = NY = NZ = args.size
-    NP = args.particles
     args.steps_ref = max(1, min(args.steps, 3))
     args.warmup_ref = 1
     if args.impl == "reference":

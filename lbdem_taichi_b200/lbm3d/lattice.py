@@ -178,7 +178,7 @@ class LatticeEngine:
         L.nx, L.ny, L.nz = self.Nx, self.Ny, self.Nz
         L.storage = self._kind
         L.omega0 = self.omega0
-        L.smag_cs = float(type(self).SmagorinskyConstant)
+        L.smag_cs = float(self.SmagorinskyConstant)
         L.smag_mode = _SMAG[self.smagorinsky]
         if self.body_force is not None:
             L.force_on = 1
@@ -212,6 +212,9 @@ class LatticeEngine:
         self._vel.copy_(torch.from_numpy(from_ref(host, 3).reshape(3, -1).astype(np.float32)))
 
     def _sync_inputs(self):
+        # the Smagorinsky constant is a class attribute in the reference
+        # (lbm_solver3d.py:97, read at :508); drivers may change it on the class or the instance
+        self._lat.smag_cs = float(self.SmagorinskyConstant)
         self.CT.flush()
         if self._links_dirty:
             N.call("lbdem_build_links", N.ptr(self._ct_dev), self.Nx, self.Ny, self.Nz, int(self.skip_inlet),

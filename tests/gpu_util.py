@@ -61,3 +61,45 @@ def rsa_spheres(rng, n, box, dmin_, dmax_, gap=1.0, zmax=None, margin=0.0, tries
     if len(rad) < n:
         raise RuntimeError(f"RSA placed only {len(rad)} of {n} spheres")
     return np.array(pos), np.array(rad)
+
+
+def rsa_spheres_grid(rng, n, box, dmin_, dmax_, gap=1.0, zmin=None, zmax=None, margin=0.0, tries=5000000):
+    """rsa_spheres for large counts: the same seeded sequential addition with a
+    hash grid of cell size (dmax + gap) for the overlap test."""
+    lo = np.array([margin, margin, margin], float)
+    hi = np.array(box, float) - margin
+    if zmin is not None:
+        lo[2] = max(lo[2], zmin)
+    if zmax is not None:
+        hi[2] = min(hi[2], zmax)
+    cs = dmax_ + gap
+    grid = {}
+    pos, rad = [], []
+    for _ in range(tries):
+        if len(rad) == n:
+            break
+        r = 0.5 * rng.uniform(dmin_, dmax_)
+        p = rng.uniform(lo + r, hi - r)
+        c = np.floor(p / cs).astype(int)
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for j in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ()):
+                        if np.sum((pos[j] - p) ** 2) < (rad[j] + r + gap) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if not ok:
+            continue
+        grid.setdefault((c[0], c[1], c[2]), []).append(len(rad))
+        pos.append(p)
+        rad.append(r)
+    if len(rad) < n:
+        raise RuntimeError(f"RSA placed only {len(rad)} of {n} spheres")
+    return np.array(pos), np.array(rad)
