@@ -173,6 +173,8 @@ typedef struct lbdem_dem {
     double *acc_moment;    /* (n,3) contact moment accumulator, zero between sub-steps */
     int32_t parity;        /* which half of cell_count holds the current binning */
     int32_t *status;
+    uint32_t *sync;        /* 2 words of caller-owned device memory for the grid barrier of the
+                              single-launch sub-step kernel (reset by the library on every call) */
 } lbdem_dem;
 
 int lbdem_abi_version(void);
@@ -244,6 +246,10 @@ int lbdem_psc_force_adjoint(const lbdem_lattice *L, const lbdem_psc *P, const lb
                             double *pos_bar, void *stream);
 
 int lbdem_dem_bin(lbdem_dem *D, void *stream);
+
+/* Kernels launched by the calling thread's last lbdem_dem_substeps (1 for the
+ * single-launch form, 2 per sub-step for the split form); for launch counts. */
+int lbdem_dem_launches_last(void);
 int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream);
 
 /* FP64 totals over the updated (non-skipped) cells of population buffer

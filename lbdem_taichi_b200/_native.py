@@ -70,7 +70,7 @@ class Dem(C.Structure):
                 ("wall_n", C.c_double * 18), ("wall_d", C.c_double * 6), ("wall_periodic", C.c_int32 * 6)] + \
                [(n, vp) for n in _DEM_PTRS] + \
                [("cell_cap", C.c_int32), ("cell_count", vp), ("cell_list", vp), ("acc_force", vp),
-                ("acc_moment", vp), ("parity", C.c_int32), ("status", vp)]
+                ("acc_moment", vp), ("parity", C.c_int32), ("status", vp), ("sync", vp)]
 
 
 EXPORTS = {
@@ -89,6 +89,7 @@ EXPORTS = {
     "lbdem_global_sums_f64": ([vp, C.c_int32, vp, vp, vp], C.c_int),
     "lbdem_global_sums_f64_noalloc": ([vp, C.c_int32, vp, vp], C.c_int),
     "lbdem_psc_map_smooth": ([vp, vp, vp, vp, vp], C.c_int),
+    "lbdem_dem_launches_last": ([], C.c_int),
     "lbdem_psc_step_adjoint_f32": ([vp, vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp], C.c_int),
     "lbdem_psc_force_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
 }
@@ -136,7 +137,7 @@ def load(path: str = LIB_PATH):
 
 def call(name: str, *args):
     rc = getattr(load(), name)(*args)
-    _launches[0] += 2 * int(args[1]) if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
+    _launches[0] += load().lbdem_dem_launches_last() if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
     if rc != LBDEM_OK:
         msg = load().lbdem_last_error().decode(errors="replace")
         raise LbdemError(f"{name} failed (code {rc}): {msg}")

@@ -84,6 +84,8 @@ __device__ M3 rot_to_x(const double *a) {
     return R;
 }
 
+constexpr int SLOTS_IN_REGS = 16;   // contact slots whose flags are fetched with the particle state
+
 struct DemArgs {
     lbdem_dem d;
     int ncell;
@@ -126,8 +128,8 @@ __global__ void k_bin(const __grid_constant__ DemArgs A) {
 // ------------------------------- contact laws ------------------------------
 // hertz.py:45-97 / linear.py:43-101 (particle-particle), hertz.py:99-153 /
 // linear.py:103-152 (particle-wall).  `wall` selects the wall variant.
-__device__ void contact_force(const lbdem_dem &d, int i, int j, bool wall, double *shear, double delta_n,
-                              const double *vc, double *F) {
+__device__ void contact_force(const lbdem_dem &d, double rad_i, double mass_i, double rad_j, double mass_j, bool wall,
+                              double *shear, double delta_n, const double *vc, double *F) {
     const double gap = -1 * delta_n;
     const double dt = d.dt;
     double inc[3] = {vc[0] * dt, vc[1] * dt, vc[2] * dt};
@@ -140,13 +142,13 @@ __device__ void contact_force(const lbdem_dem &d, int i, int j, bool wall, doubl
                                  2.0 * (2.0 - d.nu[tj]) * (1.0 + d.nu[tj]) / d.E[tj]);
         double Rs, ms, e;
         if (wall) {
-            Rs = d.radius[i];
-            ms = d.mass[i];
+            Rs = rad_i;
+            ms = mass_i;
             e = d.e[1];
             mu = d.mu[1];
         } else {
-            Rs = 1.0 / (1.0 / d.radius[i] + 1.0 / d.radius[j]);
-            ms = 1.0 / (1.0 / d.mass[i] + 1.0 / d.mass[j]);
+            Rs = 1.0 / (1.0 / rad_i + 1.0 / rad_j);
+            ms = 1.0 / (1.0 / mass_i + 1.0 / mass_j);
             e = 0.5 * (d.e[0] + d.e[0]);
             mu = 0.5 * (d.mu[0] + d.mu[0]);
         }
@@ -163,14 +165,14 @@ __device__ void contact_force(const lbdem_dem &d, int i, int j, bool wall, doubl
         double kns, kss, dpn, dps, ms;
         if (wall) {
             kns = d.kn[0]; kss = d.ks[0]; dpn = d.dpn[0]; dps = d.dps[0];
-            ms = d.mass[i];
+            ms = mass_i;
             mu = d.mu[1];
         } else {
             kns = d.kn[0] * d.kn[0] / (d.kn[0] + d.kn[0]);
             kss = d.ks[0] * d.ks[0] / (d.ks[0] + d.ks[0]);
             dpn = 0.5 * (d.dpn[0] + d.dpn[0]);
             dps = 0.5 * (d.dps[0] + d.dps[0]);
-            ms = 1.0 / (1.0 / d.mass[i] + 1.0 / d.mass[j]);
+            ms = 1.0 / (1.0 / mass_i + 1.0 / mass_j);
             mu = 0.5 * (d.mu[0] + d.mu[0]);
         }
         const double Cn = 2. * dpn * sqrt(kns * ms);
@@ -207,21 +209,41 @@ __device__ __forceinline__ void periodic_delta(const lbdem_dem &d, const double 
     }
 }
 
+// State of particle i held in registers by its contact lanes.
+struct PState {
+    double p[3], v[3], w[3], rad, mass;
+};
+
 // resolve(i, j) (demsolver.py:638-740); forces on i accumulated in Fi/Mi,
-// forces on j added atomically.
-__device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, double *Mi_acc) {
+// forces on j added atomically.  hj/ha: i's first contact slots (partner,
+// active) as they were when the sub-step started (only i's lanes touch i's
+// slots, each for its own partner).
+__device__ __forceinline__ void resolve_pair(const lbdem_dem &d, int i, const PState &P, int n_i, const int *hj,
+                                             const int *ha, int j, double *Fi_acc, double *Mi_acc) {
     const size_t base = (size_t)i * d.maxc;
-    const int n_i = d.cfn[i];   // slots in use when the sub-step started
+    // partner state: all loads issued together
+    double pj[3], vj[3], wj[3];
+    for (int t = 0; t < 3; ++t) {
+        pj[t] = d.pos[3 * j + t];
+        vj[t] = d.vel[3 * j + t];
+        wj[t] = d.omega[3 * j + t];
+    }
+    const double rad_j = d.radius[j], mass_j = d.mass[j];
     int off = -1;
-    for (int o = 0; o < n_i && o < d.maxc; ++o)
-        if (d.cf_j[base + o] == j && d.cf_active[base + o]) {
-            off = o;
-            break;
-        }
+    const int nreg = min(n_i, min(d.maxc, SLOTS_IN_REGS));
+#pragma unroll
+    for (int o = SLOTS_IN_REGS - 1; o >= 0; --o)   // lowest matching slot wins, as a forward search
+        if (o < nreg && hj[o] == j && ha[o]) off = o;
+    if (off < 0)
+        for (int o = SLOTS_IN_REGS; o < n_i && o < d.maxc; ++o)
+            if (d.cf_j[base + o] == j && d.cf_active[base + o]) {
+                off = o;
+                break;
+            }
     double dv[3];
-    periodic_delta(d, d.pos + 3 * i, d.pos + 3 * j, dv);
+    periodic_delta(d, P.p, pj, dv);
     const double distance = sqrt(dot3(dv, dv));
-    const double gap = distance - d.radius[i] - d.radius[j];
+    const double gap = distance - P.rad - rad_j;
     bool eval = false;
     if (off >= 0) {
         if (gap < 0) eval = true;
@@ -242,14 +264,15 @@ __device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, d
     }
     if (!eval) return;
     const size_t s = base + off;
+    double sh[3] = {d.cf_shear[3 * s], d.cf_shear[3 * s + 1], d.cf_shear[3 * s + 2]};
     const double len = sqrt(dot3(dv, dv));
     const double a[3] = {dv[0] / len, dv[1] / len, dv[2] / len};
     const M3 R = rot_to_x(a);
     const double delta_n = -gap;
-    const double *pi = d.pos + 3 * i;
+    const double *pi = P.p;
     double cp[3], ri[3], rj[3];
     for (int t = 0; t < 3; ++t) {
-        cp[t] = pi[t] + a[t] * (d.radius[i] - delta_n);
+        cp[t] = pi[t] + a[t] * (P.rad - delta_n);
         d.cf_pos[3 * s + t] = cp[t];
     }
     for (int t = 0; t < 3; ++t) {
@@ -257,17 +280,16 @@ __device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, d
         rj[t] = cp[t] - (pi[t] + dv[t]);
     }
     double vci[3], vcj[3], dvc[3], vc[3];
-    cross3(d.omega + 3 * i, ri, vci);
-    cross3(d.omega + 3 * j, rj, vcj);
+    cross3(P.w, ri, vci);
+    cross3(wj, rj, vcj);
     for (int t = 0; t < 3; ++t) {
-        vci[t] += d.vel[3 * i + t];
-        vcj[t] += d.vel[3 * j + t];
+        vci[t] += P.v[t];
+        vcj[t] += vj[t];
         dvc[t] = vcj[t] - vci[t];
     }
     mv(R, dvc, vc);
-    double sh[3] = {d.cf_shear[3 * s], d.cf_shear[3 * s + 1], d.cf_shear[3 * s + 2]};
     double F[3];
-    contact_force(d, i, j, false, sh, delta_n, vc, F);
+    contact_force(d, P.rad, P.mass, rad_j, mass_j, false, sh, delta_n, vc, F);
     for (int t = 0; t < 3; ++t) {
         d.cf_shear[3 * s + t] = sh[t];
         d.cf_force[3 * s + t] = F[t];
@@ -288,25 +310,25 @@ __device__ void resolve_pair(const lbdem_dem &d, int i, int j, double *Fi_acc, d
 }
 
 // evaluate_wall (demsolver.py:742-807)
-__device__ void wall_contact(const lbdem_dem &d, int i, int w, double *Fi_acc, double *Mi_acc) {
+__device__ void wall_contact(const lbdem_dem &d, int i, const PState &P, int w, double *Fi_acc, double *Mi_acc) {
     const double *nrm = d.wall_n + 3 * w;
-    const M3 R = rot_to_x(nrm);
-    const double *p = d.pos + 3 * i;
-    const double delta_n = (dot3(p, nrm) - d.wall_d[w]) + d.radius[i];
-    const double distance = d.radius[i] - delta_n;
     const size_t s = (size_t)i * 6 + w;
+    double sh[3] = {d.wcf_shear[3 * s], d.wcf_shear[3 * s + 1], d.wcf_shear[3 * s + 2]};
+    const M3 R = rot_to_x(nrm);
+    const double *p = P.p;
+    const double delta_n = (dot3(p, nrm) - d.wall_d[w]) + P.rad;
+    const double distance = P.rad - delta_n;
     double ri[3];
     for (int t = 0; t < 3; ++t) {
         ri[t] = distance * nrm[t];
         d.wcf_pos[3 * s + t] = p[t] + ri[t];
     }
     double vci[3], m[3], vc[3];
-    cross3(d.omega + 3 * i, ri, vci);
-    for (int t = 0; t < 3; ++t) m[t] = -(vci[t] + d.vel[3 * i + t]);
+    cross3(P.w, ri, vci);
+    for (int t = 0; t < 3; ++t) m[t] = -(vci[t] + P.v[t]);
     mv(R, m, vc);
-    double sh[3] = {d.wcf_shear[3 * s], d.wcf_shear[3 * s + 1], d.wcf_shear[3 * s + 2]};
     double F[3];
-    contact_force(d, i, -1, true, sh, delta_n, vc, F);
+    contact_force(d, P.rad, P.mass, 0.0, 0.0, true, sh, delta_n, vc, F);
     for (int t = 0; t < 3; ++t) {
         d.wcf_shear[3 * s + t] = sh[t];
         d.wcf_force[3 * s + t] = F[t];
@@ -333,12 +355,31 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
     const bool act = i < d.n;
     double Fi[3] = {0.0, 0.0, 0.0}, Mi[3] = {0.0, 0.0, 0.0};
     if (act) {
-        const double *o = d.pos + 3 * i;
+        // particle state, contact-slot snapshot and wall flag fetched together
+        PState P;
+        for (int t = 0; t < 3; ++t) {
+            P.p[t] = d.pos[3 * i + t];
+            P.v[t] = d.vel[3 * i + t];
+            P.w[t] = d.omega[3 * i + t];
+        }
+        P.rad = d.radius[i];
+        P.mass = d.mass[i];
+        const int n_i = d.cfn[i];   // slots in use when the sub-step started
+        const size_t base = (size_t)i * d.maxc;
+        int hj[SLOTS_IN_REGS], ha[SLOTS_IN_REGS];
+#pragma unroll
+        for (int o = 0; o < SLOTS_IN_REGS; ++o) {
+            const bool in = o < d.maxc;
+            hj[o] = in ? d.cf_j[base + o] : -1;
+            ha[o] = in ? d.cf_active[base + o] : 0;
+        }
+        const bool wall_lane = k < 6 && !d.wall_periodic[k];
+        const int wact = wall_lane ? d.wcf_active[(size_t)i * 6 + k] : 0;
         int ijk[3], dd[3];
-        ref_cell(d, o, ijk);
+        ref_cell(d, P.p, ijk);
         for (int a = 0; a < 3; ++a) {
             const double center = (ijk[a] + 0.5) * d.cell_size + d.bp_min[a];
-            dd[a] = (o[a] > center) ? 1 : -1;
+            dd[a] = (P.p[a] > center) ? 1 : -1;
         }
         const int ox = (k == 1 || k == 5 || k == 6 || k == 7) ? dd[0] : 0;
         const int oy = (k == 2 || k == 4 || k == 6 || k == 7) ? dd[1] : 0;
@@ -349,20 +390,20 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
             const int32_t *lst = d.cell_list + (size_t)c * d.cell_cap;
             for (int t = 0; t < n; ++t) {
                 const int j = lst[t];
-                if (j > i) resolve_pair(d, i, j, Fi, Mi);
+                if (j > i) resolve_pair(d, i, P, n_i, hj, ha, j, Fi, Mi);
             }
         }
-        if (k < 6 && !d.wall_periodic[k]) {
+        if (wall_lane) {
             const int w = k;
             const size_t s = (size_t)i * 6 + w;
-            const double sep = -(dot3(o, d.wall_n + 3 * w) - d.wall_d[w]);
-            if (d.wcf_active[s]) {
-                if (sep > d.radius[i]) d.wcf_active[s] = 0;
-                else wall_contact(d, i, w, Fi, Mi);
-            } else if (sep <= d.radius[i]) {
+            const double sep = -(dot3(P.p, d.wall_n + 3 * w) - d.wall_d[w]);
+            if (wact) {
+                if (sep > P.rad) d.wcf_active[s] = 0;
+                else wall_contact(d, i, P, w, Fi, Mi);
+            } else if (sep <= P.rad) {
                 d.wcf_active[s] = 1;
                 for (int t = 0; t < 3; ++t) d.wcf_shear[3 * s + t] = d.wcf_pos[3 * s + t] = d.wcf_force[3 * s + t] = 0.0;
-                wall_contact(d, i, w, Fi, Mi);
+                wall_contact(d, i, P, w, Fi, Mi);
             }
         }
     }
@@ -395,22 +436,23 @@ __device__ M3 quat2rot(const double *q) {
     return r;
 }
 
-__device__ void rotate_update(const lbdem_dem &d, int i) {
-    const double dt = d.dt;
-    const M3 Rm = quat2rot(d.quat + 4 * i);
+// Euler rotation update (demsolver.py:590-636) on values already in registers:
+// q (4), w (3), wd (3, previous angular acceleration), moment (3), inertia (9).
+__device__ void rotate_update(double dt, double q[4], double w[3], double wd[3], const double mom[3],
+                              const double inertia[9]) {
+    const M3 Rm = quat2rot(q);
     M3 I;
     for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) I.m[r][c] = d.inertia[9 * i + 3 * r + c];
+        for (int c = 0; c < 3; ++c) I.m[r][c] = inertia[3 * r + c];
     double ml[3], wl[3], Iw[3], cw[3], rhs[3], wdl[3], alpha[3];
-    mv(Rm, d.moment + 3 * i, ml);
-    mv(Rm, d.omega + 3 * i, wl);
+    mv(Rm, mom, ml);
+    mv(Rm, w, wl);
     mv(I, wl, Iw);
     cross3(wl, Iw, cw);
     for (int t = 0; t < 3; ++t) rhs[t] = ml[t] - cw[t];
     mv(inv3(I), rhs, wdl);
     mv(inv3(Rm), wdl, alpha);
-    double *w = d.omega + 3 * i, *q = d.quat + 4 * i;
-    for (int t = 0; t < 3; ++t) w[t] += 0.5 * (d.omega_dot[3 * i + t] + alpha[t]) * dt;
+    for (int t = 0; t < 3; ++t) w[t] += 0.5 * (wd[t] + alpha[t]) * dt;
     const double dq0 = -0.5 * (q[1] * w[0] + q[2] * w[1] + q[3] * w[2]);
     const double dq1 = +0.5 * (q[0] * w[0] - q[3] * w[1] + q[2] * w[2]);
     const double dq2 = +0.5 * (q[3] * w[0] + q[0] * w[1] + q[1] * w[2]);
@@ -418,7 +460,7 @@ __device__ void rotate_update(const lbdem_dem &d, int i) {
     q[0] += dq0 * dt; q[1] += dq1 * dt; q[2] += dq2 * dt; q[3] += dq3 * dt;
     const double ql = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
     for (int t = 0; t < 4; ++t) q[t] = q[t] / ql;
-    for (int t = 0; t < 3; ++t) d.omega_dot[3 * i + t] = alpha[t];
+    for (int t = 0; t < 3; ++t) wd[t] = alpha[t];
 }
 
 __device__ __forceinline__ void wrap_position(const lbdem_dem &d, double *p) {
@@ -444,43 +486,76 @@ __global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemAr
 
 __device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, int i) {
     const double dt = d.dt;
-    // clear_state (demsolver.py:422-429) + contacts, then apply_body_force (:437-448)
+    // every input of the particle is fetched before any store, so the loads
+    // overlap (one memory round trip instead of a chain)
+    double af[3], am[3], ffl[3], mfl[3], p[3], v[3], acc[3], w[3], wd[3], q[4], I[9];
     for (int t = 0; t < 3; ++t) {
-        double f = d.acc_force[3 * i + t], m = d.acc_moment[3 * i + t];
-        d.acc_force[3 * i + t] = 0.0;
-        d.acc_moment[3 * i + t] = 0.0;
-        f += d.mass[i] * d.g[t];
+        af[t] = d.acc_force[3 * i + t];
+        am[t] = d.acc_moment[3 * i + t];
+        ffl[t] = d.force_fluid[3 * i + t];
+        mfl[t] = d.moment_fluid[3 * i + t];
+        p[t] = d.pos[3 * i + t];
+        v[t] = d.vel[3 * i + t];
+        acc[t] = d.acc[3 * i + t];
+        w[t] = d.omega[3 * i + t];
+        wd[t] = d.omega_dot[3 * i + t];
+    }
+    for (int t = 0; t < 4; ++t) q[t] = d.quat[4 * i + t];
+    for (int t = 0; t < 9; ++t) I[t] = d.inertia[9 * i + t];
+    const double mass = d.mass[i];
+    const int frozen = d.freeze[i], fixed = d.fixvel[i];
+    const size_t base = (size_t)i * d.maxc;
+    const int nfirst = d.cfn[i], nadd = d.cf_add[i];
+    int act[SLOTS_IN_REGS];
+#pragma unroll
+    for (int o = 0; o < SLOTS_IN_REGS; ++o) act[o] = o < d.maxc ? d.cf_active[base + o] : 0;
+
+    // clear_state (demsolver.py:422-429) + contacts, then apply_body_force (:437-448)
+    double force[3], moment[3];
+    for (int t = 0; t < 3; ++t) {
+        double f = af[t], m = am[t];
+        f += mass * d.g[t];
         m += 0.0;
-        f += d.force_fluid[3 * i + t];
-        m += d.moment_fluid[3 * i + t];
-        d.force[3 * i + t] = f;
-        d.moment[3 * i + t] = m;
+        f += ffl[t];
+        m += mfl[t];
+        force[t] = f;
+        moment[t] = m;
     }
     // update (demsolver.py:514-636)
-    double *p = d.pos + 3 * i, *v = d.vel + 3 * i;
-    if (!d.freeze[i]) {
-        if (d.fixvel[i]) {
+    if (!frozen) {
+        if (fixed) {
             for (int t = 0; t < 3; ++t) p[t] += v[t] * dt;
             wrap_position(d, p);
-            rotate_update(d, i);
+            rotate_update(dt, q, w, wd, moment, I);
         } else {
             double a[3];
-            for (int t = 0; t < 3; ++t) a[t] = d.force[3 * i + t] / d.mass[i];
-            for (int t = 0; t < 3; ++t) v[t] += 0.5 * (d.acc[3 * i + t] + a[t]) * dt;
+            for (int t = 0; t < 3; ++t) a[t] = force[t] / mass;
+            for (int t = 0; t < 3; ++t) v[t] += 0.5 * (acc[t] + a[t]) * dt;
             for (int t = 0; t < 3; ++t) p[t] += v[t] * dt + 0.5 * a[t] * (dt * dt);
             wrap_position(d, p);
-            for (int t = 0; t < 3; ++t) d.acc[3 * i + t] = a[t];
-            rotate_update(d, i);
+            for (int t = 0; t < 3; ++t) acc[t] = a[t];
+            rotate_update(dt, q, w, wd, moment, I);
         }
     }
-    // late_clear_state / remove_inactive_contact (demsolver.py:371-386, 431-436)
-    const size_t base = (size_t)i * d.maxc;
-    const int cnt = min(d.cfn[i] + d.cf_add[i], d.maxc);
-    int w = 0;
-    for (int o = 0; o < cnt; ++o) {
-        if (!d.cf_active[base + o]) continue;
-        if (w != o) {
-            const size_t dd = base + w, ss = base + o;
+    for (int t = 0; t < 3; ++t) {
+        d.acc_force[3 * i + t] = 0.0;
+        d.acc_moment[3 * i + t] = 0.0;
+        d.force[3 * i + t] = force[t];
+        d.moment[3 * i + t] = moment[t];
+        d.pos[3 * i + t] = p[t];
+        d.vel[3 * i + t] = v[t];
+        d.acc[3 * i + t] = acc[t];
+        d.omega[3 * i + t] = w[t];
+        d.omega_dot[3 * i + t] = wd[t];
+    }
+    for (int t = 0; t < 4; ++t) d.quat[4 * i + t] = q[t];
+    // late_clear_state / remove_inactive_contact (demsolver.py:371-386, 431-436):
+    // slots are only moved when an inactive one precedes an active one
+    const int cnt = min(nfirst + nadd, d.maxc);
+    int w_ = 0;
+    auto keep = [&](int o) {
+        if (w_ != o) {
+            const size_t dd = base + w_, ss = base + o;
             d.cf_j[dd] = d.cf_j[ss];
             d.cf_active[dd] = 1;
             for (int t = 0; t < 3; ++t) {
@@ -489,13 +564,28 @@ __device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, in
                 d.cf_force[3 * dd + t] = d.cf_force[3 * ss + t];
             }
         }
-        ++w;
-    }
-    for (int o = w; o < cnt; ++o) d.cf_active[base + o] = 0;
-    d.cfn[i] = w;
+        ++w_;
+    };
+#pragma unroll
+    for (int o = 0; o < SLOTS_IN_REGS; ++o)
+        if (o < cnt && act[o]) keep(o);
+    for (int o = SLOTS_IN_REGS; o < cnt; ++o)
+        if (d.cf_active[base + o]) keep(o);
+    for (int o = w_; o < cnt; ++o) d.cf_active[base + o] = 0;
+    d.cfn[i] = w_;
     d.cf_add[i] = 0;
     // bin the new position for the next sub-step
-    bin_particle(d, i, d.cell_count + (size_t)(parity ^ 1) * ncell);
+    int ijk[3];
+    ref_cell(d, p, ijk);
+    const int c = cell_index(d, ijk[0], ijk[1], ijk[2]);
+    if (c < 0) {
+        atomicOr(d.status, (int)LBDEM_ST_GRID_OVERFLOW);
+        return;
+    }
+    int32_t *count = d.cell_count + (size_t)(parity ^ 1) * ncell;
+    const int rank = atomicAdd(count + c, 1);
+    if (rank < d.cell_cap) d.cell_list[(size_t)c * d.cell_cap + rank] = i;
+    else atomicOr(d.status, (int)LBDEM_ST_CELL_OVERFLOW);
 }
 
 // All sub-steps of one call in ONE launch: a single thread-block cluster (up
@@ -519,6 +609,68 @@ __global__ void __launch_bounds__(512) k_dem_cluster(const __grid_constant__ Dem
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
         for (int i = me; i < d.n; i += nthr) integrate_particle(d, A.ncell, parity, i);
         cl.sync();
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// All sub-steps of one call in ONE cooperative launch (the default): every
+// block of the grid is resident (cudaLaunchCooperativeKernel), the contact
+// lanes and the particles are grid-strided, and the two phases of each
+// sub-step are separated by a grid barrier.  The barrier is a counter plus a
+// generation word in caller-owned memory (reset before each launch); its wait
+// is bounded: after ~0.25 s without progress it sets LBDEM_ST_WAIT_TIMEOUT and
+// continues, so a fault can never hang the GPU.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void grid_barrier(uint32_t *sync, unsigned &gen, int32_t *status) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();   // this block's writes of the phase, visible GPU-wide
+        const unsigned target = gen + 1;
+        if (atomicAdd(sync, 1u) == gridDim.x - 1) {
+            sync[0] = 0u;   // nobody arrives again before the generation moves
+            __threadfence();
+            st_release_gpu(sync + 1, target);
+        } else {
+            unsigned it = 0;
+            while (ld_acquire_gpu(sync + 1) != target) {
+                if (++it > (1u << 22)) {
+                    atomicOr(status, (int)LBDEM_ST_WAIT_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    gen += 1;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(128) k_dem_coop(const __grid_constant__ DemArgs A, int nsub) {
+    const lbdem_dem &d = A.d;
+    const int nthr = gridDim.x * blockDim.x;
+    const int me = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nlanes = 8 * d.n;
+    unsigned gen = 0;
+    for (int s = 0; s < nsub; ++s) {
+        const int parity = (A.parity + s) & 1;
+        const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
+        for (int base = 0; base < nlanes; base += nthr) contact_lane(d, count, base + me);
+        grid_barrier(d.sync, gen, d.status);
+        int32_t *used = d.cell_count + (size_t)parity * A.ncell;
+        for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
+        for (int i = me; i < d.n; i += nthr) integrate_particle(d, A.ncell, parity, i);
+        grid_barrier(d.sync, gen, d.status);
     }
 }
 
@@ -562,7 +714,12 @@ int lbdem_dem_bin(lbdem_dem *D, void *stream) {
     return check_launch("dem_bin");
 }
 
+static thread_local int g_dem_launches = 0;
+
+int lbdem_dem_launches_last(void) { return g_dem_launches; }
+
 int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
+    g_dem_launches = 0;
     int rc = check_dem(D);
     if (rc) return rc;
     if (D->n == 0 || nsub <= 0) return LBDEM_OK;
@@ -602,10 +759,40 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
             A.parity = D->parity;
             if (cudaLaunchKernelEx(&cfg, k_dem_cluster, A, (int)nsub) == cudaSuccess) {
                 D->parity ^= (nsub & 1);
+                g_dem_launches = 1;
                 return check_launch("dem_substeps (cluster)");
             }
             cudaGetLastError();
         }
+    }
+    // default: one cooperative launch for all sub-steps when one resident wave
+    // covers the contact lanes ("split" forces two launches per sub-step)
+    if (D->sync && !(mode && strcmp(mode, "split") == 0)) {
+        int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dem_coop, 128, 0) == cudaSuccess &&
+            per_sm > 0) {
+            // one resident wave must cover every contact lane: beyond that the
+            // grid-stride loop serialises the phases' memory-latency chains and
+            // two launches per sub-step (all lanes in flight) are faster
+            const int nb = max(nb_con, nb_int);
+            if (nb <= per_sm * nsm) {
+                if (cudaMemsetAsync(D->sync, 0, 2 * sizeof(uint32_t), st) != cudaSuccess)
+                    return check_launch("dem_substeps (barrier reset)");
+                A.parity = D->parity;
+                int nsub_arg = nsub;
+                void *args[] = {&A, &nsub_arg};
+                if (cudaLaunchCooperativeKernel((void *)k_dem_coop, dim3(nb), dim3(128), args, 0, st) ==
+                    cudaSuccess) {
+                    D->parity ^= (nsub & 1);
+                    g_dem_launches = 1;
+                    return check_launch("dem_substeps (cooperative)");
+                }
+            }
+        }
+        cudaGetLastError();
     }
     for (int s = 0; s < nsub; ++s) {
         A.parity = D->parity;
@@ -613,6 +800,7 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
         k_integrate<<<nb_int, 128, 0, st>>>(A);
         D->parity ^= 1;
     }
+    g_dem_launches = 2 * nsub;
     return check_launch("dem_substeps");
 }
 

@@ -228,6 +228,7 @@ class DEMSolver:
         self.cell_list = torch.zeros(ncell * self.cell_cap, **i32)
         self.acc_force = torch.zeros((max(n, 1), 3), **f64)
         self.acc_moment = torch.zeros((max(n, 1), 3), **f64)
+        self.sync = torch.zeros(2, **i32)
         # the reference hashes cells into a 2^k table: distinct cells alias when
         # their coordinates agree in the low bits kept by Morton-code mod 2^k
         T = reference_table_size(rmax, dmin, dmax) if n else 1 << 20
@@ -270,6 +271,7 @@ class DEMSolver:
         d.cell_cap = self.cell_cap
         d.parity = 0
         d.status = N.ptr(self.status)
+        d.sync = N.ptr(self.sync)
         self._binned = False
 
     def _set_materials(self, density):

@@ -1,0 +1,87 @@
+"""The C ABI without a GPU: the library loads, exports every function that
+include/lbdem.h declares, rejects bad arguments on the host, and the ctypes
+descriptors used by the Python classes have the C structs' layout (sizes and
+member offsets compiled from the header with gcc)."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "lbdem.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\**\s*(lbdem_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_every_declared_function_is_exported():
+    from lbdem_taichi_b200 import _native as N
+    lib = N.load()
+    names = _declared()
+    assert len(names) >= 15, names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # every declared function has a ctypes signature in the bindings, and vice versa
+    assert set(names) == set(N.EXPORTS), set(names) ^ set(N.EXPORTS)
+    assert lib.lbdem_abi_version() == 1
+
+
+def test_host_side_argument_checks():
+    from lbdem_taichi_b200 import _native as N
+    lib = N.load()
+    assert lib.lbdem_psc_step_f32(None, None, None, 0, 1, 1, None) == N.LBDEM_ERR_ARG
+    assert lib.lbdem_last_error()
+    L = N.Lattice()
+    L.nx, L.ny, L.nz = 8, 8, 8
+    L.storage, L.omega0, L.scale16 = N.F32, 1.6, 1.0
+    L.links, L.row_simple, L.status = 8, 8, 8            # never dereferenced: checks come first
+    assert lib.lbdem_psc_step_f32(C.byref(L), None, None, 0, 0, 1, None) == N.LBDEM_ERR_ARG   # src == dst
+    L.smag_mode = N.SMAG_REFERENCE                       # needs the aux buffer
+    assert lib.lbdem_psc_step_f32(C.byref(L), None, None, 0, 1, 1, None) == N.LBDEM_ERR_ARG
+    L.smag_mode = N.SMAG_OFF
+    L.storage = N.F16
+    L.scale16 = 0.0                                      # 16-bit forms need a positive scale
+    assert lib.lbdem_psc_step_f16(C.byref(L), None, None, 0, 1, 1, None) == N.LBDEM_ERR_ARG
+    L.nx, L.ny, L.nz = 2048, 2048, 64                    # 19 * padded cells >= 2^32
+    L.scale16 = 4096.0
+    assert lib.lbdem_psc_step_f16(C.byref(L), None, None, 0, 1, 1, None) == N.LBDEM_ERR_ARG
+    assert b"32-bit" in lib.lbdem_last_error()
+    # the adjoint covers FP32 storage with Smagorinsky off only
+    P = N.Psc()
+    L.nx, L.ny, L.nz, L.storage = 8, 8, 8, N.F16
+    d3 = (C.c_double * 3)(1, 0, 0)
+    rc = lib.lbdem_psc_step_adjoint_f32(C.byref(L), C.byref(P), 8, None, 8, 8, 8, d3, 1, 1, None)
+    assert rc == N.LBDEM_ERR_UNSUPPORTED
+
+
+@pytest.mark.skipif(subprocess.run(["which", "gcc"], capture_output=True).returncode != 0, reason="no gcc")
+def test_ctypes_descriptors_match_the_header():
+    from lbdem_taichi_b200 import _native as N
+    structs = {"lbdem_lattice": N.Lattice, "lbdem_grains": N.Grains, "lbdem_psc": N.Psc, "lbdem_dem": N.Dem}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    with tempfile.TemporaryDirectory() as tmp:
+        src = os.path.join(tmp, "layout.c")
+        exe = os.path.join(tmp, "layout")
+        open(src, "w").write("\n".join(lines))
+        subprocess.check_call(["gcc", "-o", exe, src])
+        out = subprocess.check_output([exe], text=True).split("\n")
+    got = {}
+    for ln in out:
+        if ln:
+            a, b, c = ln.split()
+            got[(a, b)] = int(c)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

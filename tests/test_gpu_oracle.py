@@ -261,10 +261,12 @@ def test_default_max_coordinate_number_flags_overflow():
         dem.check_status()
 
 
-def test_dem_cluster_kernel_matches_split_kernels(monkeypatch):
-    """The single-launch cluster DEM path and the two-launches-per-sub-step
-    path give the same contact sets and states (FP64; only the order of the
-    atomic force sums differs)."""
+@pytest.mark.parametrize("mode", ["cooperative", "cluster"])
+def test_dem_single_launch_kernels_match_split_kernels(mode, monkeypatch):
+    """The single-launch DEM paths -- the default cooperative grid (grid
+    barriers between phases) and the opt-in single cluster -- give the
+    contact sets and states of two launches per sub-step (FP64; only the
+    order of the atomic force sums differs)."""
     rng = np.random.default_rng(13)
     g = np.stack(np.meshgrid(np.arange(8), np.arange(8), np.arange(5), indexing="ij"), -1).reshape(-1, 3)
     pos = 2.5 + g * 3.95 + rng.uniform(-0.05, 0.05, g.shape)
@@ -274,11 +276,11 @@ def test_dem_cluster_kernel_matches_split_kernels(monkeypatch):
     mass = 2.0 * 4.0 / 3.0 * np.pi * rad ** 3
     domain = (0.0, 32.0, 0.0, 32.0, 0.0, 22.0)
     res = []
-    for mode in ("cluster", "split"):
-        if mode == "cluster":
-            monkeypatch.setenv("LBDEM_DEM_KERNELS", "cluster")
-        else:
+    for m in (mode, "split"):
+        if m == "cooperative":
             monkeypatch.delenv("LBDEM_DEM_KERNELS", raising=False)
+        else:
+            monkeypatch.setenv("LBDEM_DEM_KERNELS", m)
         dem = make_dem(domain, 0.05, (0, 0, -1e-3), _hertz(), rad, mass, pos, vel, periodic=(True, True, False),
                        max_coord=24, E=1e3, wall_E=1e3)
         dem.run_substeps(17)
