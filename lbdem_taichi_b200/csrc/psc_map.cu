@@ -96,9 +96,10 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
 //     (psclattice3d.py:108-113).  FP32 with a safety margin decides the clear
 //     cases; the exact FP64 comparisons run only for cells near a threshold.
 //     Full covers are claimed at once; partial cells go to a shared list.
-//  2. one warp per partial cell counts its 5^3 sub-points
-//     (psclattice3d.py:121-131): lane (ii, jj) < 25 tests the column of five
-//     kk sub-points, the warp sums with __reduce_add_sync.  A sub-point whose
+//  2. one thread per partial cell counts its 5^3 sub-points
+//     (psclattice3d.py:121-131) from the squared per-axis offsets; the few
+//     cells with a sub-point near the surface are recounted one warp per
+//     cell (25 lanes x 5, __reduce_add_sync).  A sub-point whose
 //     FP32 squared distance lies within 1e-4 (1 + r^2) of r^2 is re-tested
 //     with the reference's exact FP64 expression (|s32 - s64| < 2e-5 (1 + r^2)
 //     for these offsets), so counts are bit-exact.
@@ -106,7 +107,8 @@ constexpr int MAP_CHUNK = 2048;
 
 __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32; w = global cell index
-    __shared__ int s_n;
+    __shared__ int s_amb[MAP_CHUNK];      // partial cells needing the exact recount (index into s_off)
+    __shared__ int s_n, s_na;
     const int g = blockIdx.x;
     double xc, yc, zc, r;
     particle_lattice(a, g, xc, yc, zc, r);
@@ -127,8 +129,6 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     const float band = (float)(1e-4 * (1.0 + rr));
     const float lo = (float)rr - band, hi = (float)rr + band;
     const unsigned tot = (unsigned)ex * (unsigned)ey * (unsigned)ez;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int ii = lane / 5, jj = lane % 5;
     // this thread's first cell, then advance by blockDim cells with carries
     const unsigned bd = blockDim.x;
     const int adx = (int)(bd % (unsigned)ex), ady = (int)((bd / (unsigned)ex) % (unsigned)ey);
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     int ix = (int)(threadIdx.x % (unsigned)ex), jy = (int)((threadIdx.x / (unsigned)ex) % (unsigned)ey);
     int kz = (int)(threadIdx.x / ((unsigned)ex * (unsigned)ey));
     for (unsigned base = 0; base < tot; base += MAP_CHUNK) {
-        if (threadIdx.x == 0) s_n = 0;
+        if (threadIdx.x == 0) s_n = s_na = 0;
         __syncthreads();
         const unsigned lim = min(tot, base + MAP_CHUNK);
         for (unsigned t = base + threadIdx.x; t < lim; t += bd) {
@@ -169,39 +169,66 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
         }
         __syncthreads();
         const int n = s_n;
-        const float oxl = 0.4f - 0.2f * (float)ii, oyl = 0.4f - 0.2f * (float)jj;
-        for (int e = warp; e < n; e += nwarp) {
+        // 2a. one thread per partial cell: 25 columns x 5 sub-points from the
+        // squared per-axis offsets (-fmad=false: each product and sum rounded
+        // as in the per-point expression).  Cells with a sub-point inside the
+        // rounding band go to a second list for an exact warp recount.
+        for (int e = threadIdx.x; e < n; e += bd) {
             const float4 o = s_off[e];
-            int cnt = 0, amb = 0;
-            if (lane < 25) {
-                const float ox = o.x + oxl, oy = o.y + oyl;
-                const float sxy = ox * ox + oy * oy;
+            float ox2[5], oy2[5], oz2[5];
 #pragma unroll
-                for (int kk = 0; kk < 5; ++kk) {
-                    const float oz = o.z + (0.4f - 0.2f * (float)kk);
-                    const float s = sxy + oz * oz;
-                    cnt += s < lo;
-                    amb |= (s >= lo) & (s <= hi);
-                }
+            for (int m = 0; m < 5; ++m) {
+                const float sh = 0.4f - 0.2f * (float)m;
+                const float ox = o.x + sh, oy = o.y + sh, oz = o.z + sh;
+                ox2[m] = ox * ox;
+                oy2[m] = oy * oy;
+                oz2[m] = oz * oz;
             }
+            int cnt = 0, amb = 0;
+#pragma unroll
+            for (int ia = 0; ia < 5; ++ia)
+#pragma unroll
+                for (int ja = 0; ja < 5; ++ja) {
+                    const float sxy = ox2[ia] + oy2[ja];
+#pragma unroll
+                    for (int kk = 0; kk < 5; ++kk) {
+                        const float sd = sxy + oz2[kk];
+                        cnt += sd < lo;
+                        amb |= (sd >= lo) & (sd <= hi);
+                    }
+                }
+            if (amb) {
+                s_amb[atomicAdd(&s_na, 1)] = e;
+            } else if (cnt > 0) {   // eps = 0 never beats the empty cell (strict >)
+                atomicMax(a.key + __float_as_uint(o.w), ((uint32_t)cnt << 24) | gbits);
+            }
+        }
+        __syncthreads();
+        // 2b. cells with near-surface sub-points: one warp per cell, lane
+        // (ii, jj) < 25 tests its column of five; points inside the band are
+        // re-tested with the reference's exact FP64 expression
+        const int na = s_na;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+        const int ii = lane / 5, jj = lane % 5;
+        const float oxl = 0.4f - 0.2f * (float)ii, oyl = 0.4f - 0.2f * (float)jj;
+        for (int e2 = warp; e2 < na; e2 += nwarp) {
+            const float4 o = s_off[s_amb[e2]];
             const unsigned c = __float_as_uint(o.w);
-            if (__any_sync(0xffffffffu, amb)) {
-                // rare: re-test the sub-points near the surface exactly (FP64)
+            int cnt = 0;
+            if (lane < 25) {
                 const int i = (int)(c % (unsigned)a.nx), j = (int)((c / (unsigned)a.nx) % (unsigned)a.ny);
                 const int k = (int)(c / ((unsigned)a.nx * (unsigned)a.ny));
-                if (amb) {
-                    const float ox = o.x + oxl, oy = o.y + oyl;
-                    const float sxy = ox * ox + oy * oy;
-                    for (int kk = 0; kk < 5; ++kk) {
-                        const float oz = o.z + (0.4f - 0.2f * (float)kk);
-                        const float s = sxy + oz * oz;
-                        if (s >= lo && s <= hi) cnt += subcell_inside_exact(xc, yc, zc, i, j, k, ii, jj, kk, r);
-                    }
+                const float ox = o.x + oxl, oy = o.y + oyl;
+                const float sxy = ox * ox + oy * oy;
+                for (int kk = 0; kk < 5; ++kk) {
+                    const float oz = o.z + (0.4f - 0.2f * (float)kk);
+                    const float sd = sxy + oz * oz;
+                    if (sd < lo) ++cnt;
+                    else if (sd <= hi) cnt += subcell_inside_exact(xc, yc, zc, i, j, k, ii, jj, kk, r);
                 }
             }
             cnt = __reduce_add_sync(0xffffffffu, cnt);
-            if (lane == 0 && cnt > 0)   // eps = 0 never beats the empty cell (strict >)
-                atomicMax(a.key + c, ((uint32_t)cnt << 24) | gbits);
+            if (lane == 0 && cnt > 0) atomicMax(a.key + c, ((uint32_t)cnt << 24) | gbits);
         }
         __syncthreads();
     }
