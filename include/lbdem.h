@@ -116,6 +116,10 @@ typedef struct lbdem_lattice {
     const uint32_t *links; /* per-cell link mask from lbdem_build_links */
     const uint8_t *row_simple; /* per (y,z) row: 1 = row and its 8 neighbour rows all plain FLUID */
     int32_t *status;       /* device status word */
+    const uint32_t *moving; /* per-cell bit q: neighbour x - c_q is a moving wall (VEL_LADD), from
+                               lbdem_build_links; NULL when the lattice has no moving walls.  The
+                               wall velocity is read from vel at the wall cell, the lagged density
+                               of the cell from rho (the step keeps it current for these cells). */
 } lbdem_lattice;
 
 typedef struct lbdem_grains {
@@ -181,7 +185,7 @@ int lbdem_abi_version(void);
 const char *lbdem_last_error(void);
 
 int lbdem_build_links(const int32_t *ct, int32_t nx, int32_t ny, int32_t nz, int32_t skip_inlet,
-                      uint32_t *links, uint8_t *row_simple, void *stream);
+                      uint32_t *links, uint8_t *row_simple, uint32_t *moving, void *stream);
 
 int lbdem_lattice_init(const lbdem_lattice *L, int32_t buf, void *stream);
 

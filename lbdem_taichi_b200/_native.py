@@ -40,7 +40,7 @@ class Lattice(C.Structure):
                 ("omega0", C.c_float), ("smag_cs", C.c_float), ("smag_mode", C.c_int32),
                 ("force_on", C.c_int32), ("force", C.c_float * 3), ("scale16", C.c_float),
                 ("f", vp * 2), ("rho", vp), ("vel", vp), ("aux", vp), ("links", vp), ("row_simple", vp),
-                ("status", vp)]
+                ("status", vp), ("moving", vp)]
 
 
 class Grains(C.Structure):
@@ -76,7 +76,7 @@ class Dem(C.Structure):
 EXPORTS = {
     "lbdem_abi_version": ([], C.c_int),
     "lbdem_last_error": ([], C.c_char_p),
-    "lbdem_build_links": ([vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
+    "lbdem_build_links": ([vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp], C.c_int),
     "lbdem_lattice_init": ([vp, C.c_int32, vp], C.c_int),
     "lbdem_psc_map": ([vp, vp, vp, vp], C.c_int),
     "lbdem_psc_step_f32": ([vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp], C.c_int),

@@ -54,6 +54,9 @@ struct StepArgs {
     void *aux;
     const uint32_t *links;
     const uint8_t *row_simple;
+    const uint32_t *moving;    // moving-wall link bits per cell (VEL_LADD neighbours), or NULL
+    float *rho;                // lagged density of moving-wall-adjacent cells (read, then rewritten)
+    const float *vel;          // wall velocity of VEL_LADD cells (SoA planes)
     const uint32_t *key;
     const float *eps;          // smooth solid fraction per cell, or NULL (exact count in the key)
     const float4 *table;
@@ -121,6 +124,7 @@ __device__ __forceinline__ V cdot(int q, V x, V y, V z) {
 struct CellForce {
     int gid;                       // owner particle, -1 if none
     float hx, hy, hz, tx, ty, tz;  // hydrodynamic force and torque (lattice units)
+    float rho;                     // density of the collision
 };
 
 // PSC quantities of one cell owned by a particle (psclattice3d.py:144-182;
@@ -251,6 +255,7 @@ __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const b
     for (int i = 0; i < L::N; ++i) {
         cf[i].gid = -1;
         cf[i].hx = cf[i].hy = cf[i].hz = cf[i].tx = cf[i].ty = cf[i].tz = 0.f;
+        cf[i].rho = L::get(rho, i);
     }
     if (!psc) {
         // BGK: h' = (1-om) h + om feq_h + g_h, one opposite pair at a time.
@@ -364,6 +369,27 @@ __device__ __forceinline__ void reduce_forces(const StepArgs &a, CellForce c) {
 #define ONE_MIN_BLOCKS 4
 #endif
 
+// Moving walls (VEL_LADD neighbours, lbm_solver3d.py:222-225): the bounced
+// population gains 2 w_q rho (c_q . u_wall)/cs^2, rho being the cell's density
+// of the previous collision (kept in rho[] for these cells) and u_wall the
+// velocity stored at the wall cell; in h units that is 6 S rho (c_q . u_wall).
+__device__ __noinline__ void moving_wall_terms(const StepArgs &a, uint32_t cell, int x, int y, int z, float h[Q]) {
+    const uint32_t mv = a.moving[cell];
+    const float k = 6.f * a.S * a.rho[cell];
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+#pragma unroll
+    for (int q = 1; q < Q; ++q) {
+        if (!(mv & LINK_BB(q))) continue;
+        int xn = x - cx(q), yn = y - cy(q), zn = z - cz(q);
+        xn = xn < 0 ? nx - 1 : (xn >= nx ? 0 : xn);
+        yn = yn < 0 ? ny - 1 : (yn >= ny ? 0 : yn);
+        zn = zn < 0 ? nz - 1 : (zn >= nz ? 0 : zn);
+        const size_t n = ((size_t)zn * ny + yn) * nx + xn;
+        const float cu = cx(q) * a.vel[n] + cy(q) * a.vel[a.nc + n] + cz(q) * a.vel[2 * a.nc + n];
+        h[q] += k * cu;
+    }
+}
+
 template <typename T, bool GATHER, int SMAG>
 __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -426,6 +452,7 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     float h[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(raw[q]);
+    if (GATHER && (lk & LINK_MOVING)) moving_wall_terms(a, cell, x, y, z, h);
     const bool psc = a.key != nullptr && __any_sync(0xffffffffu, key != 0u);
     CellForce cf[1];
     const bool acts[1] = {act};
@@ -436,6 +463,7 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     collide<float, SMAG>(
         a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { h[q] = v; },
         [&](int k, float v) { aux[k] = v; });
+    if (act && (lk & LINK_MOVING)) a.rho[cell] = cf[0].rho;   // lagged density of the next stream
     if (act) {
         T *d = static_cast<T *>(a.dst) + own;
 #pragma unroll
@@ -482,6 +510,16 @@ __global__ void __launch_bounds__(256) k_stream_moments(const StepArgs a, float 
         T v;
         if (q != 0 && (lk & LINK_BB(q))) {
             v = src[own + qinv(q) * 32];
+            if ((lk & LINK_MOVING) && (a.moving[cell] & LINK_BB(q))) {
+                // moving wall (lbm_solver3d.py:222-225), lagged density of the cell
+                const int xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : x);
+                const int ys = cy(q) == 1 ? ym : (cy(q) == -1 ? yp : y);
+                const int zs = cz(q) == 1 ? zm : (cz(q) == -1 ? zp : z);
+                const size_t n = ((size_t)zs * ny + ys) * nx + xs;
+                const float cu = cx(q) * vel_out[n] + cy(q) * vel_out[nc + n] + cz(q) * vel_out[2 * nc + n];
+                const float d = Store<T>::dec(v, wq(q) * a.dec) + 6.f * wq(q) * rho_out[cell] * cu;
+                v = Store<T>::enc(d, a.enc / wq(q));
+            }
         } else {
             const int xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : x);
             const int ys = cy(q) == 1 ? ym : (cy(q) == -1 ? yp : y);
@@ -536,14 +574,16 @@ __global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_i
     }
 }
 
-// link masks from CellType (lbm_solver3d.py:203-236)
-__global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inlet, uint32_t *links) {
+// link masks from CellType (lbm_solver3d.py:203-236): bounce-back bit q when
+// the neighbour x - c_q is OBSTACLE or a moving wall (VEL_LADD); for the
+// latter also bit q of moving[] and LINK_MOVING
+__global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inlet, uint32_t *links, uint32_t *moving) {
     const size_t nc = (size_t)nx * ny * nz;
     const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (c >= nc) return;
     const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
     const int32_t own = ct[c];
-    uint32_t L = 0;
+    uint32_t L = 0, M = 0;
     if (own & (LBDEM_CT_OBSTACLE | LBDEM_CT_VEL_LADD | LBDEM_CT_FREE_SLIP | LBDEM_CT_VEL_INLET_LADD)) L |= LINK_SKIP;
     int32_t mskip = LBDEM_CT_OBSTACLE | LBDEM_CT_VEL_LADD | LBDEM_CT_FREE_SLIP;
     if (skip_inlet) mskip |= LBDEM_CT_VEL_INLET_LADD;
@@ -557,9 +597,16 @@ __global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inle
         yn = yn >= ny ? 0 : (yn < 0 ? ny - 1 : yn);
         zn = zn >= nz ? 0 : (zn < 0 ? nz - 1 : zn);
         const int32_t ctn = ct[((size_t)zn * ny + yn) * nx + xn];
-        if (!(ctn & prop) && (ctn & LBDEM_CT_OBSTACLE)) L |= LINK_BB(q);
+        if (ctn & prop) continue;
+        if (ctn & LBDEM_CT_OBSTACLE) {
+            L |= LINK_BB(q);
+        } else if (ctn & LBDEM_CT_VEL_LADD) {
+            L |= LINK_BB(q) | LINK_MOVING;
+            M |= LINK_BB(q);
+        }
     }
     links[c] = L;
+    if (moving) moving[c] = M;
 }
 
 // row flag: every cell of the (y,z) row is an updated FLUID cell without
@@ -695,6 +742,9 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
     a.aux = L->aux;
     a.links = L->links;
     a.row_simple = L->row_simple;
+    a.moving = L->moving;
+    a.rho = L->rho;
+    a.vel = L->vel;
     a.status = L->status;
     if (!a.links || !a.row_simple || !a.status) {
         set_error("links, row_simple and status are required");
@@ -702,6 +752,10 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
     }
     if (L->smag_mode == LBDEM_SMAG_REFERENCE && !L->aux) {
         set_error("LBDEM_SMAG_REFERENCE needs the aux buffer");
+        return LBDEM_ERR_ARG;
+    }
+    if (L->moving && (!L->rho || !L->vel)) {
+        set_error("moving walls need the rho and vel fields");
         return LBDEM_ERR_ARG;
     }
     return LBDEM_OK;
@@ -893,14 +947,14 @@ int lbdem_abi_version(void) { return LBDEM_ABI_VERSION; }
 const char *lbdem_last_error(void) { return g_err; }
 
 int lbdem_build_links(const int32_t *ct, int32_t nx, int32_t ny, int32_t nz, int32_t skip_inlet, uint32_t *links,
-                      uint8_t *row_simple, void *stream) {
+                      uint8_t *row_simple, uint32_t *moving, void *stream) {
     if (!ct || !links || !row_simple || nx <= 0 || ny <= 0 || nz <= 0) {
         set_error("build_links: bad arguments");
         return LBDEM_ERR_ARG;
     }
     cudaStream_t st = (cudaStream_t)stream;
     const size_t nc = (size_t)nx * ny * nz;
-    k_links<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(ct, nx, ny, nz, skip_inlet, links);
+    k_links<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(ct, nx, ny, nz, skip_inlet, links, moving);
     const int nrows = ny * nz;
     k_rows<<<(nrows + 7) / 8, 256, 0, st>>>(links, nx, nrows, row_simple);
     return check_launch("build_links");

@@ -48,6 +48,9 @@ class FrozenBedDrag:
             raise ValueError("the adjoint covers FP32 storage with Smagorinsky off")
         if lat.dem.n == 0:
             raise ValueError("no particles")
+        lat._sync_inputs()
+        if lat.has_moving_walls:
+            raise ValueError("the adjoint covers fixed walls (OBSTACLE) only, not moving walls (VEL_LADD)")
         if int(n_steps) < 1 or int(checkpoint_every) < 1:
             raise ValueError("n_steps and checkpoint_every must be positive")
         self.lat = lat

@@ -26,7 +26,7 @@ from .lbmutils import CellType, UnitConverter
 _STORAGE = {"f32": (N.F32, torch.float32, 1.0), "f16": (N.F16, torch.float16, 4096.0),
             "bf16": (N.BF16, torch.bfloat16, 1.0)}
 _SMAG = {"off": N.SMAG_OFF, "reference": N.SMAG_REFERENCE, "local": N.SMAG_LOCAL}
-_UNSUPPORTED = (CellType.FREE_SLIP | CellType.VEL_LADD | CellType.VEL_ZOUHE | CellType.VEL_EXIT
+_UNSUPPORTED = (CellType.FREE_SLIP | CellType.VEL_ZOUHE | CellType.VEL_EXIT
                 | CellType.Pre_ZOUHE | CellType.VEL_INLET_LADD | CellType.INTERFACE | CellType.GAS)
 
 W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
@@ -149,6 +149,8 @@ class LatticeEngine:
         self._aux = (torch.zeros((nblk, 5, 32), dtype=tdtype, device=dev)
                      if smagorinsky == "reference" else None)
         self._links = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self._moving = None
+        self.has_moving_walls = False
         self._rows = torch.zeros(self.Ny * self.Nz, dtype=torch.uint8, device=dev)
         self._ct_dev = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -201,9 +203,17 @@ class LatticeEngine:
         bad = np.bitwise_and(host, _UNSUPPORTED)
         if bad.any():
             raise NotImplementedError(
-                "cell types other than FLUID and OBSTACLE (moving walls, Zou-He, exits, free slip, "
-                "free surface) are not supported by the fused kernel")
+                "cell types other than FLUID, OBSTACLE and VEL_LADD (Zou-He, exits, Ladd inlets, free "
+                "slip, free surface) are not supported by the fused kernel")
         self._ct_dev.copy_(torch.from_numpy(from_ref(host.astype(np.int32)).reshape(-1)))
+        # moving walls: per-cell moving-link bits, allocated on first use
+        if np.bitwise_and(host, CellType.VEL_LADD).any():
+            if self._moving is None:
+                self._moving = torch.zeros(self.ncells, dtype=torch.int32, device="cuda")
+            self._lat.moving = N.ptr(self._moving)
+        else:
+            self._lat.moving = None
+        self.has_moving_walls = self._lat.moving is not None
 
     def _push_rho(self, host):
         self._rho.copy_(torch.from_numpy(from_ref(host).reshape(-1).astype(np.float32)))
@@ -218,7 +228,8 @@ class LatticeEngine:
         self.CT.flush()
         if self._links_dirty:
             N.call("lbdem_build_links", N.ptr(self._ct_dev), self.Nx, self.Ny, self.Nz, int(self.skip_inlet),
-                   N.ptr(self._links), N.ptr(self._rows), N.stream_handle())
+                   N.ptr(self._links), N.ptr(self._rows), N.ptr(self._moving) if self._lat.moving else None,
+                   N.stream_handle())
             self._links_dirty = False
         self.rho.flush()
         self.vel.flush()

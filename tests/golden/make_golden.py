@@ -384,9 +384,46 @@ def scen_coupled():
     save("coupled", omega0=np.float64(1.0 / 0.6), nsteps=np.int64(nsteps), **init, **out)
 
 
+def scen_couette_ladd():
+    """PSCLattice3D between two moving walls (VEL_LADD cells, the modified
+    bounce-back of lbm_solver3d.py:222-225, as in the shear-suspension
+    driver shear_fullyresolved.py:36-45) with one sphere, lattice units."""
+    rng = np.random.default_rng(41)
+    nx, ny, nz = 12, 10, 12
+    U = 0.02
+    pos = np.array([[5.6, 4.7, 5.3]])
+    rad = np.array([2.4])
+    vel = np.array([[0.001, 0.0, 0.0]])
+    omg = np.array([[0.0, 0.002, 0.0]])
+    domain = (0.0, float(nx), 0.0, float(ny), 0.0, float(nz))
+    dem = make_dem(domain, 0.25, (0.0, 0.0, 0.0), HertzContactConfig(0.3, 0.3, 0.9, 0.9),
+                   rad, 2.0, pos, vel, omega=omg, periodic=(True, True, False))
+    lat = PSCLattice3D(nx, ny, nz, 1.0 / 0.7, 1.0, 1.0, 1.0, dem)
+    ct = lat.CT.arr
+    ct[:, :, 0] = CellType.VEL_LADD
+    ct[:, :, -1] = CellType.VEL_LADD
+    random_flow(lat, rng, 0.01, 0.003)
+    lat.vel.arr[:, :, 0, :] = (-U, 0.0, 0.0)
+    lat.vel.arr[:, :, -1, :] = (U, 0.005, 0.0)
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy(),
+                gpos=pos, grad=rad, gvel=vel, gomega=omg, domain=np.array(domain))
+    lat.initialize()
+    out = {}
+    for s in range(3):
+        lat.collide()
+        out[f"force_fluid_{s}"] = dem.gf.force_fluid.to_numpy()
+        out[f"moment_fluid_{s}"] = dem.gf.moment_fluid.to_numpy()
+        lat.stream()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save("couette_ladd", omega0=np.float64(1.0 / 0.7), nsteps=np.int64(3), **init, **out)
+
+
 SCENARIOS = {
     "bgk_smag": scen_bgk_smag, "forced": scen_forced, "psc": scen_psc, "hybrid": scen_hybrid,
     "dem_hertz": scen_dem_hertz, "dem_linear": scen_dem_linear, "coupled": scen_coupled,
+    "couette_ladd": scen_couette_ladd,
 }
 
 if __name__ == "__main__":

@@ -101,6 +101,32 @@ def test_psc_physical_units(api):
     lat.check_status()
 
 
+@pytest.mark.parametrize("read_every_step", [True, False])
+def test_moving_walls_ladd(api, read_every_step):
+    """VEL_LADD walls (lbm_solver3d.py:222-225) around a PSC sphere.  Reading
+    the fields after every step streams through lbdem_stream_moments; reading
+    only at the end streams inside the fused step kernel."""
+    _, PSC, _, _ = api
+    g = load("couette_ladd")
+    nx, ny, nz = g["ct"].shape
+    dem = _golden_grains_dem(g, 0.25, 2.0)
+    lat = PSC(nx, ny, nz, float(g["omega0"]), 1.0, 1.0, 1.0, dem)
+    _setup(lat, g)
+    lat.initialize()
+    fl = g["ct"] == 1
+    n = int(g["nsteps"])
+    for s in range(n):
+        lat.collide()
+        assert relmax(dem.gf.force_fluid.to_numpy(), g[f"force_fluid_{s}"]) < 1e-4
+        assert relmax(dem.gf.moment_fluid.to_numpy(), g[f"moment_fluid_{s}"]) < 1e-4
+        lat.stream()
+        if read_every_step or s == n - 1:
+            assert np.abs(lat.f.to_numpy() - g[f"f_{s}"])[fl].max() < 1e-6
+            assert np.abs(lat.rho.to_numpy() - g[f"rho_{s}"])[fl].max() < 1e-6
+            assert relmax(lat.vel.to_numpy()[fl], g[f"vel_{s}"][fl]) < 2e-5
+    lat.check_status()
+
+
 def test_hybrid_psc_smagorinsky(api):
     _, PSC, _, _ = api
     g = load("hybrid")

@@ -75,6 +75,28 @@ def test_psc_matches_reference():
         assert relmax(lat.vel, g[f"vel_{s}"]) < TOL
 
 
+def test_moving_walls_ladd_match_reference():
+    """VEL_LADD walls (modified bounce-back with the wall velocity,
+    lbm_solver3d.py:222-225) around a PSC sphere."""
+    g = load("couette_ladd")
+    dom = g["domain"]
+    lat = _lattice_from(g, psc=True, dom_min=(dom[0], dom[2], dom[4]))
+    gr = _grains(g)
+    lat.initialize()
+    for s in range(int(g["nsteps"])):
+        lat.grains2lattice(gr)
+        lat.collide()
+        lat.lattice2grains(gr)
+        assert relmax(gr.force_fluid, g[f"force_fluid_{s}"]) < TOL
+        assert relmax(gr.moment_fluid, g[f"moment_fluid_{s}"]) < TOL
+        lat.stream()
+        assert relmax(lat.f, g[f"f_{s}"]) < TOL
+        assert relmax(lat.rho, g[f"rho_{s}"]) < TOL
+        assert relmax(lat.vel, g[f"vel_{s}"]) < TOL
+    # the walls drive a shear: the wall-adjacent fluid moves with them
+    assert g["vel_2"][:, :, -2, 0].mean() > 0 > g["vel_2"][:, :, 1, 0].mean()
+
+
 def test_hybrid_psc_smagorinsky_matches_reference():
     g = load("hybrid")
     dom = g["domain"]
