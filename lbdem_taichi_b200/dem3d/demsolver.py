@@ -274,6 +274,36 @@ class DEMSolver:
         d.sync = N.ptr(self.sync)
         self._binned = False
 
+    # ---------------------------------------------------------------- restart
+    _STATE_EXTRA = ("cf_j", "cf_active", "cfn", "cf_add", "cf_shear", "cf_pos", "cf_force", "wcf_active", "wcf_shear",
+                    "wcf_pos", "wcf_force", "acc_force", "acc_moment")
+
+    def state_dict(self):
+        """Complete particle and contact state (host copies) for a restart; the
+        reference keeps no restart state, only its p4p/p4c frames."""
+        d = {"grain." + k: v.detach().cpu().clone() for k, v in self._t.items()}
+        for k in self._STATE_EXTRA:
+            d["contact." + k] = getattr(self, k).detach().cpu().clone()
+        d["n"] = self.n
+        d["maxc"] = self.maxc
+        return d
+
+    def load_state_dict(self, d):
+        if int(d["n"]) != self.n or int(d["maxc"]) != self.maxc:
+            raise ValueError("restart state is for a different particle count or contact capacity")
+        for k, v in self._t.items():
+            v.copy_(d["grain." + k])
+        for k in self._STATE_EXTRA:
+            getattr(self, k).copy_(d["contact." + k])
+        self.status.zero_()
+        self._binned = False   # the broad-phase lists are rebuilt from the restored positions
+
+    def save_state(self, path):
+        torch.save(self.state_dict(), path)
+
+    def load_state(self, path):
+        self.load_state_dict(torch.load(path, weights_only=True))
+
     def _set_materials(self, density):
         """Material table (demsolver.py:222-290): [0] particles, [1] walls."""
         cfg, d = self.config, self._d

@@ -289,6 +289,46 @@ class LatticeEngine:
         for fld in (self.rho, self.vel, self.f, self.omega):
             fld.invalidate()
 
+    # ------------------------------------------------------------ restart
+    def state_dict(self):
+        """Post-stream populations (storage form, blocked layout), density,
+        velocity and the lagged Smagorinsky state, as host copies, for a
+        restart (the reference saves no populations).  Taken between steps;
+        a pending stream is applied first."""
+        if not self._initialized:
+            raise RuntimeError("initialize() the lattice before taking its state")
+        self._sync_inputs()
+        buf = self._materialize()
+        d = {"shape": (self.Nx, self.Ny, self.Nz), "storage": self.storage, "smagorinsky": self.smagorinsky,
+             "omega0": self.omega0, "f": self._f[buf].detach().cpu().clone(),
+             "rho": self._rho.detach().cpu().clone(), "vel": self._vel.detach().cpu().clone()}
+        if self._aux is not None:
+            d["aux"] = self._aux.detach().cpu().clone()
+        return d
+
+    def load_state_dict(self, d):
+        if tuple(d["shape"]) != (self.Nx, self.Ny, self.Nz) or d["storage"] != self.storage:
+            raise ValueError("restart state is for another lattice size or storage form")
+        if d["smagorinsky"] != self.smagorinsky:
+            raise ValueError("restart state was taken with another Smagorinsky mode")
+        self._sync_inputs()
+        self._f[0].copy_(d["f"])
+        self._rho.copy_(d["rho"])
+        self._vel.copy_(d["vel"])
+        if self._aux is not None:
+            self._aux.copy_(d["aux"])
+        self.rho.invalidate()
+        self.vel.invalidate()
+        self._cur, self._cur_kind, self._collided = 0, "f", None
+        self._initialized = True
+        self._invalidate_views()
+
+    def save_state(self, path):
+        torch.save(self.state_dict(), path)
+
+    def load_state(self, path):
+        self.load_state_dict(torch.load(path, weights_only=True))
+
     # ------------------------------------------------------------ kernels
     def initialize(self):
         """f = feq(rho, vel) on updated cells (lbm_solver3d.py:157-171)."""

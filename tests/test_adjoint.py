@@ -128,4 +128,4 @@ def test_drag_loss_autograd_function():
     np.testing.assert_allclose(F.grad.numpy(), 3.0 * gF, rtol=1e-12)
     np.testing.assert_allclose(P.grad.numpy(), 3.0 * gP, rtol=1e-12, atol=1e-18)
     Lo = frozen_bed_drag((nx, ny, nz), OMEGA, _channel(nx, ny, nz), rad, pos, F0, 15)
-    assert abs(float(loss) - Lo) <= 2e-5 * abs(Lo)
+    assert abs(loss.item() - Lo) <= 2e-5 * abs(Lo)
