@@ -112,7 +112,9 @@ typedef struct lbdem_lattice {
     void *f[2];            /* population buffers, 19*32*NB*Ny*Nz elements of the storage type (blocked) */
     float *rho;            /* Ncells, FP32 (moments; also the initial state) */
     float *vel;            /* 3*Ncells, FP32 SoA (ux | uy | uz) */
-    void *aux;             /* LBDEM_SMAG_REFERENCE: 5*32*NB*Ny*Nz of the storage type (blocked), else NULL */
+    void *aux;             /* lagged state (drho, u, omega) of the last collision, 5*32*NB*Ny*Nz of the
+                              storage type (blocked): required by LBDEM_SMAG_REFERENCE and by
+                              lbdem_stress, NULL otherwise (then the step neither reads nor writes it) */
     const uint32_t *links; /* per-cell link mask from lbdem_build_links */
     const uint8_t *row_simple; /* per (y,z) row: 1 = row and its 8 neighbour rows all plain FLUID */
     int32_t *status;       /* device status word */
@@ -207,6 +209,11 @@ int lbdem_psc_step_bf16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_
 /* Stream the post-collision populations of f[src] into f[dst] and write
  * rho/vel of FLUID cells (the reference's stream(), no collision). */
 int lbdem_stream_moments(const lbdem_lattice *L, int32_t src, int32_t dst, void *stream);
+
+/* Stress diagnostics (BasicLattice3D.compute_stress, src/lbm3d/lbm_solver3d.py:347-404)
+ * of the post-stream populations in f[buf] against the lagged state in aux:
+ * out = 7 FP32 planes of Ncells (xx, yy, zz, xy, xz, yz, shear magnitude). */
+int lbdem_stress(const lbdem_lattice *L, int32_t buf, float *out, void *stream);
 
 /* Expand the owner keys into the reference's per-cell PSC fields. */
 int lbdem_psc_decode(const lbdem_lattice *L, const lbdem_psc *P, int32_t *id, float *volfrac,

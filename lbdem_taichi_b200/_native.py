@@ -90,6 +90,7 @@ EXPORTS = {
     "lbdem_global_sums_f64_noalloc": ([vp, C.c_int32, vp, vp], C.c_int),
     "lbdem_psc_map_smooth": ([vp, vp, vp, vp, vp], C.c_int),
     "lbdem_dem_launches_last": ([], C.c_int),
+    "lbdem_stress": ([vp, C.c_int32, vp, vp], C.c_int),
     "lbdem_psc_step_adjoint_f32": ([vp, vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp], C.c_int),
     "lbdem_psc_force_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
 }
@@ -101,7 +102,7 @@ KERNELS_PER_CALL = {"lbdem_build_links": 2, "lbdem_lattice_init": 1, "lbdem_psc_
                     "lbdem_psc_step_f32": 1, "lbdem_psc_step_f16": 1, "lbdem_psc_step_bf16": 1,
                     "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
                     "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2,
-                    "lbdem_psc_map_smooth": 3, "lbdem_psc_step_adjoint_f32": 1, "lbdem_psc_force_adjoint": 1}
+                    "lbdem_psc_map_smooth": 3, "lbdem_stress": 1, "lbdem_psc_step_adjoint_f32": 1, "lbdem_psc_force_adjoint": 1}
 _launches = [0]
 
 

@@ -67,6 +67,7 @@ struct StepArgs {
     uint32_t nb;               // x-blocks per row, ceil(Nx / 32)
     uint32_t rs;               // population elements per row, nb * 19 * 32
     uint32_t ars;              // auxiliary elements per row, nb * 5 * 32
+    int keep_lag;              // aux present: keep (drho, u, omega) of every collision (stress diagnostics)
 };
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
@@ -248,6 +249,15 @@ __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const b
         }
     }
 
+    if (SMAG != LBDEM_SMAG_REFERENCE && a.keep_lag) {
+        // lagged state for the stress diagnostics: this collision's moments and omega
+        const V third = L::splat(1.f / 3.f);
+        aux_out(0, drho);
+        aux_out(1, u3x * third);
+        aux_out(2, u3y * third);
+        aux_out(3, u3z * third);
+        aux_out(4, om);
+    }
     const V S = L::splat(a.S);
     const V SR = S * rho;
     const V rg3x = rho * L::splat(a.g3x), rg3y = rho * L::splat(a.g3y), rg3z = rho * L::splat(a.g3z);
@@ -468,7 +478,7 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
         T *d = static_cast<T *>(a.dst) + own;
 #pragma unroll
         for (int q = 0; q < Q; ++q) d[q * 32] = Store<T>::narrow(h[q]);
-        if (SMAG == LBDEM_SMAG_REFERENCE) {
+        if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
             T *ap = static_cast<T *>(a.aux) + aown;
 #pragma unroll
             for (int k = 0; k < 5; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
@@ -696,6 +706,50 @@ __global__ void k_sums_final(const double *partials, int nblocks, double *out) {
     }
 }
 
+// Stress diagnostics (compute_stress, lbm_solver3d.py:347-404) from the
+// post-stream populations and the lagged state of the last collision:
+// sigma = -(1 - omega/2) (sum c c (f - w) - (drho cs^2 delta + rho u u)),
+// out: 7 planes of Ncells (xx, yy, zz, xy, xz, yz, von Mises shear
+// magnitude); skipped cells are not written.
+template <typename T>
+__global__ void __launch_bounds__(256) k_stress(const StepArgs a, float *out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const uint32_t row = (uint32_t)(z * a.ny + y);
+    const uint32_t cell = row * (uint32_t)a.nx + (uint32_t)x;
+    uint32_t lk = LINK_FLUID;
+    if (!a.row_simple[row]) lk = a.links[cell];
+    if (lk & LINK_SKIP) return;
+    const T *p = static_cast<const T *>(a.src) + (row * a.rs + xslot((uint32_t)x, QB));
+    float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
+#pragma unroll
+    for (int q = 1; q < Q; ++q) {
+        const float d = Store<T>::dec(p[q * 32], wq(q) * a.dec);
+        if (cx(q)) sxx += d;
+        if (cy(q)) syy += d;
+        if (cz(q)) szz += d;
+        if (cx(q) * cy(q)) sxy += (float)(cx(q) * cy(q)) * d;
+        if (cx(q) * cz(q)) sxz += (float)(cx(q) * cz(q)) * d;
+        if (cy(q) * cz(q)) syz += (float)(cy(q) * cz(q)) * d;
+    }
+    const T *ap = static_cast<const T *>(a.aux) + (row * a.ars + xslot((uint32_t)x, AB));
+    const float dr = aux_dec<T>(ap[0]), ux = aux_dec<T>(ap[32]), uy = aux_dec<T>(ap[64]), uz = aux_dec<T>(ap[96]);
+    const float om = aux_dec<T>(ap[128]);
+    const float rho = 1.f + dr, ecs = dr * CS2;
+    const float k = -(1.f - 0.5f * om);
+    const size_t nc = a.nc;
+    const float txy = k * (sxy - rho * ux * uy), txz = k * (sxz - rho * ux * uz), tyz = k * (syz - rho * uy * uz);
+    out[cell] = k * (sxx - (ecs + rho * ux * ux));
+    out[nc + cell] = k * (syy - (ecs + rho * uy * uy));
+    out[2 * nc + cell] = k * (szz - (ecs + rho * uz * uz));
+    out[3 * nc + cell] = txy;
+    out[4 * nc + cell] = txz;
+    out[5 * nc + cell] = tyz;
+    out[6 * nc + cell] = sqrtf(0.5f * (txy * txy + txz * txz + tyz * tyz));
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -740,6 +794,7 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
         a.g3z = 3.f * S * L->force[2];
     }
     a.aux = L->aux;
+    a.keep_lag = L->aux != nullptr;
     a.links = L->links;
     a.row_simple = L->row_simple;
     a.moving = L->moving;
@@ -841,8 +896,24 @@ static int launch_init(const lbdem_lattice *L, int buf, cudaStream_t st) {
     a.dst = L->f[buf];
     dim3 grid, block;
     step_geometry(L, grid, block);
-    k_init<T><<<grid, block, 0, st>>>(a, L->rho, L->vel, L->smag_mode == LBDEM_SMAG_REFERENCE);
+    k_init<T><<<grid, block, 0, st>>>(a, L->rho, L->vel, L->aux != nullptr);
     return check_launch("lattice_init");
+}
+
+template <typename T>
+static int launch_stress(const lbdem_lattice *L, int buf, float *out, cudaStream_t st) {
+    StepArgs a;
+    int rc = fill_args(L, a);
+    if (rc) return rc;
+    if (buf < 0 || buf > 1 || !out || !L->aux) {
+        set_error("stress: needs the post-stream buffer index, an output array and the lagged state (aux)");
+        return LBDEM_ERR_ARG;
+    }
+    a.src = L->f[buf];
+    dim3 grid, block;
+    step_geometry(L, grid, block);
+    k_stress<T><<<grid, block, 0, st>>>(a, out);
+    return check_launch("stress");
 }
 
 template <typename T>
@@ -999,6 +1070,16 @@ int lbdem_stream_moments(const lbdem_lattice *L, int32_t src, int32_t dst, void 
         case LBDEM_BF16: return launch_stream_moments<__nv_bfloat16>(L, src, dst, st);
     }
     set_error("unknown storage form %d", L->storage);
+    return LBDEM_ERR_ARG;
+}
+
+int lbdem_stress(const lbdem_lattice *L, int32_t buf, float *out, void *stream) {
+    if (!L) return LBDEM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (L->storage == LBDEM_F32) return launch_stress<float>(L, buf, out, st);
+    if (L->storage == LBDEM_F16) return launch_stress<__half>(L, buf, out, st);
+    if (L->storage == LBDEM_BF16) return launch_stress<__nv_bfloat16>(L, buf, out, st);
+    set_error("stress: unknown storage");
     return LBDEM_ERR_ARG;
 }
 

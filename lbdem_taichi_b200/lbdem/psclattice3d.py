@@ -15,6 +15,8 @@ reference PSC lattice exactly):
   body_force   lattice-unit body force added as in ForcedLattice3D (default none)
   storage      "f32" | "f16" | "bf16" population storage (FP32 arithmetic)
   keep_hydroforce  also store the per-cell hydrodynamic force field
+  stress       keep the lagged state that compute_stress() needs (the reference's
+               stress diagnostics, lbm_solver3d.py:347-456)
   solid_fraction   "exact" (the reference's 5^3 sub-sample count) or "smooth"
                (a C1 ramp of one lattice spacing across the same effective
                surface, differentiable in the particle positions; used by
@@ -36,9 +38,9 @@ from ..lbm3d.lbmutils import CellType
 class PSCLattice3D(LatticeEngine):
     def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, demslover: DEMSolver, *, smagorinsky="off",
                  body_force=None, storage="f32", keep_hydroforce=False, skip_inlet=False,
-                 solid_fraction="exact"):
+                 solid_fraction="exact", stress=False):
         super().__init__(Nx, Ny, Nz, omega, dx, dt, rho, smagorinsky=smagorinsky, body_force=body_force,
-                         storage=storage, skip_inlet=skip_inlet)
+                         storage=storage, skip_inlet=skip_inlet, stress=stress)
         if solid_fraction not in ("exact", "smooth"):
             raise ValueError('solid_fraction must be "exact" or "smooth"')
         self.dem = demslover

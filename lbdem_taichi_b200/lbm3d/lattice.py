@@ -30,6 +30,7 @@ _UNSUPPORTED = (CellType.FREE_SLIP | CellType.VEL_ZOUHE | CellType.VEL_EXIT
                 | CellType.Pre_ZOUHE | CellType.VEL_INLET_LADD | CellType.INTERFACE | CellType.GAS)
 
 W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+_STRESS_FIELDS = ("stress_xx", "stress_yy", "stress_zz", "stress_xy", "stress_xz", "stress_yz", "shear_stress_mag")
 C_Q = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
                 [1, 1, 0], [-1, -1, 0], [1, -1, 0], [-1, 1, 0], [1, 0, 1], [-1, 0, -1], [1, 0, -1],
                 [-1, 0, 1], [0, 1, 1], [0, -1, -1], [0, 1, -1], [0, -1, 1]], dtype=np.float64)
@@ -121,7 +122,7 @@ class LatticeEngine:
     SmagorinskyConstant = 0.1
 
     def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, smagorinsky="off", body_force=None,
-                 storage="f32", skip_inlet=True):
+                 storage="f32", skip_inlet=True, stress=False):
         N.require_cuda()
         if storage not in _STORAGE:
             raise ValueError(f"storage must be one of {sorted(_STORAGE)}")
@@ -146,8 +147,11 @@ class LatticeEngine:
         self._f = [torch.zeros((nblk, 19, 32), dtype=tdtype, device=dev) for _ in range(2)]
         self._rho = torch.ones(nc, dtype=torch.float32, device=dev)
         self._vel = torch.zeros((3, nc), dtype=torch.float32, device=dev)
-        self._aux = (torch.zeros((nblk, 5, 32), dtype=tdtype, device=dev)
-                     if smagorinsky == "reference" else None)
+        # lagged state (drho, u, omega) of the last collision: needed by the
+        # reference Smagorinsky form and by the stress diagnostics
+        self.stress_enabled = bool(stress) or smagorinsky == "reference"
+        self._aux = (torch.zeros((nblk, 5, 32), dtype=tdtype, device=dev) if self.stress_enabled else None)
+        self._stress = None
         self._links = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._moving = None
         self.has_moving_walls = False
@@ -171,6 +175,8 @@ class LatticeEngine:
         self.vel = LatticeField(self, "vel", shp + (3,), np.float64, self._pull_vel, self._push_vel)
         self.f = LatticeField(self, "f", shp + (19,), np.float64, self._pull_f)
         self.omega = LatticeField(self, "omega", shp, np.float64, self._pull_omega)
+        for m, name in enumerate(_STRESS_FIELDS):
+            setattr(self, name, LatticeField(self, name, shp, np.float64, lambda m=m: self._pull_stress(m)))
         self._lat = N.Lattice()
         self._fill_desc()
 
@@ -289,6 +295,46 @@ class LatticeEngine:
         for fld in (self.rho, self.vel, self.f, self.omega):
             fld.invalidate()
 
+    # ------------------------------------------------------------ diagnostics
+    def compute_stress(self):
+        """Stress tensor and shear magnitude of the current (post-stream) state
+        (lbm_solver3d.py:347-404): sigma = -(1 - omega/2) sum c c (f - feq),
+        feq and omega of the last collision.  Needs the lagged state: construct
+        the lattice with stress=True (implied by smagorinsky="reference")."""
+        if not self.stress_enabled:
+            raise RuntimeError("construct the lattice with stress=True to keep the state compute_stress needs")
+        self._sync_inputs()
+        buf = self._materialize()
+        if self._stress is None:
+            self._stress = torch.zeros((7, self.ncells), dtype=torch.float32, device="cuda")
+        N.call("lbdem_stress", C.byref(self._lat), buf, N.ptr(self._stress), N.stream_handle())
+        for name in _STRESS_FIELDS:
+            getattr(self, name).invalidate()
+
+    def _pull_stress(self, m):
+        if self._stress is None:
+            return np.zeros((self.Nx, self.Ny, self.Nz))
+        return to_ref(self._stress[m].cpu().numpy().reshape(self.Nz, self.Ny, self.Nx).astype(np.float64))
+
+    def compute_plane_average_stress(self, axis: int, position: int):
+        """Mean (xy, xz, yz) stress over the FLUID cells of the plane normal to
+        `axis` at index `position` (lbm_solver3d.py:406-456); zeros for an
+        empty plane.  Uses the stress of the last compute_stress()."""
+        if self._stress is None:
+            return np.zeros(3)
+        st = self._stress.view(7, self.Nz, self.Ny, self.Nx)
+        ct = self._ct_dev.view(self.Nz, self.Ny, self.Nx)
+        # reference axis 0/1/2 = x/y/z; device arrays are [z][y][x]
+        dim = 2 - int(axis)
+        sel = [slice(None)] * 3
+        sel[dim] = int(position)
+        fl = (ct[tuple(sel)] & CellType.FLUID) != 0
+        n = int(fl.sum().item())
+        if n == 0:
+            return np.zeros(3)
+        out = torch.stack([st[k][tuple(sel)][fl].double().sum() for k in (3, 4, 5)]) / n
+        return out.cpu().numpy()
+
     # ------------------------------------------------------------ restart
     def state_dict(self):
         """Post-stream populations (storage form, blocked layout), density,
@@ -392,9 +438,9 @@ class BasicLattice3D(LatticeEngine):
     """BGK + Smagorinsky lattice (BasicLattice3D.collide, lbm_solver3d.py:176-192:
     computeOmega with the previous step's feq and omega, then BGK)."""
 
-    def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, storage="f32", smagorinsky="reference"):
+    def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, storage="f32", smagorinsky="reference", stress=False):
         super().__init__(Nx, Ny, Nz, omega, dx, dt, rho, smagorinsky=smagorinsky, storage=storage,
-                         skip_inlet=True)
+                         skip_inlet=True, stress=stress)
 
 
 class ForcedLattice3D(LatticeEngine):

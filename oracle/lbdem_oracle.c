@@ -320,6 +320,33 @@ void orc_stream(orc_lat *L) {
     }
 }
 
+/* lbm_solver3d.py:347-404: stress from the non-equilibrium part of the
+ * post-stream populations against the equilibrium stored by the last collide,
+ * sigma = -(1 - omega/2) sum c c (f - feq); out: 7 per cell (xx, yy, zz, xy,
+ * xz, yz, von Mises shear magnitude); skipped cells are left untouched. */
+void orc_compute_stress(const orc_lat *L, double *out) {
+    long nc = (long)L->nx * L->ny * L->nz;
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < nc; c++) {
+        if (L->ct[c] & (CT_OBSTACLE | CT_VEL_LADD | CT_FREE_SLIP | CT_VEL_INLET_LADD)) continue;
+        double relax = 1.0 - 0.5 * L->omega[c];
+        double xx = 0, yy = 0, zz = 0, xy = 0, xz = 0, yz = 0;
+        for (int q = 0; q < Q; q++) {
+            double fneq = L->f[Q * c + q] - L->feq[Q * c + q];
+            xx += CX[q] * CX[q] * fneq;
+            yy += CY[q] * CY[q] * fneq;
+            zz += CZ[q] * CZ[q] * fneq;
+            xy += CX[q] * CY[q] * fneq;
+            xz += CX[q] * CZ[q] * fneq;
+            yz += CY[q] * CZ[q] * fneq;
+        }
+        double *o = out + 7 * c;
+        o[0] = -relax * xx; o[1] = -relax * yy; o[2] = -relax * zz;
+        o[3] = -relax * xy; o[4] = -relax * xz; o[5] = -relax * yz;
+        o[6] = sqrt(0.5 * (o[3] * o[3] + o[4] * o[4] + o[5] * o[5]));
+    }
+}
+
 /* FP64 totals of mass and momentum over FLUID cells (for conservation checks). */
 void orc_global_sums(const orc_lat *L, double *out4) {
     long nc = (long)L->nx * L->ny * L->nz;

@@ -48,6 +48,7 @@ def lib():
         _lib.orc_dem_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         _lib.orc_dem_candidates.restype = C.c_int
         _lib.orc_map_smooth.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.orc_compute_stress.argtypes = [C.c_void_p, C.c_void_p]
         _lib.orc_adjoint_collide.argtypes = [C.c_void_p] + [C.c_void_p] * 5 + [C.c_int]
         _lib.orc_adjoint_stream.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_pos_adjoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -139,6 +140,25 @@ class OracleLattice:
         out = np.zeros(4)
         lib().orc_global_sums(self._bind(), _p(out))
         return out
+
+    def compute_stress(self):
+        """(Nx, Ny, Nz, 7): xx, yy, zz, xy, xz, yz, shear magnitude (lbm_solver3d.py:347-404);
+        zero on skipped cells as the reference's fields."""
+        out = np.zeros(self.shape + (7,))
+        lib().orc_compute_stress(self._bind(), _p(out))
+        self.stress = out
+        return out
+
+    def plane_average_stress(self, axis, position):
+        """lbm_solver3d.py:406-456: mean (xy, xz, yz) stress over the FLUID cells of a plane."""
+        sl = [slice(None)] * 3
+        sl[axis] = position
+        fl = (self.ct[tuple(sl)] & CT_FLUID) != 0
+        st = self.stress[tuple(sl)]
+        n = int(fl.sum())
+        if n == 0:
+            return np.zeros(3)
+        return np.array([st[..., 3][fl].sum() / n, st[..., 4][fl].sum() / n, st[..., 5][fl].sum() / n])
 
     # reverse mode on a frozen bed (smooth solid fraction)
     def map_smooth(self, g: "OracleGrains"):

@@ -417,6 +417,14 @@ def scen_couette_ladd():
         out[f"f_{s}"] = lat.f.to_numpy()
         out[f"rho_{s}"] = lat.rho.to_numpy()
         out[f"vel_{s}"] = lat.vel.to_numpy()
+        # stress diagnostics of the shear driver (lbm_solver3d.py:347-456)
+        lat.compute_stress()
+        for k in ("stress_xx", "stress_yy", "stress_zz", "stress_xy", "stress_xz", "stress_yz",
+                  "shear_stress_mag"):
+            out[f"{k}_{s}"] = getattr(lat, k).to_numpy()
+        out[f"plane_top_{s}"] = np.asarray(lat.compute_plane_average_stress(2, nz - 2), np.float64)
+        out[f"plane_y_{s}"] = np.asarray(lat.compute_plane_average_stress(1, 3), np.float64)
+        out[f"plane_x_{s}"] = np.asarray(lat.compute_plane_average_stress(0, 4), np.float64)
     save("couette_ladd", omega0=np.float64(1.0 / 0.7), nsteps=np.int64(3), **init, **out)
 
 

@@ -110,7 +110,7 @@ def test_moving_walls_ladd(api, read_every_step):
     g = load("couette_ladd")
     nx, ny, nz = g["ct"].shape
     dem = _golden_grains_dem(g, 0.25, 2.0)
-    lat = PSC(nx, ny, nz, float(g["omega0"]), 1.0, 1.0, 1.0, dem)
+    lat = PSC(nx, ny, nz, float(g["omega0"]), 1.0, 1.0, 1.0, dem, stress=True)
     _setup(lat, g)
     lat.initialize()
     fl = g["ct"] == 1
@@ -124,6 +124,13 @@ def test_moving_walls_ladd(api, read_every_step):
             assert np.abs(lat.f.to_numpy() - g[f"f_{s}"])[fl].max() < 1e-6
             assert np.abs(lat.rho.to_numpy() - g[f"rho_{s}"])[fl].max() < 1e-6
             assert relmax(lat.vel.to_numpy()[fl], g[f"vel_{s}"][fl]) < 2e-5
+            # stress diagnostics of the shear driver (lbm_solver3d.py:347-456)
+            lat.compute_stress()
+            for k in ("stress_xx", "stress_yy", "stress_zz", "stress_xy", "stress_xz", "stress_yz",
+                      "shear_stress_mag"):
+                assert np.abs(getattr(lat, k).to_numpy() - g[f"{k}_{s}"])[fl].max() < 2e-7, k
+            for key, (axis, pos) in (("plane_top", (2, nz - 2)), ("plane_y", (1, 3)), ("plane_x", (0, 4))):
+                assert np.abs(lat.compute_plane_average_stress(axis, pos) - g[f"{key}_{s}"]).max() < 2e-7, key
     lat.check_status()
 
 

@@ -93,6 +93,13 @@ def test_moving_walls_ladd_match_reference():
         assert relmax(lat.f, g[f"f_{s}"]) < TOL
         assert relmax(lat.rho, g[f"rho_{s}"]) < TOL
         assert relmax(lat.vel, g[f"vel_{s}"]) < TOL
+        st = lat.compute_stress()
+        for m, k in enumerate(("stress_xx", "stress_yy", "stress_zz", "stress_xy", "stress_xz", "stress_yz",
+                               "shear_stress_mag")):
+            assert relmax(st[..., m], g[f"{k}_{s}"]) < 1e-9, k
+        nz = lat.shape[2]
+        for key, (axis, pos) in (("plane_top", (2, nz - 2)), ("plane_y", (1, 3)), ("plane_x", (0, 4))):
+            assert relmax(lat.plane_average_stress(axis, pos), g[f"{key}_{s}"]) < 1e-9, key
     # the walls drive a shear: the wall-adjacent fluid moves with them
     assert g["vel_2"][:, :, -2, 0].mean() > 0 > g["vel_2"][:, :, 1, 0].mean()
 
