@@ -383,7 +383,7 @@ __device__ __forceinline__ void reduce_forces(const StepArgs &a, CellForce c) {
 // population gains 2 w_q rho (c_q . u_wall)/cs^2, rho being the cell's density
 // of the previous collision (kept in rho[] for these cells) and u_wall the
 // velocity stored at the wall cell; in h units that is 6 S rho (c_q . u_wall).
-__device__ __noinline__ void moving_wall_terms(const StepArgs &a, uint32_t cell, int x, int y, int z, float h[Q]) {
+__device__ __forceinline__ void moving_wall_terms(const StepArgs &a, uint32_t cell, int x, int y, int z, float h[Q]) {
     const uint32_t mv = a.moving[cell];
     const float k = 6.f * a.S * a.rho[cell];
     const int nx = a.nx, ny = a.ny, nz = a.nz;
