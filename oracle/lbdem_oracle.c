@@ -260,8 +260,101 @@ void orc_lattice2grains(orc_lat *L, orc_grains *G) {
     }
 }
 
-/* lbm_solver3d.py:197-240, 276-303, 308-342 (wet-node boundary conditions at
- * :242-250 are not part of this path) */
+/* Face of a boundary cell from its orientation bits, in the reference's
+ * precedence LEFT, RIGHT, BOTTOM, TOP, BACK, FRONT (lbm_solver3d.py:522-527,
+ * 647-658, 686-816, 831-960): axis a (0 x, 1 y, 2 z) and the inward sign s
+ * (+1 for LEFT / BOTTOM / BACK, whose interior neighbour is at +1 along a). */
+static int face_of(int32_t ct, int *a, int *s) {
+    if (ct & CT_LEFT) { *a = 0; *s = 1; }
+    else if (ct & CT_RIGHT) { *a = 0; *s = -1; }
+    else if (ct & CT_BOTTOM) { *a = 1; *s = 1; }
+    else if (ct & CT_TOP) { *a = 1; *s = -1; }
+    else if (ct & CT_BACK) { *a = 2; *s = 1; }
+    else if (ct & CT_FRONT) { *a = 2; *s = -1; }
+    else return 0;
+    return 1;
+}
+
+static inline double cq(int axis, int q) { return axis == 0 ? CX[q] : (axis == 1 ? CY[q] : CZ[q]); }
+
+/* Zou-He non-equilibrium bounce-back, velocity (vel_zouHe,
+ * lbm_solver3d.py:671-821) or pressure (pre_zouHe, :823-960), written once for
+ * the six faces.  With K the populations with c_a = 0 and O those leaving the
+ * domain (c_a = -s):
+ *   velocity: rho = (sum K + 2 sum O) / (1 - s u_a), u = vel (preset);
+ *   pressure: rho preset, u_a = s (1 - (sum K + 2 sum O) / rho) (stored in
+ *             vel[a]); the unknowns use u = u_a e_a only;
+ *   N_b = 1/2 sum_K c_b f - [velocity] rho u_b / 3   (each tangential b);
+ *   unknown q (c_a = s): f_q = f_qbar + rho (c_q . u) / 3        on the axis,
+ *                        f_q = f_qbar + rho (c_q . u) / 6 - c_qb N_b  diagonal. */
+static void zou_he(orc_lat *L, long c, int32_t ct, int pressure) {
+    int a, s;
+    if (!face_of(ct, &a, &s)) return;
+    double *f = L->f + Q * c;
+    double *vel = L->vel + 3 * c;
+    double K = 0.0, O = 0.0;
+    for (int q = 0; q < Q; q++) {
+        double ca = cq(a, q);
+        if (ca == 0.0) K += f[q];
+        else if (ca == -s) O += f[q];
+    }
+    double rho, u[3];
+    if (pressure) {
+        rho = L->rho[c];
+        vel[a] = s * (1.0 - (K + 2.0 * O) / rho);
+        u[0] = u[1] = u[2] = 0.0;
+        u[a] = vel[a];
+    } else {
+        rho = (K + 2.0 * O) / (1.0 - s * vel[a]);
+        L->rho[c] = rho;
+        u[0] = vel[0]; u[1] = vel[1]; u[2] = vel[2];
+    }
+    double N[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < 3; b++) {
+        if (b == a) continue;
+        double t = 0.0;
+        for (int q = 0; q < Q; q++)
+            if (cq(a, q) == 0.0) t += cq(b, q) * f[q];
+        N[b] = 0.5 * t - (pressure ? 0.0 : rho * u[b] / 3.0);
+    }
+    for (int q = 1; q < Q; q++) {
+        if (cq(a, q) != s) continue;
+        double cu = CX[q] * u[0] + CY[q] * u[1] + CZ[q] * u[2];
+        int b = -1;
+        for (int bb = 0; bb < 3; bb++)
+            if (bb != a && cq(bb, q) != 0.0) b = bb;
+        if (b < 0) f[q] = f[QINV[q]] + rho * cu / 3.0;
+        else f[q] = f[QINV[q]] + rho * cu / 6.0 - cq(b, q) * N[b];
+    }
+}
+
+/* Convective exit (bc_vel_exit, lbm_solver3d.py:645-663): velocity of the
+ * interior neighbour, rho = 1, f = feq (compute_feq also stores feq). */
+static void vel_exit(orc_lat *L, long c, int i, int j, int k, int32_t ct) {
+    int a, s;
+    if (!face_of(ct, &a, &s)) return;
+    int n3[3] = {i, j, k};
+    n3[a] += s;
+    long n = cidx(L, n3[0], n3[1], n3[2]);
+    for (int d = 0; d < 3; d++) L->vel[3 * c + d] = L->vel[3 * n + d];
+    L->rho[c] = 1.0;
+    compute_feq(L, c);
+    for (int q = 0; q < Q; q++) L->f[Q * c + q] = L->feq[Q * c + q];
+}
+
+/* Ladd velocity inlet (bc_ladd_inlet, lbm_solver3d.py:516-527): the inlet's
+ * density becomes that of its interior neighbour. */
+static void ladd_inlet(orc_lat *L, long c, int i, int j, int k, int32_t ct) {
+    int a, s;
+    if (!face_of(ct, &a, &s)) return;
+    int n3[3] = {i, j, k};
+    n3[a] += s;
+    L->rho[c] = L->rho[cidx(L, n3[0], n3[1], n3[2])];
+}
+
+/* lbm_solver3d.py:197-250, 276-303, 308-342: pull streaming with the
+ * neighbour rules, moments of FLUID cells, then the wet-node boundary
+ * conditions (:242-250) in a second pass over the lattice. */
 void orc_stream(orc_lat *L) {
     int nx = L->nx, ny = L->ny, nz = L->nz;
     long nc = (long)nx * ny * nz;
@@ -317,6 +410,19 @@ void orc_stream(orc_lat *L) {
             L->vel[3 * c + 1] = u1 / r;
             L->vel[3 * c + 2] = u2 / r;
         }
+    }
+    /* second pass: the reference runs it as a parallel loop; each cell reads
+     * only its own populations and its interior neighbour's moments */
+    for (long c = 0; c < nc; c++) {
+        int32_t ct = L->ct[c];
+        if (!(ct & (CT_VEL_ZOUHE | CT_VEL_EXIT | CT_PRE_ZOUHE | CT_VEL_INLET_LADD))) continue;
+        int i = (int)(c / ((long)ny * nz));
+        int j = (int)((c / nz) % ny);
+        int k = (int)(c % nz);
+        if (ct & CT_VEL_ZOUHE) zou_he(L, c, ct, 0);
+        else if (ct & CT_VEL_EXIT) vel_exit(L, c, i, j, k, ct);
+        else if (ct & CT_PRE_ZOUHE) zou_he(L, c, ct, 1);
+        else ladd_inlet(L, c, i, j, k, ct);
     }
 }
 

@@ -428,10 +428,108 @@ def scen_couette_ladd():
     save("couette_ladd", omega0=np.float64(1.0 / 0.7), nsteps=np.int64(3), **init, **out)
 
 
+def _scen_open(name, axis, low, high, U, seed):
+    """PSCLattice3D with open boundaries on the two faces normal to `axis`:
+    `low` / `high` are (CellType bits, value) -- VEL_INLET_LADD and VEL_ZOUHE
+    take a velocity along the axis, Pre_ZOUHE a density (wet-node and Ladd-inlet
+    rules of lbm_solver3d.py:216-250, 516-527, 671-962); the other axes are
+    periodic; one sphere; lattice units."""
+    rng = np.random.default_rng(seed)
+    shape = [10, 9, 8]
+    shape[axis] = 14
+    nx, ny, nz = shape
+    pos = np.array([[nx / 2 - 0.3, ny / 2 + 0.2, nz / 2 - 0.1]])
+    rad = np.array([2.2])
+    domain = (0.0, float(nx), 0.0, float(ny), 0.0, float(nz))
+    per = [True, True, True]
+    per[axis] = False
+    dem = make_dem(domain, 0.25, (0.0, 0.0, 0.0), HertzContactConfig(0.3, 0.3, 0.9, 0.9),
+                   rad, 2.0, pos, np.zeros((1, 3)), periodic=tuple(per))
+    lat = PSCLattice3D(nx, ny, nz, 1.0 / 0.7, 1.0, 1.0, 1.0, dem)
+    random_flow(lat, rng, 0.005, 0.002)
+    ct = lat.CT.arr
+    for (bits, val), idx in ((low, 0), (high, shape[axis] - 1)):
+        sl = [slice(None)] * 3
+        sl[axis] = idx
+        sl = tuple(sl)
+        ct[sl] = bits
+        if bits & CellType.Pre_ZOUHE:
+            lat.rho.arr[sl] = val
+            lat.vel.arr[sl] = 0.0
+        else:
+            v = np.zeros(3)
+            v[axis] = val
+            lat.vel.arr[sl] = v
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy(),
+                gpos=pos, grad=rad, gvel=np.zeros((1, 3)), gomega=np.zeros((1, 3)), domain=np.array(domain),
+                periodic=np.array(per))
+    lat.initialize()
+    out = {}
+    for s in range(4):
+        lat.collide()
+        out[f"force_fluid_{s}"] = dem.gf.force_fluid.to_numpy()
+        lat.stream()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save(name, omega0=np.float64(1.0 / 0.7), nsteps=np.int64(4), **init, **out)
+
+
+def scen_open_x():
+    """The packed-bed pressure-drop driver's boundaries (pressure_drop_fully.py:106-116):
+    Ladd velocity inlet at x = 0, Zou-He pressure outlet at x = Nx-1."""
+    _scen_open("open_x", 0, (CellType.VEL_INLET_LADD | CellType.LEFT, 0.02),
+               (CellType.Pre_ZOUHE | CellType.RIGHT, 1.0), 0.02, 51)
+
+
+def scen_open_y():
+    """Zou-He velocity inlet at y = 0, Zou-He pressure outlet at y = Ny-1."""
+    _scen_open("open_y", 1, (CellType.VEL_ZOUHE | CellType.BOTTOM, 0.015),
+               (CellType.Pre_ZOUHE | CellType.TOP, 0.998), 0.015, 52)
+
+
+def scen_open_z():
+    """Zou-He pressure at z = 0, Ladd velocity inlet at z = Nz-1 (flow towards -z)."""
+    _scen_open("open_z", 2, (CellType.Pre_ZOUHE | CellType.BACK, 1.001),
+               (CellType.VEL_INLET_LADD | CellType.FRONT, -0.02), -0.02, 53)
+
+
+def scen_open_xr():
+    """Zou-He pressure at x = 0, Zou-He velocity inlet at x = Nx-1 (flow towards -x)."""
+    _scen_open("open_xr", 0, (CellType.Pre_ZOUHE | CellType.LEFT, 1.0),
+               (CellType.VEL_ZOUHE | CellType.RIGHT, -0.018), -0.018, 54)
+
+
+def scen_open_exit_x():
+    """Zou-He velocity inlet at x = 0, convective exit (VEL_EXIT) at x = Nx-1."""
+    _scen_open("open_exit_x", 0, (CellType.VEL_ZOUHE | CellType.LEFT, 0.02),
+               (CellType.VEL_EXIT | CellType.RIGHT, 0.0), 0.02, 55)
+
+
+def scen_open_exit_z():
+    """Convective exit at z = 0, Zou-He velocity inlet at z = Nz-1 (flow towards -z)."""
+    _scen_open("open_exit_z", 2, (CellType.VEL_EXIT | CellType.BACK, 0.0),
+               (CellType.VEL_ZOUHE | CellType.FRONT, -0.02), -0.02, 56)
+
+
+def scen_open_yr():
+    """Zou-He pressure at y = 0, Zou-He velocity at y = Ny-1."""
+    _scen_open("open_yr", 1, (CellType.Pre_ZOUHE | CellType.BOTTOM, 1.002),
+               (CellType.VEL_ZOUHE | CellType.TOP, 0.015), 0.015, 57)
+
+
+def scen_open_zb():
+    """Zou-He velocity at z = 0, Zou-He pressure at z = Nz-1."""
+    _scen_open("open_zb", 2, (CellType.VEL_ZOUHE | CellType.BACK, 0.02),
+               (CellType.Pre_ZOUHE | CellType.FRONT, 1.0), 0.02, 58)
+
+
 SCENARIOS = {
     "bgk_smag": scen_bgk_smag, "forced": scen_forced, "psc": scen_psc, "hybrid": scen_hybrid,
     "dem_hertz": scen_dem_hertz, "dem_linear": scen_dem_linear, "coupled": scen_coupled,
-    "couette_ladd": scen_couette_ladd,
+    "couette_ladd": scen_couette_ladd, "open_x": scen_open_x, "open_y": scen_open_y, "open_z": scen_open_z,
+    "open_xr": scen_open_xr, "open_exit_x": scen_open_exit_x, "open_exit_z": scen_open_exit_z,
+    "open_yr": scen_open_yr, "open_zb": scen_open_zb,
 }
 
 if __name__ == "__main__":
