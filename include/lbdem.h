@@ -44,6 +44,8 @@
  *                             hertz.py:45-153, linear.py:43-152)
  *  lbdem_build_links      <- CellType dispatch in BasicLattice3D.stream
  *                            src/lbm3d/lbm_solver3d.py:203-236
+ *  lbdem_boundary_cells   <- second pass of BasicLattice3D.stream (wet-node cells)
+ *                            src/lbm3d/lbm_solver3d.py:242-250
  *  lbdem_global_sums_f64  <- (no counterpart; FP64 conservation totals)
  *  lbdem_psc_map_smooth,
  *  lbdem_psc_step_adjoint_f32,
@@ -62,7 +64,7 @@
 extern "C" {
 #endif
 
-#define LBDEM_ABI_VERSION 1
+#define LBDEM_ABI_VERSION 2
 
 /* return codes */
 #define LBDEM_OK 0
@@ -99,6 +101,12 @@ extern "C" {
 #define LBDEM_CT_VEL_EXIT 128
 #define LBDEM_CT_PRE_ZOUHE 256
 #define LBDEM_CT_VEL_INLET_LADD 262144
+#define LBDEM_CT_RIGHT 4096    /* face bits of open-boundary cells (x = Nx-1) */
+#define LBDEM_CT_LEFT 8192     /* x = 0 */
+#define LBDEM_CT_TOP 16384     /* y = Ny-1 */
+#define LBDEM_CT_BOTTOM 32768  /* y = 0 */
+#define LBDEM_CT_FRONT 65536   /* z = Nz-1 */
+#define LBDEM_CT_BACK 131072   /* z = 0 */
 
 typedef struct lbdem_lattice {
     int32_t nx, ny, nz;
@@ -121,7 +129,17 @@ typedef struct lbdem_lattice {
     const uint32_t *moving; /* per-cell bit q: neighbour x - c_q is a moving wall (VEL_LADD), from
                                lbdem_build_links; NULL when the lattice has no moving walls.  The
                                wall velocity is read from vel at the wall cell, the lagged density
-                               of the cell from rho (the step keeps it current for these cells). */
+                               of the cell from rho (the step keeps it current for these cells).
+                               Also set for Ladd velocity inlets (VEL_INLET_LADD), whose links
+                               use the inlet's velocity and density. */
+    /* Open boundaries (Zou-He velocity / pressure, convective exits, Ladd
+     * inlets, free-slip neighbours): the cells listed by lbdem_boundary_cells
+     * are streamed and collided by a boundary pass that every step and
+     * stream call runs after its main kernel.  bnd_na + bnd_nb = 0 (and the
+     * pointers NULL) for a lattice without such cells. */
+    const int32_t *ct;          /* CellType per cell (device), required when bnd_na + bnd_nb > 0 */
+    const uint32_t *bnd_cells;  /* bnd_na first-pass cells, then bnd_nb second-pass cells (exits, inlets) */
+    uint32_t bnd_na, bnd_nb;
 } lbdem_lattice;
 
 typedef struct lbdem_grains {
@@ -188,6 +206,16 @@ const char *lbdem_last_error(void);
 
 int lbdem_build_links(const int32_t *ct, int32_t nx, int32_t ny, int32_t nz, int32_t skip_inlet,
                       uint32_t *links, uint8_t *row_simple, uint32_t *moving, void *stream);
+
+/* Deterministic list (lattice order) of the cells that the boundary pass
+ * handles, from the link masks: first-pass cells (Zou-He, free-slip
+ * neighbours), then second-pass cells (exits and Ladd inlets, which read their
+ * interior neighbour's fresh moments).  counts (device, 2 uint32) receives
+ * (n_a, n_b); at most `capacity` indices are written to `cells`, so a caller
+ * reads counts and calls again with a larger array when n_a + n_b exceeds it.
+ * scratch: 2 * Ny * Nz int32 of caller memory. */
+int lbdem_boundary_cells(const uint32_t *links, int32_t nx, int32_t ny, int32_t nz, uint32_t *cells,
+                         uint32_t capacity, uint32_t *counts, int32_t *scratch, void *stream);
 
 int lbdem_lattice_init(const lbdem_lattice *L, int32_t buf, void *stream);
 

@@ -16,6 +16,7 @@ LBDEM_ERR_ARG, LBDEM_ERR_LAUNCH, LBDEM_ERR_UNSUPPORTED = 1, 2, 3
 ST_NAN, ST_RHO, ST_VELMAX = 1, 2, 4
 ST_CONTACT_OVERFLOW, ST_GRID_OVERFLOW, ST_GID_OVERFLOW, ST_CELL_OVERFLOW = 8, 16, 32, 64
 ST_WAIT_TIMEOUT = 128
+ABI_VERSION = 2        # LBDEM_ABI_VERSION of include/lbdem.h
 F32, F16, BF16 = 0, 1, 2
 SMAG_OFF, SMAG_REFERENCE, SMAG_LOCAL = 0, 1, 2
 SUM_BLOCKS = 1184
@@ -40,7 +41,8 @@ class Lattice(C.Structure):
                 ("omega0", C.c_float), ("smag_cs", C.c_float), ("smag_mode", C.c_int32),
                 ("force_on", C.c_int32), ("force", C.c_float * 3), ("scale16", C.c_float),
                 ("f", vp * 2), ("rho", vp), ("vel", vp), ("aux", vp), ("links", vp), ("row_simple", vp),
-                ("status", vp), ("moving", vp)]
+                ("status", vp), ("moving", vp), ("ct", vp), ("bnd_cells", vp), ("bnd_na", C.c_uint32),
+                ("bnd_nb", C.c_uint32)]
 
 
 class Grains(C.Structure):
@@ -93,6 +95,7 @@ EXPORTS = {
     "lbdem_stress": ([vp, C.c_int32, vp, vp], C.c_int),
     "lbdem_psc_step_adjoint_f32": ([vp, vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp], C.c_int),
     "lbdem_psc_force_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
+    "lbdem_boundary_cells": ([vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_uint32, vp, vp, vp], C.c_int),
 }
 
 _lib = None
@@ -102,7 +105,10 @@ KERNELS_PER_CALL = {"lbdem_build_links": 2, "lbdem_lattice_init": 1, "lbdem_psc_
                     "lbdem_psc_step_f32": 1, "lbdem_psc_step_f16": 1, "lbdem_psc_step_bf16": 1,
                     "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
                     "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2,
-                    "lbdem_psc_map_smooth": 3, "lbdem_stress": 1, "lbdem_psc_step_adjoint_f32": 1, "lbdem_psc_force_adjoint": 1}
+                    "lbdem_psc_map_smooth": 3, "lbdem_stress": 1, "lbdem_psc_step_adjoint_f32": 1, "lbdem_psc_force_adjoint": 1,
+                    "lbdem_boundary_cells": 3}
+# calls followed by the boundary pass: one more kernel per non-empty phase
+_BOUNDARY_CALLS = ("lbdem_psc_step_f32", "lbdem_psc_step_f16", "lbdem_psc_step_bf16", "lbdem_stream_moments")
 _launches = [0]
 
 
@@ -130,15 +136,22 @@ def load(path: str = LIB_PATH):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = res
-    if lib.lbdem_abi_version() != 1:
+    if lib.lbdem_abi_version() != ABI_VERSION:
         raise LbdemError("liblbdem.so ABI version mismatch")
     _lib = lib
     return lib
 
 
+def _boundary_phases(arg):
+    L = getattr(arg, "_obj", None)
+    return int(L.bnd_na > 0) + int(L.bnd_nb > 0) if isinstance(L, Lattice) else 0
+
+
 def call(name: str, *args):
     rc = getattr(load(), name)(*args)
     _launches[0] += load().lbdem_dem_launches_last() if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
+    if name in _BOUNDARY_CALLS:
+        _launches[0] += _boundary_phases(args[0])
     if rc != LBDEM_OK:
         msg = load().lbdem_last_error().decode(errors="replace")
         raise LbdemError(f"{name} failed (code {rc}): {msg}")

@@ -262,6 +262,10 @@ extern "C" int lbdem_psc_step_adjoint_f32(const lbdem_lattice *L, const lbdem_ps
         set_error("psc_step_adjoint: the adjoint covers FP32 storage with Smagorinsky off");
         return LBDEM_ERR_UNSUPPORTED;
     }
+    if (L->moving || L->bnd_na + L->bnd_nb > 0) {
+        set_error("psc_step_adjoint: the adjoint covers fixed walls only (no moving walls, inlets or open boundaries)");
+        return LBDEM_ERR_UNSUPPORTED;
+    }
     const size_t nb = ((size_t)L->nx + 31) / 32;
     if (nb * 32 * L->ny * L->nz * Q >= (1ull << 32)) {
         set_error("psc_step_adjoint: lattice too large for 32-bit element offsets");

@@ -26,6 +26,16 @@ __host__ __device__ constexpr int cz(int q) {
          : q == 6 || q == 12 || q == 13 || q == 16 || q == 17 ? -1 : 0;
 }
 __host__ __device__ constexpr int qinv(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
+// specular images of direction q in a wall normal to x / y / z
+// (qsyx / qsyy / qsyz, lbm_solver3d.py:50-57): the direction with that
+// component of c_q negated
+__host__ __device__ constexpr int qmirror(int q, int axis) {
+    for (int p = 0; p < 19; ++p) {
+        const int mx = axis == 0 ? -cx(q) : cx(q), my = axis == 1 ? -cy(q) : cy(q), mz = axis == 2 ? -cz(q) : cz(q);
+        if (cx(p) == mx && cy(p) == my && cz(p) == mz) return p;
+    }
+    return q;
+}
 __host__ __device__ constexpr float wq(int q) {
     return q == 0 ? 1.0f / 3.0f : (q <= 6 ? 1.0f / 18.0f : 1.0f / 36.0f);
 }
@@ -46,6 +56,39 @@ constexpr uint32_t LINK_FLUID = 1u << 20;  // FLUID: moments are recomputed
 constexpr uint32_t LINK_MAP_SKIP = 1u << 21;  // PSC map skips the cell
 constexpr uint32_t LINK_MOVING = 1u << 22;    // some bounce-back neighbour is a moving wall (VEL_LADD)
 __host__ __device__ constexpr uint32_t LINK_BB(int q) { return 1u << q; }  // neighbour x-c_q is OBSTACLE
+// Open boundaries (wet-node conditions of the stream's second pass,
+// lbm_solver3d.py:242-250, and free-slip neighbours): such cells are streamed
+// and collided by the boundary pass after the fused step instead of by it.
+constexpr uint32_t LINK_DEFER = 1u << 23;    // Zou-He / exit / Ladd inlet cell, or a free-slip neighbour
+constexpr uint32_t LINK_PHASE_B = 1u << 24;  // deferred cell that reads its interior neighbour (exit, inlet)
+constexpr uint32_t LINK_KEEP = 1u << 25;     // interior neighbour of an exit or inlet: the step stores rho/u
+constexpr uint32_t LINK_INLET = 1u << 26;    // the cell is a Ladd velocity inlet (VEL_INLET_LADD)
+
+// Face of an open-boundary cell from its orientation bits, in the reference's
+// precedence LEFT, RIGHT, BOTTOM, TOP, BACK, FRONT (lbm_solver3d.py:522-527,
+// 647-658, 686-816, 831-960): axis (0 x, 1 y, 2 z) and inward sign s (+1 when
+// the interior neighbour is at +1 along the axis); false without a face bit.
+__host__ __device__ inline bool face_of(int32_t ct, int &axis, int &s) {
+    if (ct & LBDEM_CT_LEFT) { axis = 0; s = 1; }
+    else if (ct & LBDEM_CT_RIGHT) { axis = 0; s = -1; }
+    else if (ct & LBDEM_CT_BOTTOM) { axis = 1; s = 1; }
+    else if (ct & LBDEM_CT_TOP) { axis = 1; s = -1; }
+    else if (ct & LBDEM_CT_BACK) { axis = 2; s = 1; }
+    else if (ct & LBDEM_CT_FRONT) { axis = 2; s = -1; }
+    else return false;
+    return true;
+}
+
+// Which wet-node rule of the stream's second pass (lbm_solver3d.py:242-250)
+// applies to a cell, in the reference's order.
+enum WetRule { WET_NONE = 0, WET_VEL_ZOUHE, WET_EXIT, WET_PRE_ZOUHE, WET_INLET };
+__host__ __device__ inline int wet_rule(int32_t ct) {
+    if (ct & LBDEM_CT_VEL_ZOUHE) return WET_VEL_ZOUHE;
+    if (ct & LBDEM_CT_VEL_EXIT) return WET_EXIT;
+    if (ct & LBDEM_CT_PRE_ZOUHE) return WET_PRE_ZOUHE;
+    if (ct & LBDEM_CT_VEL_INLET_LADD) return WET_INLET;
+    return WET_NONE;
+}
 
 // Storage forms.  Every form stores the scaled deviation
 // h = (f - w) * S / w (S = 1 for FP32, scale16 for the 16-bit forms): the

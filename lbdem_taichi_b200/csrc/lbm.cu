@@ -54,9 +54,11 @@ struct StepArgs {
     void *aux;
     const uint32_t *links;
     const uint8_t *row_simple;
-    const uint32_t *moving;    // moving-wall link bits per cell (VEL_LADD neighbours), or NULL
-    float *rho;                // lagged density of moving-wall-adjacent cells (read, then rewritten)
-    const float *vel;          // wall velocity of VEL_LADD cells (SoA planes)
+    const uint32_t *moving;    // velocity-link bits per cell (VEL_LADD / VEL_INLET_LADD neighbours), or NULL
+    float *rho;                // lagged density of moving-wall-adjacent cells (read, then rewritten);
+                               // inlet densities; moments of LINK_KEEP cells
+    float *vel;                // wall / inlet velocities (SoA planes); moments of LINK_KEEP cells
+    const int32_t *ct;         // CellType (boundary pass only)
     const uint32_t *key;
     const float *eps;          // smooth solid fraction per cell, or NULL (exact count in the key)
     const float4 *table;
@@ -169,10 +171,15 @@ __device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float
 // previous (drho, ux, uy, uz, omega); the current ones go to aux_out(k, v)
 // (reference Smagorinsky mode).  psc: the warp holds at least one owned cell (warp-
 // uniform), so every cell takes the PSC form, fluid cells with B = 0.
-template <class V, int SMAG, class Out, class AuxOut>
+// macro(rho, 3ux, 3uy, 3uz) receives the moments once they are known.
+// OVR: collide with the density and velocity in ovr[4] = (rho, ux, uy, uz)
+// instead of the moments of h -- the boundary pass, where a wet-node rule set
+// them (the reference always collides with its rho / vel fields).
+template <class V, int SMAG, bool OVR = false, class Out, class AuxOut, class Macro>
 __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const bool act[], const int xs[], int y,
                                         int z, const V aux[5], bool psc, const uint32_t key[], const float eps[],
-                                        CellForce cf[], Out &&out, AuxOut &&aux_out) {
+                                        CellForce cf[], Out &&out, AuxOut &&aux_out, Macro &&macro,
+                                        const float *ovr = nullptr) {
     using L = Lanes<V>;
     // Opposite pairs (q, q+1), q odd: sp = h_q + h_{q+1}, am = h_q - h_{q+1}.
     // Pair p = (q-1)/2 has direction c_q: p0 (1,0,0), p1 (0,1,0), p2 (0,0,1),
@@ -186,14 +193,29 @@ __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const b
     // moments (compute_rho_vel, lbm_solver3d.py:276-303)
     const V W1 = L::splat(a.W1), W2 = L::splat(a.W2);
     const V pxy = sp[3] + sp[4], pxz = sp[5] + sp[6], pyz = sp[7] + sp[8];
-    const V drho = vfma(L::splat(a.W0), h[0], vfma(W1, (sp[0] + sp[1]) + sp[2], W2 * ((pxy + pxz) + pyz)));
-    const V jx = vfma(W1, am[0], W2 * ((am[3] + am[4]) + (am[5] + am[6])));
-    const V jy = vfma(W1, am[1], W2 * ((am[3] - am[4]) + (am[7] + am[8])));
-    const V jz = vfma(W1, am[2], W2 * ((am[5] - am[6]) + (am[7] - am[8])));
+    V drho = vfma(L::splat(a.W0), h[0], vfma(W1, (sp[0] + sp[1]) + sp[2], W2 * ((pxy + pxz) + pyz)));
+    V jx = vfma(W1, am[0], W2 * ((am[3] + am[4]) + (am[5] + am[6])));
+    V jy = vfma(W1, am[1], W2 * ((am[3] - am[4]) + (am[7] + am[8])));
+    V jz = vfma(W1, am[2], W2 * ((am[5] - am[6]) + (am[7] - am[8])));
+    if constexpr (OVR) {
+        // PSC force with the set (rho, u): -B sum_q Os_q c_q = B (2 j - rho (u + u_s)),
+        // i.e. the closed form below with j replaced by 2 j - rho u
+        const V r = L::splat(ovr[0]);
+        jx = vfma(L::splat(2.f), jx, -r * L::splat(ovr[1]));
+        jy = vfma(L::splat(2.f), jy, -r * L::splat(ovr[2]));
+        jz = vfma(L::splat(2.f), jz, -r * L::splat(ovr[3]));
+        drho = r - L::splat(1.f);
+    }
     const V rho = L::splat(1.f) + drho;
     const V irho = L::rcp(rho);
     const V i3 = L::splat(3.f) * irho;
-    const V u3x = jx * i3, u3y = jy * i3, u3z = jz * i3;                         // 3u
+    V u3x, u3y, u3z;                                                               // 3u
+    if constexpr (OVR) {
+        u3x = L::splat(3.f * ovr[1]); u3y = L::splat(3.f * ovr[2]); u3z = L::splat(3.f * ovr[3]);
+    } else {
+        u3x = jx * i3; u3y = jy * i3; u3z = jz * i3;
+    }
+    macro(rho, u3x, u3y, u3z);
     const V nU = vfma(u3x, u3x, vfma(u3y, u3y, u3z * u3z)) * L::splat(-1.f / 3.f);   // -3 u^2
 #pragma unroll
     for (int i = 0; i < L::N; ++i) {
@@ -383,9 +405,11 @@ __device__ __forceinline__ void reduce_forces(const StepArgs &a, CellForce c) {
 // population gains 2 w_q rho (c_q . u_wall)/cs^2, rho being the cell's density
 // of the previous collision (kept in rho[] for these cells) and u_wall the
 // velocity stored at the wall cell; in h units that is 6 S rho (c_q . u_wall).
+// Ladd inlets (VEL_INLET_LADD neighbours, :225-229) use the inlet's density.
 __device__ __forceinline__ void moving_wall_terms(const StepArgs &a, uint32_t cell, int x, int y, int z, float h[Q]) {
     const uint32_t mv = a.moving[cell];
-    const float k = 6.f * a.S * a.rho[cell];
+    const float k = 6.f * a.S;
+    const float rc = a.rho[cell];
     const int nx = a.nx, ny = a.ny, nz = a.nz;
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
@@ -396,7 +420,8 @@ __device__ __forceinline__ void moving_wall_terms(const StepArgs &a, uint32_t ce
         zn = zn < 0 ? nz - 1 : (zn >= nz ? 0 : zn);
         const size_t n = ((size_t)zn * ny + yn) * nx + xn;
         const float cu = cx(q) * a.vel[n] + cy(q) * a.vel[a.nc + n] + cz(q) * a.vel[2 * a.nc + n];
-        h[q] += k * cu;
+        const float r = (a.links[n] & LINK_INLET) ? a.rho[n] : rc;
+        h[q] += k * r * cu;
     }
 }
 
@@ -451,7 +476,7 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     uint32_t key = (a.key != nullptr) ? a.key[cell] : 0u;
     uint32_t lk = LINK_FLUID;
     if (!a.row_simple[row]) lk = a.links[cell];
-    const bool act = inb && !(lk & LINK_SKIP);
+    const bool act = inb && !(lk & (LINK_SKIP | LINK_DEFER));
     if (!act) key = 0u;
     if (GATHER && (lk & 0x7FFFEu)) {
         const T *p = src + own;
@@ -472,7 +497,16 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     // post-collision values overwrite h[] and aux[] and are stored together
     collide<float, SMAG>(
         a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { h[q] = v; },
-        [&](int k, float v) { aux[k] = v; });
+        [&](int k, float v) { aux[k] = v; },
+        [&](float r, float u3x, float u3y, float u3z) {
+            // post-stream moments of an exit's / inlet's interior neighbour, read by the boundary pass
+            if (GATHER && act && (lk & LINK_KEEP) && a.vel != nullptr) {
+                a.rho[cell] = r;
+                a.vel[cell] = u3x * (1.f / 3.f);
+                a.vel[a.nc + cell] = u3y * (1.f / 3.f);
+                a.vel[2 * a.nc + cell] = u3z * (1.f / 3.f);
+            }
+        });
     if (act && (lk & LINK_MOVING)) a.rho[cell] = cf[0].rho;   // lagged density of the next stream
     if (act) {
         T *d = static_cast<T *>(a.dst) + own;
@@ -506,7 +540,7 @@ __global__ void __launch_bounds__(256) k_stream_moments(const StepArgs a, float 
     const uint32_t cell = row * (uint32_t)nx + (uint32_t)x;
     uint32_t lk = LINK_FLUID;
     if (!a.row_simple[row]) lk = a.links[cell];
-    if (lk & LINK_SKIP) return;
+    if (lk & (LINK_SKIP | LINK_DEFER)) return;   // deferred cells: the boundary pass
     const T *src = static_cast<const T *>(a.src);
     T *dst = static_cast<T *>(a.dst);
     const uint32_t rs = a.rs;
@@ -521,13 +555,15 @@ __global__ void __launch_bounds__(256) k_stream_moments(const StepArgs a, float 
         if (q != 0 && (lk & LINK_BB(q))) {
             v = src[own + qinv(q) * 32];
             if ((lk & LINK_MOVING) && (a.moving[cell] & LINK_BB(q))) {
-                // moving wall (lbm_solver3d.py:222-225), lagged density of the cell
+                // velocity link (lbm_solver3d.py:222-229)
                 const int xs = cx(q) == 1 ? xm : (cx(q) == -1 ? xp : x);
                 const int ys = cy(q) == 1 ? ym : (cy(q) == -1 ? yp : y);
                 const int zs = cz(q) == 1 ? zm : (cz(q) == -1 ? zp : z);
                 const size_t n = ((size_t)zs * ny + ys) * nx + xs;
                 const float cu = cx(q) * vel_out[n] + cy(q) * vel_out[nc + n] + cz(q) * vel_out[2 * nc + n];
-                const float d = Store<T>::dec(v, wq(q) * a.dec) + 6.f * wq(q) * rho_out[cell] * cu;
+                // wall: the cell's lagged density; Ladd inlet: the inlet's (:225-229)
+                const float r = (a.links[n] & LINK_INLET) ? rho_out[n] : rho_out[cell];
+                const float d = Store<T>::dec(v, wq(q) * a.dec) + 6.f * wq(q) * r * cu;
                 v = Store<T>::enc(d, a.enc / wq(q));
             }
         } else {
@@ -552,9 +588,273 @@ __global__ void __launch_bounds__(256) k_stream_moments(const StepArgs a, float 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Boundary pass: cells with a wet-node rule (Zou-He velocity / pressure,
+// convective exit, Ladd inlet; lbm_solver3d.py:242-250) or a free-slip
+// neighbour, one thread per listed cell, after the main kernel of a step or
+// stream call.  First-pass cells (Zou-He, free slip) only read the previous
+// post-collision populations; second-pass cells (exits, inlets) read the
+// moments that the main kernel and the first pass stored for their interior
+// neighbours.
+// ---------------------------------------------------------------------------
+enum { BND_GATHER = 0, BND_LOCAL = 1, BND_STREAM = 2 };
+
+__device__ __forceinline__ int comp(int q, int axis) { return axis == 0 ? cx(q) : (axis == 1 ? cy(q) : cz(q)); }
+
+// Post-stream populations of one cell with every neighbour rule of the
+// stream's first pass (lbm_solver3d.py:207-236; periodic wrap :308-342):
+// propagation, bounce-back, moving wall / Ladd inlet, specular free slip.
+template <typename T>
+__device__ __forceinline__ void gather_general(const StepArgs &a, int x, int y, int z, uint32_t cell, float h[Q]) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const size_t nc = a.nc;
+    const T *src = static_cast<const T *>(a.src);
+    const uint32_t rs = a.rs;
+    auto slot = [&](int xx, int yy, int zz) { return (uint32_t)(zz * ny + yy) * rs + xslot((uint32_t)xx, QB); };
+    const uint32_t own = slot(x, y, z);
+    const int32_t prop = LBDEM_CT_FLUID | LBDEM_CT_VEL_ZOUHE | LBDEM_CT_VEL_EXIT | LBDEM_CT_PRE_ZOUHE;
+    h[0] = Store<T>::widen(src[own]);
+#pragma unroll
+    for (int q = 1; q < Q; ++q) {
+        int xn = x - cx(q), yn = y - cy(q), zn = z - cz(q);
+        xn = xn >= nx ? 0 : (xn < 0 ? nx - 1 : xn);
+        yn = yn >= ny ? 0 : (yn < 0 ? ny - 1 : yn);
+        zn = zn >= nz ? 0 : (zn < 0 ? nz - 1 : zn);
+        const size_t n = ((size_t)zn * ny + yn) * nx + xn;
+        const int32_t ctn = a.ct[n];
+        float v;
+        if (ctn & prop) {
+            v = Store<T>::widen(src[slot(xn, yn, zn) + q * 32]);
+        } else if (ctn & LBDEM_CT_OBSTACLE) {
+            v = Store<T>::widen(src[own + qinv(q) * 32]);
+        } else if (ctn & (LBDEM_CT_VEL_LADD | LBDEM_CT_VEL_INLET_LADD)) {
+            const float r = (ctn & LBDEM_CT_VEL_LADD) ? a.rho[cell] : a.rho[n];
+            const float cu = cx(q) * a.vel[n] + cy(q) * a.vel[nc + n] + cz(q) * a.vel[2 * nc + n];
+            v = Store<T>::widen(src[own + qinv(q) * 32]) + 6.f * a.S * r * cu;
+        } else if ((ctn & LBDEM_CT_FREE_SLIP) && (ctn & (LBDEM_CT_LEFT | LBDEM_CT_RIGHT))) {
+            v = Store<T>::widen(src[slot(x, yn, zn) + qmirror(q, 0) * 32]);
+        } else if ((ctn & LBDEM_CT_FREE_SLIP) && (ctn & (LBDEM_CT_BOTTOM | LBDEM_CT_TOP))) {
+            v = Store<T>::widen(src[slot(xn, y, zn) + qmirror(q, 1) * 32]);
+        } else if ((ctn & LBDEM_CT_FREE_SLIP) && (ctn & (LBDEM_CT_BACK | LBDEM_CT_FRONT))) {
+            v = Store<T>::widen(src[slot(xn, yn, z) + qmirror(q, 2) * 32]);
+        } else {
+            v = Store<T>::widen(src[slot(xn, yn, zn) + q * 32]);   // same as the main kernel
+        }
+        h[q] = v;
+    }
+}
+
+// Zou-He non-equilibrium bounce-back (vel_zouHe, lbm_solver3d.py:671-821;
+// pre_zouHe, :823-960) on the h form, written once for the six faces.  With
+// d = f - w = h w / S, K the directions with c_a = 0 and O those leaving the
+// domain (c_a = -s), using sum_K w + 2 sum_O w = 1:
+//   velocity: rho = (1 + sum_K d + 2 sum_O d) / (1 - s u_a), u = stored velocity
+//   pressure: rho stored, u_a = s (rho - 1 - sum_K d - 2 sum_O d) / rho, and the
+//             unknowns use u = u_a e_a only (no tangential term)
+//   N_b = 1/2 sum_K c_b d - [velocity] rho u_b / 3
+//   unknown q (c_a = s): d_q = d_qbar + rho (c_q.u) / 3 (axis), + rho (c_q.u) / 6 - c_qb N_b (diagonal),
+// i.e. h_q = h_qbar + 6 S rho (c_q.u) [- 36 S c_qb N_b].  Returns the (rho, u)
+// the reference's collision then uses; false for a cell without a face bit
+// (the reference leaves it untouched).
+__device__ __forceinline__ bool zou_he(const StepArgs &a, int32_t ct, bool pressure, float h[Q], float &rho,
+                                       float u[3]) {
+    int ax, s;
+    if (!face_of(ct, ax, s)) return false;
+    float Dk = 0.f, Do = 0.f, T[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const float d = h[q] * (wq(q) * a.dec);
+        const int ca = comp(q, ax);
+        if (ca == 0) {
+            Dk += d;
+            T[0] += (float)cx(q) * d;
+            T[1] += (float)cy(q) * d;
+            T[2] += (float)cz(q) * d;
+        } else if (ca == -s) {
+            Do += d;
+        }
+    }
+    float uu[3];
+    if (pressure) {
+        u[ax] = (float)s * ((rho - 1.f) - Dk - 2.f * Do) / rho;
+        uu[0] = uu[1] = uu[2] = 0.f;
+        uu[ax] = u[ax];
+    } else {
+        rho = (1.f + Dk + 2.f * Do) / (1.f - (float)s * u[ax]);
+        uu[0] = u[0]; uu[1] = u[1]; uu[2] = u[2];
+    }
+    float N[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) N[b] = 0.5f * T[b] - (pressure ? 0.f : rho * uu[b] * (1.f / 3.f));
+    const float k6 = 6.f * a.S * rho, k36 = 36.f * a.S;
+#pragma unroll
+    for (int q = 1; q < Q; ++q) {
+        if (comp(q, ax) != s) continue;
+        const float cu = (float)cx(q) * uu[0] + (float)cy(q) * uu[1] + (float)cz(q) * uu[2];
+        float corr = 0.f;
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            if (b != ax && comp(q, b) != 0) corr = (float)comp(q, b) * N[b];
+        h[q] = h[qinv(q)] + k6 * cu - k36 * corr;
+    }
+    return true;
+}
+
+template <typename T, int SMAG, int MODE>
+__global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32_t *__restrict__ cells, uint32_t n) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < n;
+    const uint32_t cell = cells[valid ? t : 0];
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const size_t nc = a.nc;
+    const int x = (int)(cell % (uint32_t)nx), y = (int)((cell / (uint32_t)nx) % (uint32_t)ny);
+    const int z = (int)(cell / ((uint32_t)nx * (uint32_t)ny));
+    const uint32_t row = cell / (uint32_t)nx;
+    const uint32_t own = row * a.rs + xslot((uint32_t)x, QB);
+    const uint32_t aown = row * a.ars + xslot((uint32_t)x, AB);
+    const int32_t ct = a.ct[cell];
+    const uint32_t lk = a.links[cell];
+    const int rule = (lk & LINK_INLET) ? WET_INLET : wet_rule(ct);
+    const T *src = static_cast<const T *>(a.src);
+    T *dst = static_cast<T *>(a.dst);
+    float h[Q];
+    float rho = a.rho[cell];
+    float u[3] = {a.vel[cell], a.vel[nc + cell], a.vel[2 * nc + cell]};
+    float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
+    if (a.aux != nullptr) {
+        const T *ap = static_cast<const T *>(a.aux) + aown;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ap[k * 32]);
+    }
+    // interior neighbour of a face cell (no periodic wrap, lbm_solver3d.py:522-527, 647-658)
+    int ax = 0, s = 0;
+    size_t nbr = cell;
+    if (face_of(ct, ax, s)) {
+        int m[3] = {x, y, z};
+        const int lim[3] = {nx, ny, nz};
+        m[ax] = min(max(m[ax] + s, 0), lim[ax] - 1);
+        nbr = ((size_t)m[2] * ny + m[1]) * nx + m[0];
+    }
+    bool fields = false;   // (rho, u) come from the rule or the stored fields, not the moments
+    bool collide_it = true;
+    if (rule == WET_INLET) {
+        // The inlet's populations f never stream (the first pass skips it) but it
+        // collides, and a free-slip mirror may read its post-collision ones: f
+        // lives in the step's dst slot (gather) or src slot (post-stream input),
+        // the post-collision populations in the other buffer.  Its density
+        // follows the interior neighbour's (bc_ladd_inlet).
+        if (MODE != BND_STREAM) {
+            const T *f0 = MODE == BND_GATHER ? static_cast<const T *>(a.dst) + own : src + own;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(f0[q * 32]);
+        }
+        if (MODE != BND_LOCAL) {
+            rho = a.rho[nbr];
+            if (valid) a.rho[cell] = rho;
+        }
+        fields = true;
+        collide_it = !(lk & LINK_MAP_SKIP);
+    } else if (rule == WET_EXIT && MODE != BND_LOCAL) {
+        // bc_vel_exit: u of the interior neighbour, rho = 1, f = feq (which is also
+        // the equilibrium the next Smagorinsky / stress evaluation lags on)
+        u[0] = a.vel[nbr]; u[1] = a.vel[nc + nbr]; u[2] = a.vel[2 * nc + nbr];
+        rho = 1.f;
+        if (valid) {
+            a.rho[cell] = 1.f;
+            a.vel[cell] = u[0]; a.vel[nc + cell] = u[1]; a.vel[2 * nc + cell] = u[2];
+        }
+        const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float cu = cx(q) * u[0] + cy(q) * u[1] + cz(q) * u[2];
+            h[q] = a.S * (3.f * cu + 4.5f * cu * cu - 1.5f * usq);
+        }
+        aux[0] = 0.f; aux[1] = u[0]; aux[2] = u[1]; aux[3] = u[2];
+        fields = true;
+    } else if (MODE != BND_LOCAL) {
+        gather_general<T>(a, x, y, z, cell, h);
+        if (rule == WET_VEL_ZOUHE || rule == WET_PRE_ZOUHE) {
+            const bool pressure = rule == WET_PRE_ZOUHE;
+            if (zou_he(a, ct, pressure, h, rho, u) && valid) {
+                if (pressure) a.vel[(size_t)ax * nc + cell] = u[ax];
+                else a.rho[cell] = rho;
+            }
+            fields = true;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(src[own + q * 32]);
+        fields = rule != WET_NONE;
+    }
+    if (!fields) {
+        // free-slip neighbour without a wet-node rule: moments as the first pass
+        // (MODE != BND_STREAM for inlets: an inlet always has fields set)
+        float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float d = h[q] * (wq(q) * a.dec);
+            dr += d; jx += cx(q) * d; jy += cy(q) * d; jz += cz(q) * d;
+        }
+        rho = 1.f + dr;
+        u[0] = jx / rho; u[1] = jy / rho; u[2] = jz / rho;
+        if (MODE != BND_LOCAL && valid && (lk & LINK_FLUID)) {
+            a.rho[cell] = rho;
+            a.vel[cell] = u[0]; a.vel[nc + cell] = u[1]; a.vel[2 * nc + cell] = u[2];
+        }
+    }
+    if (MODE == BND_STREAM) {
+        if (valid && rule != WET_INLET) {   // an inlet's f already sits in dst
+#pragma unroll
+            for (int q = 0; q < Q; ++q) dst[own + q * 32] = Store<T>::narrow(h[q]);
+            if (rule == WET_EXIT && a.aux != nullptr) {
+                T *ap = static_cast<T *>(a.aux) + aown;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+            }
+        }
+        return;
+    }
+    const bool act = valid && collide_it;
+    uint32_t key = (a.key != nullptr && act) ? a.key[cell] : 0u;
+    const bool psc = a.key != nullptr && __any_sync(0xffffffffu, key != 0u);
+    CellForce cf[1];
+    const bool acts[1] = {act};
+    const int xs[1] = {x};
+    const uint32_t keys[1] = {key};
+    const float epss[1] = {(a.eps != nullptr && key) ? a.eps[cell] : 0.f};
+    const float ovr[4] = {rho, u[0], u[1], u[2]};
+    float hout[Q];
+    collide<float, SMAG, true>(
+        a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { hout[q] = v; },
+        [&](int k, float v) { aux[k] = v; }, [](float, float, float, float) {}, ovr);
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) dst[own + q * 32] = Store<T>::narrow(hout[q]);
+        if (MODE == BND_GATHER && rule == WET_INLET) {
+            // the buffer read as src this step is the next step's dst: it takes f
+            T *keep = const_cast<T *>(src) + own;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) keep[q * 32] = Store<T>::narrow(h[q]);
+        }
+    }
+    if (act) {
+        if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
+            T *ap = static_cast<T *>(a.aux) + aown;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+        }
+        if (a.hydro_out) {
+            a.hydro_out[cell] = cf[0].hx;
+            a.hydro_out[nc + cell] = cf[0].hy;
+            a.hydro_out[2 * nc + cell] = cf[0].hz;
+        }
+    }
+    if (psc) reduce_forces(a, cf[0]);
+}
+
 // f = feq(rho, u) (initialize, psclattice3d.py:60-75)
 template <typename T>
-__global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_in, int smag_ref) {
+__global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_in, int smag_ref, void *other) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
@@ -563,16 +863,27 @@ __global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_i
     const uint32_t row = (uint32_t)(z * a.ny + y);
     const uint32_t c = row * (uint32_t)a.nx + (uint32_t)x;
     T *dst = static_cast<T *>(a.dst) + (row * a.rs + xslot((uint32_t)x, QB));
-    const bool skip = (a.links[c] & LINK_SKIP) != 0;
+    // initialize() skips the map's skip set: OBSTACLE / VEL_LADD / FREE_SLIP, and
+    // Ladd inlets where the lattice skips them (lbm_solver3d.py:163, psclattice3d.py:66).
+    // No collision ever writes those cells, so they keep the reference's
+    // zero-initialised populations, f = 0, in both buffers (a free-slip mirror
+    // can read them, lbm_solver3d.py:230-236).
+    const bool skip = (a.links[c] & LINK_MAP_SKIP) != 0;
     const float rho = skip ? 1.f : rho_in[c];
     const float ux = skip ? 0.f : vel_in[c], uy = skip ? 0.f : vel_in[nc + c], uz = skip ? 0.f : vel_in[2 * nc + c];
     const float drho = rho - 1.f;
     const float usq = ux * ux + uy * uy + uz * uz;
+    if (skip) {
+        T *o = static_cast<T *>(other) + (row * a.rs + xslot((uint32_t)x, QB));
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
-        const float fe = wq(q) * (drho + rho * (3.f * cu + 4.5f * cu * cu - 1.5f * usq));
-        dst[q * 32] = Store<T>::enc(fe, a.enc / wq(q));
+        for (int q = 0; q < Q; ++q) dst[q * 32] = o[q * 32] = Store<T>::narrow(-a.S);
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float cu = cx(q) * ux + cy(q) * uy + cz(q) * uz;
+            const float fe = wq(q) * (drho + rho * (3.f * cu + 4.5f * cu * cu - 1.5f * usq));
+            dst[q * 32] = Store<T>::enc(fe, a.enc / wq(q));
+        }
     }
     if (smag_ref) {
         T *ax = static_cast<T *>(a.aux) + (row * a.ars + xslot((uint32_t)x, AB));
@@ -584,9 +895,11 @@ __global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_i
     }
 }
 
-// link masks from CellType (lbm_solver3d.py:203-236): bounce-back bit q when
-// the neighbour x - c_q is OBSTACLE or a moving wall (VEL_LADD); for the
-// latter also bit q of moving[] and LINK_MOVING
+// link masks from CellType (lbm_solver3d.py:203-250): bounce-back bit q when
+// the neighbour x - c_q is OBSTACLE, a moving wall (VEL_LADD) or a Ladd inlet
+// (VEL_INLET_LADD); for the latter two also bit q of moving[] and LINK_MOVING.
+// Cells with a wet-node rule or a free-slip neighbour are deferred to the
+// boundary pass; the interior neighbour of an exit or inlet keeps its moments.
 __global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inlet, uint32_t *links, uint32_t *moving) {
     const size_t nc = (size_t)nx * ny * nz;
     const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -594,11 +907,17 @@ __global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inle
     const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
     const int32_t own = ct[c];
     uint32_t L = 0, M = 0;
-    if (own & (LBDEM_CT_OBSTACLE | LBDEM_CT_VEL_LADD | LBDEM_CT_FREE_SLIP | LBDEM_CT_VEL_INLET_LADD)) L |= LINK_SKIP;
-    int32_t mskip = LBDEM_CT_OBSTACLE | LBDEM_CT_VEL_LADD | LBDEM_CT_FREE_SLIP;
+    const int32_t walls = LBDEM_CT_OBSTACLE | LBDEM_CT_VEL_LADD | LBDEM_CT_FREE_SLIP;
+    const bool sskip = (own & (walls | LBDEM_CT_VEL_INLET_LADD)) != 0;
+    if (sskip) L |= LINK_SKIP;
+    int32_t mskip = walls;
     if (skip_inlet) mskip |= LBDEM_CT_VEL_INLET_LADD;
     if (own & mskip) L |= LINK_MAP_SKIP;
     if (own & LBDEM_CT_FLUID) L |= LINK_FLUID;
+    if (own & LBDEM_CT_VEL_INLET_LADD) L |= LINK_INLET;
+    const int rule = wet_rule(own);
+    if (rule == WET_INLET && !(own & walls)) L |= LINK_DEFER | LINK_PHASE_B;
+    if (!sskip && rule != WET_NONE) L |= LINK_DEFER | (rule == WET_EXIT ? LINK_PHASE_B : 0u);
     const int32_t prop = LBDEM_CT_FLUID | LBDEM_CT_VEL_ZOUHE | LBDEM_CT_VEL_EXIT | LBDEM_CT_PRE_ZOUHE;
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
@@ -610,10 +929,27 @@ __global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inle
         if (ctn & prop) continue;
         if (ctn & LBDEM_CT_OBSTACLE) {
             L |= LINK_BB(q);
-        } else if (ctn & LBDEM_CT_VEL_LADD) {
+        } else if (ctn & (LBDEM_CT_VEL_LADD | LBDEM_CT_VEL_INLET_LADD)) {
             L |= LINK_BB(q) | LINK_MOVING;
             M |= LINK_BB(q);
+        } else if ((ctn & LBDEM_CT_FREE_SLIP) && !sskip) {
+            L |= LINK_DEFER;
         }
+    }
+    // interior neighbour of an exit / inlet face cell (the face's +s side;
+    // the reference reads it without periodic wrap, lbm_solver3d.py:522-527, 647-658)
+    if (!(L & LINK_DEFER) && !sskip) {
+        const int p[3] = {x, y, z}, n[3] = {nx, ny, nz};
+        for (int a = 0; a < 3; ++a)
+            for (int s = -1; s <= 1; s += 2) {
+                int m[3] = {p[0], p[1], p[2]};
+                m[a] -= s;   // candidate boundary cell whose interior neighbour (at +s) is this cell
+                if (m[a] < 0 || m[a] >= n[a]) continue;
+                const int32_t cm = ct[((size_t)m[2] * ny + m[1]) * nx + m[0]];
+                const int r = wet_rule(cm);
+                int fa, fs;
+                if ((r == WET_EXIT || r == WET_INLET) && face_of(cm, fa, fs) && fa == a && fs == s) L |= LINK_KEEP;
+            }
     }
     links[c] = L;
     if (moving) moving[c] = M;
@@ -625,7 +961,7 @@ __global__ void k_rows(const uint32_t *links, int nx, int nrows, uint8_t *row_si
     const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     if (row >= nrows) return;
-    const uint32_t bad_mask = LINK_SKIP | 0x7FFFEu;
+    const uint32_t bad_mask = LINK_SKIP | LINK_DEFER | LINK_KEEP | 0x7FFFEu;
     int ok = 1;
     for (int x = lane; x < nx; x += 32) {
         const uint32_t L = links[(size_t)row * nx + x];
@@ -750,6 +1086,77 @@ __global__ void __launch_bounds__(256) k_stress(const StepArgs a, float *out) {
     out[6 * nc + cell] = sqrtf(0.5f * (txy * txy + txz * txz + tyz * tyz));
 }
 
+// Boundary-pass cell list in lattice order: per-row counts (one warp per
+// row), one block's exclusive scan over the rows, then an ordered fill.
+__global__ void k_bnd_count(const uint32_t *links, int nx, int nrows, int32_t *cnt) {
+    const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (row >= nrows) return;
+    int na = 0, nb = 0;
+    for (int x0 = 0; x0 < nx; x0 += 32) {
+        const int x = x0 + lane;
+        const uint32_t L = x < nx ? links[(size_t)row * nx + x] : 0u;
+        na += __popc(__ballot_sync(0xffffffffu, (L & LINK_DEFER) && !(L & LINK_PHASE_B)));
+        nb += __popc(__ballot_sync(0xffffffffu, (L & LINK_DEFER) && (L & LINK_PHASE_B)));
+    }
+    if (lane == 0) {
+        cnt[row] = na;
+        cnt[nrows + row] = nb;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_bnd_scan(int32_t *cnt, int nrows, uint32_t *counts) {
+    __shared__ int32_t sh[1024];
+    const int t = threadIdx.x;
+    for (int part = 0; part < 2; ++part) {
+        int32_t *c = cnt + (size_t)part * nrows;
+        int32_t carry = 0;
+        for (int base = 0; base < nrows; base += 1024) {
+            const int i = base + t;
+            const int32_t v = i < nrows ? c[i] : 0;
+            sh[t] = v;
+            __syncthreads();
+            for (int o = 1; o < 1024; o <<= 1) {
+                const int32_t add = t >= o ? sh[t - o] : 0;
+                __syncthreads();
+                sh[t] += add;
+                __syncthreads();
+            }
+            if (i < nrows) c[i] = carry + sh[t] - v;
+            const int32_t tot = sh[1023];
+            __syncthreads();
+            carry += tot;
+        }
+        if (t == 0) counts[part] = (uint32_t)carry;
+    }
+}
+
+__global__ void k_bnd_fill(const uint32_t *links, int nx, int nrows, const int32_t *off, const uint32_t *counts,
+                           uint32_t *cells, uint32_t cap) {
+    const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (row >= nrows) return;
+    uint32_t pa = (uint32_t)off[row], pb = counts[0] + (uint32_t)off[nrows + row];
+    const uint32_t below = (1u << lane) - 1u;
+    for (int x0 = 0; x0 < nx; x0 += 32) {
+        const int x = x0 + lane;
+        const uint32_t L = x < nx ? links[(size_t)row * nx + x] : 0u;
+        const bool fa = (L & LINK_DEFER) && !(L & LINK_PHASE_B), fb = (L & LINK_DEFER) && (L & LINK_PHASE_B);
+        const uint32_t ma = __ballot_sync(0xffffffffu, fa), mb = __ballot_sync(0xffffffffu, fb);
+        const uint32_t c = (uint32_t)row * (uint32_t)nx + (uint32_t)x;
+        if (fa) {
+            const uint32_t i = pa + __popc(ma & below);
+            if (i < cap) cells[i] = c;
+        }
+        if (fb) {
+            const uint32_t i = pb + __popc(mb & below);
+            if (i < cap) cells[i] = c;
+        }
+        pa += __popc(ma);
+        pb += __popc(mb);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -813,7 +1220,23 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
         set_error("moving walls need the rho and vel fields");
         return LBDEM_ERR_ARG;
     }
+    a.ct = L->ct;
+    if (L->bnd_na + L->bnd_nb > 0 && (!L->ct || !L->bnd_cells || !L->rho || !L->vel)) {
+        set_error("open boundaries need ct, bnd_cells and the rho and vel fields");
+        return LBDEM_ERR_ARG;
+    }
     return LBDEM_OK;
+}
+
+// Boundary pass of a step (MODE BND_GATHER / BND_LOCAL) or stream call
+// (BND_STREAM): first-pass cells, then second-pass cells.
+template <typename T, int SMAG, int MODE>
+static void launch_boundary(const lbdem_lattice *L, const StepArgs &a, cudaStream_t st) {
+    if (L->bnd_na > 0)
+        k_boundary<T, SMAG, MODE><<<(L->bnd_na + 127) / 128, 128, 0, st>>>(a, L->bnd_cells, L->bnd_na);
+    if (L->bnd_nb > 0)
+        k_boundary<T, SMAG, MODE><<<(L->bnd_nb + 127) / 128, 128, 0, st>>>(a, L->bnd_cells + L->bnd_na,
+                                                                            L->bnd_nb);
 }
 
 static void step_geometry(const lbdem_lattice *L, dim3 &grid, dim3 &block, int nthreads = 256) {
@@ -853,7 +1276,11 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
     }
     dim3 grid, block;
     step_geometry(L, grid, block, ONE_THREADS);
-#define LBDEM_STEP_CASE(G_, S_) k_psc_step<T, G_, S_><<<grid, block, 0, st>>>(a)
+#define LBDEM_STEP_CASE(G_, S_)                                        \
+    do {                                                               \
+        k_psc_step<T, G_, S_><<<grid, block, 0, st>>>(a);              \
+        launch_boundary<T, S_, G_ ? BND_GATHER : BND_LOCAL>(L, a, st); \
+    } while (0)
     if (gather) {
         if (L->smag_mode == LBDEM_SMAG_OFF) LBDEM_STEP_CASE(true, LBDEM_SMAG_OFF);
         else if (L->smag_mode == LBDEM_SMAG_REFERENCE) LBDEM_STEP_CASE(true, LBDEM_SMAG_REFERENCE);
@@ -881,6 +1308,7 @@ static int launch_stream_moments(const lbdem_lattice *L, int src, int dst, cudaS
     dim3 grid, block;
     step_geometry(L, grid, block);
     k_stream_moments<T><<<grid, block, 0, st>>>(a, L->rho, L->vel);
+    launch_boundary<T, LBDEM_SMAG_OFF, BND_STREAM>(L, a, st);
     return check_launch("stream_moments");
 }
 
@@ -889,14 +1317,14 @@ static int launch_init(const lbdem_lattice *L, int buf, cudaStream_t st) {
     StepArgs a;
     int rc = fill_args(L, a);
     if (rc) return rc;
-    if (buf < 0 || buf > 1 || !L->rho || !L->vel) {
+    if (buf < 0 || buf > 1 || !L->rho || !L->vel || !L->f[0] || !L->f[1]) {
         set_error("lattice_init: bad buffers");
         return LBDEM_ERR_ARG;
     }
     a.dst = L->f[buf];
     dim3 grid, block;
     step_geometry(L, grid, block);
-    k_init<T><<<grid, block, 0, st>>>(a, L->rho, L->vel, L->aux != nullptr);
+    k_init<T><<<grid, block, 0, st>>>(a, L->rho, L->vel, L->aux != nullptr, L->f[1 - buf]);
     return check_launch("lattice_init");
 }
 
@@ -1029,6 +1457,24 @@ int lbdem_build_links(const int32_t *ct, int32_t nx, int32_t ny, int32_t nz, int
     const int nrows = ny * nz;
     k_rows<<<(nrows + 7) / 8, 256, 0, st>>>(links, nx, nrows, row_simple);
     return check_launch("build_links");
+}
+
+int lbdem_boundary_cells(const uint32_t *links, int32_t nx, int32_t ny, int32_t nz, uint32_t *cells,
+                         uint32_t capacity, uint32_t *counts, int32_t *scratch, void *stream) {
+    if (!links || !counts || !scratch || nx <= 0 || ny <= 0 || nz <= 0 || (capacity > 0 && !cells)) {
+        set_error("boundary_cells: bad arguments");
+        return LBDEM_ERR_ARG;
+    }
+    if ((size_t)nx * ny * nz >= (1ull << 32)) {
+        set_error("boundary_cells: cell indices are 32-bit");
+        return LBDEM_ERR_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nrows = ny * nz;
+    k_bnd_count<<<(nrows + 7) / 8, 256, 0, st>>>(links, nx, nrows, scratch);
+    k_bnd_scan<<<1, 1024, 0, st>>>(scratch, nrows, counts);
+    if (capacity > 0) k_bnd_fill<<<(nrows + 7) / 8, 256, 0, st>>>(links, nx, nrows, scratch, counts, cells, capacity);
+    return check_launch("boundary_cells");
 }
 
 int lbdem_lattice_init(const lbdem_lattice *L, int32_t buf, void *stream) {

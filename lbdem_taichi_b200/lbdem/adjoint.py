@@ -49,8 +49,9 @@ class FrozenBedDrag:
         if lat.dem.n == 0:
             raise ValueError("no particles")
         lat._sync_inputs()
-        if lat.has_moving_walls:
-            raise ValueError("the adjoint covers fixed walls (OBSTACLE) only, not moving walls (VEL_LADD)")
+        if lat.has_moving_walls or lat.has_open_boundaries:
+            raise ValueError("the adjoint covers fixed walls (OBSTACLE) only, not moving walls (VEL_LADD), "
+                             "inlets or other open boundaries")
         if int(n_steps) < 1 or int(checkpoint_every) < 1:
             raise ValueError("n_steps and checkpoint_every must be positive")
         self.lat = lat

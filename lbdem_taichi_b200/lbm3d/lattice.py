@@ -26,8 +26,12 @@ from .lbmutils import CellType, UnitConverter
 _STORAGE = {"f32": (N.F32, torch.float32, 1.0), "f16": (N.F16, torch.float16, 4096.0),
             "bf16": (N.BF16, torch.bfloat16, 1.0)}
 _SMAG = {"off": N.SMAG_OFF, "reference": N.SMAG_REFERENCE, "local": N.SMAG_LOCAL}
-_UNSUPPORTED = (CellType.FREE_SLIP | CellType.VEL_ZOUHE | CellType.VEL_EXIT
-                | CellType.Pre_ZOUHE | CellType.VEL_INLET_LADD | CellType.INTERFACE | CellType.GAS)
+# free-surface cell types (the reference's PSC path never sets them)
+_UNSUPPORTED = CellType.INTERFACE | CellType.GAS
+# cell types handled by the boundary pass: wet-node rules of the stream's second
+# pass (lbm_solver3d.py:242-250) and free-slip walls (whose neighbours it streams)
+_OPEN = CellType.VEL_ZOUHE | CellType.VEL_EXIT | CellType.Pre_ZOUHE | CellType.VEL_INLET_LADD | CellType.FREE_SLIP
+_FACES = CellType.LEFT | CellType.RIGHT | CellType.BOTTOM | CellType.TOP | CellType.BACK | CellType.FRONT
 
 W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
 _STRESS_FIELDS = ("stress_xx", "stress_yy", "stress_zz", "stress_xy", "stress_xz", "stress_yz", "shear_stress_mag")
@@ -50,6 +54,15 @@ def from_ref(a, comps=None):
     if comps is None:
         return np.ascontiguousarray(a.transpose(2, 1, 0))
     return np.ascontiguousarray(a.transpose(3, 2, 1, 0))
+
+
+class _CellVector(np.ndarray):
+    """One cell's vector of a writable field: component writes
+    (``lattice.vel[i, j, k][0] = u``, as Taichi allows) go back to the field."""
+
+    def __setitem__(self, k, v):
+        super().__setitem__(k, v)
+        self._field[self._idx] = np.asarray(self)
 
 
 class LatticeField:
@@ -85,7 +98,14 @@ class LatticeField:
 
     def __getitem__(self, idx):
         v = self._get_host()[idx]
-        return v.copy() if isinstance(v, np.ndarray) else v
+        if not isinstance(v, np.ndarray):
+            return v
+        v = v.copy()
+        if self._push is not None and v.ndim == 1 and len(self._shape) == 4 and isinstance(idx, tuple) \
+                and len(idx) == 3 and all(isinstance(i, (int, np.integer)) for i in idx):
+            v = v.view(_CellVector)
+            v._field, v._idx = self, idx
+        return v
 
     def _writable(self):
         if self._push is None:
@@ -155,6 +175,11 @@ class LatticeEngine:
         self._links = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._moving = None
         self.has_moving_walls = False
+        # open boundaries: cells of the boundary pass (lbdem_boundary_cells)
+        self.has_open_boundaries = False
+        self._bnd = None
+        self._bnd_counts = torch.zeros(2, dtype=torch.int32, device=dev)
+        self._bnd_scratch = None
         self._rows = torch.zeros(self.Ny * self.Nz, dtype=torch.uint8, device=dev)
         self._ct_dev = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -199,6 +224,7 @@ class LatticeEngine:
         L.aux = N.ptr(self._aux)
         L.links, L.row_simple = N.ptr(self._links), N.ptr(self._rows)
         L.status = N.ptr(self._status)
+        L.ct = N.ptr(self._ct_dev)
 
     # ------------------------------------------------------------ host mirrors
     def _host_dirty(self, name):
@@ -208,18 +234,43 @@ class LatticeEngine:
     def _push_ct(self, host):
         bad = np.bitwise_and(host, _UNSUPPORTED)
         if bad.any():
-            raise NotImplementedError(
-                "cell types other than FLUID, OBSTACLE and VEL_LADD (Zou-He, exits, Ladd inlets, free "
-                "slip, free surface) are not supported by the fused kernel")
+            raise NotImplementedError("free-surface cell types (INTERFACE, GAS) are not supported")
+        slip = np.bitwise_and(host, CellType.FREE_SLIP) != 0
+        if (slip & (np.bitwise_and(host, _FACES) == 0)).any():
+            raise ValueError("FREE_SLIP cells need a face bit (LEFT/RIGHT/BOTTOM/TOP/BACK/FRONT) for the mirror "
+                             "direction (lbm_solver3d.py:230-236)")
         self._ct_dev.copy_(torch.from_numpy(from_ref(host.astype(np.int32)).reshape(-1)))
-        # moving walls: per-cell moving-link bits, allocated on first use
-        if np.bitwise_and(host, CellType.VEL_LADD).any():
+        self.has_open_boundaries = bool(np.bitwise_and(host, _OPEN).any())
+        # moving walls and Ladd inlets: per-cell velocity-link bits, allocated on first use
+        if np.bitwise_and(host, CellType.VEL_LADD | CellType.VEL_INLET_LADD).any():
             if self._moving is None:
                 self._moving = torch.zeros(self.ncells, dtype=torch.int32, device="cuda")
             self._lat.moving = N.ptr(self._moving)
         else:
             self._lat.moving = None
         self.has_moving_walls = self._lat.moving is not None
+
+    def _build_boundary_list(self):
+        """Cells of the boundary pass, in lattice order (one host read of the counts)."""
+        L = self._lat
+        if not self.has_open_boundaries:
+            L.bnd_cells, L.bnd_na, L.bnd_nb = None, 0, 0
+            return
+        if self._bnd_scratch is None:
+            self._bnd_scratch = torch.zeros(2 * self.Ny * self.Nz, dtype=torch.int32, device="cuda")
+        if self._bnd is None:
+            # six faces' worth; grown below when the lattice holds more boundary cells
+            n0 = 2 * (self.Ny * self.Nz + self.Nx * self.Nz + self.Nx * self.Ny) + 64
+            self._bnd = torch.zeros(n0, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            cap = self._bnd.numel()
+            N.call("lbdem_boundary_cells", N.ptr(self._links), self.Nx, self.Ny, self.Nz, N.ptr(self._bnd), cap,
+                   N.ptr(self._bnd_counts), N.ptr(self._bnd_scratch), N.stream_handle())
+            na, nb = (int(v) for v in self._bnd_counts.cpu())
+            if na + nb <= cap:
+                break
+            self._bnd = torch.zeros(na + nb, dtype=torch.int32, device="cuda")
+        L.bnd_cells, L.bnd_na, L.bnd_nb = N.ptr(self._bnd), na, nb
 
     def _push_rho(self, host):
         self._rho.copy_(torch.from_numpy(from_ref(host).reshape(-1).astype(np.float32)))
@@ -236,6 +287,7 @@ class LatticeEngine:
             N.call("lbdem_build_links", N.ptr(self._ct_dev), self.Nx, self.Ny, self.Nz, int(self.skip_inlet),
                    N.ptr(self._links), N.ptr(self._rows), N.ptr(self._moving) if self._lat.moving else None,
                    N.stream_handle())
+            self._build_boundary_list()
             self._links_dirty = False
         self.rho.flush()
         self.vel.flush()
@@ -358,7 +410,10 @@ class LatticeEngine:
         if d["smagorinsky"] != self.smagorinsky:
             raise ValueError("restart state was taken with another Smagorinsky mode")
         self._sync_inputs()
+        # both buffers: cells no collision writes (walls, skipped inlets) and a
+        # Ladd inlet's populations must read the same from either
         self._f[0].copy_(d["f"])
+        self._f[1].copy_(d["f"])
         self._rho.copy_(d["rho"])
         self._vel.copy_(d["vel"])
         if self._aux is not None:

@@ -524,12 +524,76 @@ def scen_open_zb():
                (CellType.Pre_ZOUHE | CellType.FRONT, 1.0), 0.02, 58)
 
 
+def scen_open_slip():
+    """The pressure-drop channel with free-slip side walls: Ladd inlet at
+    x = 0, Zou-He pressure at x = Nx-1, FREE_SLIP walls at y = 0 / Ny-1 set
+    last (they own the corner cells), one PSC sphere (lbm_solver3d.py:230-236)."""
+    rng = np.random.default_rng(59)
+    nx, ny, nz = 14, 10, 8
+    pos = np.array([[nx / 2 - 0.3, ny / 2 + 0.2, nz / 2 - 0.1]])
+    rad = np.array([2.2])
+    domain = (0.0, float(nx), 0.0, float(ny), 0.0, float(nz))
+    dem = make_dem(domain, 0.25, (0.0, 0.0, 0.0), HertzContactConfig(0.3, 0.3, 0.9, 0.9),
+                   rad, 2.0, pos, np.zeros((1, 3)), periodic=(False, False, True))
+    lat = PSCLattice3D(nx, ny, nz, 1.0 / 0.7, 1.0, 1.0, 1.0, dem)
+    random_flow(lat, rng, 0.005, 0.002)
+    ct = lat.CT.arr
+    ct[0] = CellType.VEL_INLET_LADD | CellType.LEFT
+    lat.vel.arr[0] = (0.02, 0.0, 0.0)
+    ct[-1] = CellType.Pre_ZOUHE | CellType.RIGHT
+    lat.rho.arr[-1] = 1.0
+    lat.vel.arr[-1] = 0.0
+    ct[:, 0] = CellType.FREE_SLIP | CellType.BOTTOM
+    ct[:, -1] = CellType.FREE_SLIP | CellType.TOP
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy(),
+                gpos=pos, grad=rad, gvel=np.zeros((1, 3)), gomega=np.zeros((1, 3)), domain=np.array(domain))
+    lat.initialize()
+    out = {}
+    for s in range(4):
+        lat.collide()
+        out[f"force_fluid_{s}"] = dem.gf.force_fluid.to_numpy()
+        lat.stream()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save("open_slip", omega0=np.float64(1.0 / 0.7), nsteps=np.int64(4), **init, **out)
+
+
+def scen_open_smag():
+    """BasicLattice3D (Smagorinsky, inlets skipped by initialize/collide) with a
+    Ladd inlet at x = 0, a convective exit at x = Nx-1 and FREE_SLIP walls at
+    z = 0 / Nz-1: the exit's equilibrium overwrite feeds the next computeOmega
+    (lbm_solver3d.py:176-192, 645-663)."""
+    rng = np.random.default_rng(60)
+    nx, ny, nz = 14, 8, 9
+    lat = BasicLattice3D(nx, ny, nz, 1.0 / 0.55, 1.0, 1.0, 1.0)
+    random_flow(lat, rng, 0.03, 0.004)
+    ct = lat.CT.arr
+    ct[0] = CellType.VEL_INLET_LADD | CellType.LEFT
+    lat.vel.arr[0] = (0.04, 0.0, 0.0)
+    ct[-1] = CellType.VEL_EXIT | CellType.RIGHT
+    ct[:, :, 0] = CellType.FREE_SLIP | CellType.BACK
+    ct[:, :, -1] = CellType.FREE_SLIP | CellType.FRONT
+    init = dict(ct=lat.CT.to_numpy(), rho0=lat.rho.to_numpy(), vel0=lat.vel.to_numpy())
+    lat.initialize()
+    out = {}
+    for s in range(4):
+        lat.collide()
+        out[f"omega_{s}"] = lat.omega.to_numpy()
+        lat.stream()
+        out[f"f_{s}"] = lat.f.to_numpy()
+        out[f"rho_{s}"] = lat.rho.to_numpy()
+        out[f"vel_{s}"] = lat.vel.to_numpy()
+    save("open_smag", omega0=np.float64(1.0 / 0.55), cs=np.float64(BasicLattice3D.SmagorinskyConstant),
+         nsteps=np.int64(4), **init, **out)
+
+
 SCENARIOS = {
     "bgk_smag": scen_bgk_smag, "forced": scen_forced, "psc": scen_psc, "hybrid": scen_hybrid,
     "dem_hertz": scen_dem_hertz, "dem_linear": scen_dem_linear, "coupled": scen_coupled,
     "couette_ladd": scen_couette_ladd, "open_x": scen_open_x, "open_y": scen_open_y, "open_z": scen_open_z,
     "open_xr": scen_open_xr, "open_exit_x": scen_open_exit_x, "open_exit_z": scen_open_exit_z,
-    "open_yr": scen_open_yr, "open_zb": scen_open_zb,
+    "open_yr": scen_open_yr, "open_zb": scen_open_zb, "open_slip": scen_open_slip, "open_smag": scen_open_smag,
 }
 
 if __name__ == "__main__":

@@ -29,7 +29,7 @@ def test_every_declared_function_is_exported():
     assert not missing, missing
     # every declared function has a ctypes signature in the bindings, and vice versa
     assert set(names) == set(N.EXPORTS), set(names) ^ set(N.EXPORTS)
-    assert lib.lbdem_abi_version() == 1
+    assert lib.lbdem_abi_version() == N.ABI_VERSION == 2
 
 
 def test_host_side_argument_checks():
@@ -58,6 +58,17 @@ def test_host_side_argument_checks():
     d3 = (C.c_double * 3)(1, 0, 0)
     rc = lib.lbdem_psc_step_adjoint_f32(C.byref(L), C.byref(P), 8, None, 8, 8, 8, d3, 1, 1, None)
     assert rc == N.LBDEM_ERR_UNSUPPORTED
+    # ... and fixed walls only: open boundaries are refused
+    L.storage = N.F32
+    L.bnd_na, L.bnd_nb = 4, 0
+    rc = lib.lbdem_psc_step_adjoint_f32(C.byref(L), C.byref(P), 8, None, 8, 8, 8, d3, 1, 1, None)
+    assert rc == N.LBDEM_ERR_UNSUPPORTED
+    # a boundary pass needs the cell types, the list and the macroscopic fields
+    assert lib.lbdem_psc_step_f32(C.byref(L), None, None, 0, 1, 1, None) == N.LBDEM_ERR_ARG
+    assert b"open boundaries" in lib.lbdem_last_error()
+    # the list builder validates its arguments before any launch
+    assert lib.lbdem_boundary_cells(None, 8, 8, 8, None, 0, 8, 8, None) == N.LBDEM_ERR_ARG
+    assert lib.lbdem_boundary_cells(8, 8, 8, 8, None, 16, 8, 8, None) == N.LBDEM_ERR_ARG   # capacity, no array
 
 
 @pytest.mark.skipif(subprocess.run(["which", "gcc"], capture_output=True).returncode != 0, reason="no gcc")

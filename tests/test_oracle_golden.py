@@ -104,7 +104,8 @@ def test_moving_walls_ladd_match_reference():
     assert g["vel_2"][:, :, -2, 0].mean() > 0 > g["vel_2"][:, :, 1, 0].mean()
 
 
-OPEN_SCENARIOS = ("open_x", "open_y", "open_z", "open_xr", "open_exit_x", "open_exit_z", "open_yr", "open_zb")
+OPEN_SCENARIOS = ("open_x", "open_y", "open_z", "open_xr", "open_exit_x", "open_exit_z", "open_yr", "open_zb",
+                  "open_slip")
 
 
 @pytest.mark.parametrize("name", OPEN_SCENARIOS)
@@ -130,6 +131,22 @@ def test_open_boundaries_match_reference(name):
     # the boundaries act: the flow through the lattice is along the open axis
     axis = int(np.argmax(g["ct"].shape))
     assert abs(g["vel_3"][..., axis].mean()) > 1e-3
+
+
+def test_open_boundaries_smagorinsky_match_reference():
+    """BasicLattice3D (Smagorinsky; initialize/collide skip the Ladd inlet) with
+    a Ladd inlet, a convective exit and free-slip walls."""
+    g = load("open_smag")
+    lat = _lattice_from(g, smag=True, smag_cs=float(g["cs"]), skip_inlet=True)
+    lat.initialize()
+    for s in range(int(g["nsteps"])):
+        lat.collide()
+        assert relmax(lat.omega, g[f"omega_{s}"]) < TOL
+        lat.stream()
+        assert relmax(lat.f, g[f"f_{s}"]) < TOL
+        assert relmax(lat.rho, g[f"rho_{s}"]) < TOL
+        assert relmax(lat.vel, g[f"vel_{s}"]) < TOL
+    assert g["omega_3"].min() < float(g["omega0"]) - 1e-3
 
 
 def test_hybrid_psc_smagorinsky_matches_reference():
