@@ -12,6 +12,7 @@ collide-stream with force reduction -> 10 DEM sub-steps.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16]
     python bench.py --workload c5        # 512x512x256 channel, 20000 spheres, LES
     python bench.py --workload c1        # single sphere settling, 64x64x128
+    python bench.py --workload pdrop     # packed-bed pressure drop, 722x242x242, open boundaries
     python bench.py --impl reference     # FP64 CPU restatement of the reference path
     python bench.py --adjoint [--adjoint-fd K]   # drag gradient on the frozen-bed channel (below)
 
@@ -58,6 +59,16 @@ WORKLOADS = {
                     "(lagged), Hertz with the bottom wall, 10 DEM sub-steps",
                shape=(64, 64, 128), n=1, dmin=12.0, dmax=12.0, gap=0.0, walls_z=True, tau=0.6, cs=0.1,
                fluid_force=None, gravity=(0.0, 0.0, -1e-5 * (1.0 - 1.0 / 2.5)), rho_p=2.5, vel_sigma=0.0, sub=10),
+    # the packed-bed pressure-drop driver's configuration (pressure_drop_fully.py:106-116, 120-170, 200-245):
+    # 30 x 10 x 10 particle diameters at 24 cells per diameter, tau 0.68, Re 0.8 (inlet 2.0e-3 lu), frozen
+    # bed, linear contacts, one DEM sub-step, Ladd velocity inlet at x = 0, Zou-He pressure (rho = 1) at
+    # x = Nx-1, periodic y / z; the bed is seeded random sequential addition (the driver reads a packing file)
+    "pdrop": dict(desc="packed-bed pressure drop 722x242x242, Ladd velocity inlet 2.0e-3 at x=0, Zou-He pressure "
+                       "outlet rho=1 at x=Nx-1, periodic y/z, 1500 frozen spheres d=24 (RSA, 24 lu clear of the "
+                       "inlet and outlet), tau=0.68, Smagorinsky off, linear contacts, 1 DEM sub-step",
+                  shape=(722, 242, 242), n=1500, dmin=24.0, dmax=24.0, gap=0.5, walls_z=False, tau=0.68, cs=None,
+                  fluid_force=None, gravity=(0.0, 0.0, 0.0), rho_p=2.5, vel_sigma=0.0, sub=1, u_in=2.0e-3,
+                  x_clear=24.0),
 }
 W = dict(WORKLOADS["c2"], key="c2")
 NX, NY, NZ = W["shape"]
@@ -83,6 +94,10 @@ def workload(seed=2024):
     if W["key"] == "c1":
         pos = np.array([[NX / 2 + rng.uniform(-0.5, 0.5), NY / 2 + rng.uniform(-0.5, 0.5), NZ - 18.0]])
         rad = np.array([0.5 * W["dmin"]])
+    elif "u_in" in W:
+        xc = W["x_clear"]
+        pos, rad = rsa_spheres_grid(rng, NP, (NX - 2 * xc, NY, NZ), W["dmin"], W["dmax"], gap=W["gap"], margin=0.5)
+        pos[:, 0] += xc
     else:
         zlo = 1.0 if W["walls_z"] else None
         zhi = NZ - 1.0 if W["walls_z"] else None
@@ -97,28 +112,49 @@ def cell_types():
     ct = np.full((NX, NY, NZ), 1, np.int32)
     if W["walls_z"]:
         ct[:, :, 0] = ct[:, :, -1] = 8
+    if "u_in" in W:
+        ct[0] = 262144 | 8192     # VEL_INLET_LADD | LEFT
+        ct[-1] = 256 | 4096       # Pre_ZOUHE | RIGHT
     return ct
+
+
+def open_presets(vel, rho):
+    """Inlet velocity and outlet density of the open-boundary workload (in place)."""
+    vel[0, ..., 0] = W["u_in"]
+    rho[-1] = 1.0
 
 
 def build_gpu(storage, pos, rad, vel, mass):
     from lbdem_taichi_b200 import Vector3
-    from lbdem_taichi_b200.dem3d.demconfig import DEMSolverConfig, DomainBounds, HertzContactConfig
+    from lbdem_taichi_b200.dem3d.demconfig import (DEMSolverConfig, DomainBounds, HertzContactConfig,
+                                                   LinearContactConfig)
     from lbdem_taichi_b200.dem3d.demsolver import DEMSolver
     from lbdem_taichi_b200.lbdem.psclattice3d import PSCLattice3D
     domain = (0.0, float(NX), 0.0, float(NY), 0.0, float(NZ))
-    cfg = DEMSolverConfig(DomainBounds(*domain), 1.0 / SUB, Vector3(*W["gravity"]),
-                          HertzContactConfig(pp_friction=0.3, pw_friction=0.3, pp_restitution=0.9, pw_restitution=0.9))
+    opened = "u_in" in W
+    contact = (LinearContactConfig(stiffness_normal=4.5e3, stiffness_tangential=2.5e3, damping_normal=0.3,
+                                   damping_tangential=0.2, pp_friction=0.15, pw_friction=0.15) if opened else
+               HertzContactConfig(pp_friction=0.3, pw_friction=0.3, pp_restitution=0.9, pw_restitution=0.9))
+    cfg = DEMSolverConfig(DomainBounds(*domain), 1.0 / SUB, Vector3(*W["gravity"]), contact)
     cfg.set_particle_properties(elastic_modulus=1e5, poisson_ratio=0.3, max_coordinate_number=16)
     cfg.set_wall_properties(elastic_modulus=1e5, poisson_ratio=0.3)
-    cfg.set_periodic_boundaries(True, True, not W["walls_z"])
+    cfg.set_periodic_boundaries(not opened, True, not W["walls_z"])
     dem = DEMSolver(cfg)
     dem.init_particle_arrays(rad, mass, pos, vel, Vector3(0, 0, 0), Vector3(NX, NY, NZ))
-    dem.set_contact_model("hertz")
-    lat = PSCLattice3D(NX, NY, NZ, 1.0 / TAU, 1.0, 1.0, 1.0, dem, smagorinsky="reference",
+    dem.set_contact_model("linear" if opened else "hertz")
+    if opened:
+        dem.gf.freeze.from_numpy(np.ones(len(rad), np.int32))
+    lat = PSCLattice3D(NX, NY, NZ, 1.0 / TAU, 1.0, 1.0, 1.0, dem, smagorinsky="off" if CS is None else "reference",
                        body_force=W["fluid_force"], storage=storage)
-    lat.SmagorinskyConstant = CS
-    if W["walls_z"]:
+    if CS is not None:
+        lat.SmagorinskyConstant = CS
+    if W["walls_z"] or opened:
         lat.CT.from_numpy(cell_types())
+    if opened:
+        v, r = lat.vel.to_numpy(), lat.rho.to_numpy()
+        open_presets(v, r)
+        lat.vel.from_numpy(v)
+        lat.rho.from_numpy(r)
     lat.initialize()
     return lat, dem
 
@@ -304,7 +340,7 @@ def run_gpu(args):
         "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 2 * NP * 3 * 8,
                 "d2h_bytes_per_step": 4 * NP * 3 * 8},
         "gpu_launches": launches,
-        "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4), "dem_10_substeps": round(dem_ms, 4),
+        "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4), f"dem_{SUB}_substeps": round(dem_ms, 4),
                       "host_launch_per_step": round(cpu_launch_ms, 4)},
         "clocks": clocks,
     }
@@ -328,7 +364,11 @@ def cpu_sample(pos, rad, vel, mass, nz_slab):
     carrying every particle: same per-cell work (grains2lattice probes all
     particles for every cell), NX x NY x `nz_slab` cells."""
     from oracle.oracle import OracleDEM, OracleGrains, OracleLattice
-    lat = OracleLattice(NX, NY, nz_slab, 1.0 / TAU, smag=True, psc=True, force=W["fluid_force"], smag_cs=CS)
+    lat = OracleLattice(NX, NY, nz_slab, 1.0 / TAU, smag=CS is not None, psc=True, force=W["fluid_force"],
+                        smag_cs=CS if CS is not None else 0.1)
+    lat.ct[...] = cell_types()[:, :, :nz_slab]
+    if "u_in" in W:
+        open_presets(lat.vel, lat.rho)
     dem = OracleDEM(pos, vel, rad, mass, dt=1.0 / SUB, gravity=W["gravity"], domain=(0, NX, 0, NY, 0, NZ),
                     periodic=(True, True, not W["walls_z"]), E=1e5, nu=0.3, wall_E=1e5, wall_nu=0.3, pp_mu=0.3,
                     pw_mu=0.3, pp_e=0.9, pw_e=0.9, max_coord=16)
