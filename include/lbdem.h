@@ -163,6 +163,17 @@ typedef struct lbdem_psc {
     float *hydro_out;          /* optional per-cell hydrodynamic force (3*Ncells) or NULL */
     float *eps;                /* smooth solid fraction per cell (lbdem_psc_map_smooth), or NULL:
                                   the step then takes the exact 5^3 count from the key */
+    /* Map reuse (no counterpart in the reference, which remaps every step): with
+     * map_moved set (2 uint32 of caller device memory) and map_reuse = 1,
+     * lbdem_psc_map first checks whether any particle's lattice centre or
+     * mapping radius differs from the previous exact map's; if none does, the
+     * owner keys are already exact and only the particle table and the force
+     * accumulators are refreshed.  Set map_reuse = 0 whenever the cell types
+     * (link masks) changed since the previous map.  map_parity is the
+     * library's own toggle (start at 0). */
+    uint32_t *map_moved;
+    int32_t map_reuse;
+    int32_t map_parity;
 } lbdem_psc;
 
 typedef struct lbdem_dem {

@@ -24,6 +24,7 @@ struct MapArgs {
     float4 *table;
     double *prev;
     int have_prev;
+    const uint32_t *moved;   // map reuse: any particle moved since the previous map (device word), or NULL
     double *ff, *mf;
     int32_t *status;
 };
@@ -43,7 +44,8 @@ __device__ __forceinline__ void particle_lattice(const MapArgs &a, int g, double
 // force accumulators, and write the FP32 particle table used by the step.
 __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
     const int g = blockIdx.x;
-    if (a.have_prev) {
+    const bool reuse = a.moved != nullptr && *a.moved == 0u;   // keys are exact already
+    if (a.have_prev && !reuse) {
         const double pxc = a.prev[4 * g], pyc = a.prev[4 * g + 1], pzc = a.prev[4 * g + 2];
         const double lim = a.prev[4 * g + 3] + HALF_DIAG + 1e-6;
         if (lim > 0.0) {
@@ -81,6 +83,19 @@ __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
     }
 }
 
+// Map reuse check: flag[0] = 1 when some particle's lattice centre or mapping
+// radius differs (bitwise) from the previous map's; flag[1] (the other call
+// parity's word) is cleared for the next call.
+__global__ void k_map_moved(const MapArgs a, uint32_t *flag, uint32_t *other) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g == 0) *other = 0u;
+    if (g >= a.n) return;
+    double xc, yc, zc, r;
+    particle_lattice(a, g, xc, yc, zc, r);
+    const double *p = a.prev + 4 * (size_t)g;
+    if (!(xc == p[0] && yc == p[1] && zc == p[2] && r == p[3])) *flag = 1u;
+}
+
 // Exact FP64 sub-cell test, in the reference's operation order
 // (psclattice3d.py:125-128): sqrt(dx^2 + dy^2 + dz^2) < r.
 __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, double zc, int i, int j, int k, int ii,
@@ -109,6 +124,7 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32; w = global cell index
     __shared__ int s_amb[MAP_CHUNK];      // partial cells needing the exact recount (index into s_off)
     __shared__ int s_n, s_na;
+    if (a.moved != nullptr && *a.moved == 0u) return;   // reuse: nothing moved, keys unchanged
     const int g = blockIdx.x;
     double xc, yc, zc, r;
     particle_lattice(a, g, xc, yc, zc, r);
@@ -321,6 +337,7 @@ extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const 
         a.have_prev = 0;
         a.ff = G->force_fluid; a.mf = G->moment_fluid;
         a.status = L->status;
+        a.moved = nullptr;
         k_map_clear<<<G->n, 128, 0, st>>>(a);
         k_map_smooth<<<G->n, 256, 0, st>>>(a, reinterpret_cast<unsigned long long *>(scratch));
     }
@@ -357,7 +374,16 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     a.have_prev = P->have_prev;
     a.ff = G->force_fluid; a.mf = G->moment_fluid;
     a.status = L->status;
+    a.moved = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
+    if (P->map_moved && P->map_reuse && P->have_prev) {
+        // the previous exact map's centres are in prev: skip the remap when none changed
+        const int par = P->map_parity & 1;
+        uint32_t *flag = P->map_moved + par;
+        k_map_moved<<<(G->n + 255) / 256, 256, 0, st>>>(a, flag, P->map_moved + (1 - par));
+        a.moved = flag;
+        P->map_parity = 1 - par;
+    }
     k_map_clear<<<G->n, 128, 0, st>>>(a);
     k_map_scatter<<<G->n, 256, 0, st>>>(a);
     P->have_prev = 1;

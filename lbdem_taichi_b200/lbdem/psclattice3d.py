@@ -61,6 +61,12 @@ class PSCLattice3D(LatticeEngine):
         p.key, p.table, p.prev = N.ptr(self._key), N.ptr(self._table), N.ptr(self._prev)
         p.have_prev = 0
         p.hydro_out = N.ptr(self._hydro)
+        # map reuse: a bed whose particles did not move keeps its exact owner
+        # keys (the check runs on the device; the cell types must not have changed)
+        self._map_moved = torch.zeros(2, dtype=torch.int32, device=dev)
+        p.map_moved = N.ptr(self._map_moved)
+        p.map_reuse, p.map_parity = 0, 0
+        self._mapped_epoch = -1
         if solid_fraction == "smooth":
             self._eps = torch.zeros(nc, dtype=torch.float32, device=dev)
             self._map_scratch = torch.zeros(nc, dtype=torch.int64, device=dev)
@@ -123,8 +129,10 @@ class PSCLattice3D(LatticeEngine):
             N.call("lbdem_psc_map_smooth", C.byref(self._lat), C.byref(self._psc), C.byref(self._grains),
                    N.ptr(self._map_scratch), N.stream_handle())
         else:
+            self._psc.map_reuse = int(self._mapped_epoch == self._links_epoch)
             N.call("lbdem_psc_map", C.byref(self._lat), C.byref(self._psc), C.byref(self._grains),
                    N.stream_handle())
+            self._mapped_epoch = self._links_epoch
         self._decoded = None
 
     def initialize(self):

@@ -186,6 +186,7 @@ class LatticeEngine:
         self._sum_out = torch.zeros(4, dtype=torch.float64, device=dev)
         self._sum_part = torch.zeros(N.SUM_PARTIALS, dtype=torch.float64, device=dev)
         self._links_dirty = True
+        self._links_epoch = 0          # counts link-mask rebuilds (cell-type changes)
         self._initialized = False
         self._cur = 0
         self._cur_kind = "f"
@@ -289,6 +290,7 @@ class LatticeEngine:
                    N.stream_handle())
             self._build_boundary_list()
             self._links_dirty = False
+            self._links_epoch += 1
         self.rho.flush()
         self.vel.flush()
 
