@@ -124,7 +124,6 @@ typedef struct lbdem_lattice {
                               storage type (blocked): required by LBDEM_SMAG_REFERENCE and by
                               lbdem_stress, NULL otherwise (then the step neither reads nor writes it) */
     const uint32_t *links; /* per-cell link mask from lbdem_build_links */
-    const uint8_t *row_simple; /* per (y,z) row: 1 = row and its 8 neighbour rows all plain FLUID */
     int32_t *status;       /* device status word */
     const uint32_t *moving; /* per-cell bit q: neighbour x - c_q is a moving wall (VEL_LADD), from
                                lbdem_build_links; NULL when the lattice has no moving walls.  The
@@ -140,6 +139,11 @@ typedef struct lbdem_lattice {
     const int32_t *ct;          /* CellType per cell (device), required when bnd_na + bnd_nb > 0 */
     const uint32_t *bnd_cells;  /* bnd_na first-pass cells, then bnd_nb second-pass cells (exits, inlets) */
     uint32_t bnd_na, bnd_nb;
+    void *bnd_f0;               /* 19 * bnd_nb elements of the storage type ([q][t], t = second-pass index):
+                                   the Ladd inlets' constant populations, captured by the first step after
+                                   lattice_init or a stream call; required when bnd_nb > 0 */
+    int32_t bnd_slip;           /* 1: the lattice has FREE_SLIP cells (their mirrors read inlets'
+                                   post-collision populations, which are then stored) */
 } lbdem_lattice;
 
 typedef struct lbdem_grains {
@@ -216,7 +220,7 @@ int lbdem_abi_version(void);
 const char *lbdem_last_error(void);
 
 int lbdem_build_links(const int32_t *ct, int32_t nx, int32_t ny, int32_t nz, int32_t skip_inlet,
-                      uint32_t *links, uint8_t *row_simple, uint32_t *moving, void *stream);
+                      uint32_t *links, uint32_t *moving, void *stream);
 
 /* Deterministic list (lattice order) of the cells that the boundary pass
  * handles, from the link masks: first-pass cells (Zou-He, free-slip

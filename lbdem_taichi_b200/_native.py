@@ -40,9 +40,9 @@ class Lattice(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("storage", C.c_int32),
                 ("omega0", C.c_float), ("smag_cs", C.c_float), ("smag_mode", C.c_int32),
                 ("force_on", C.c_int32), ("force", C.c_float * 3), ("scale16", C.c_float),
-                ("f", vp * 2), ("rho", vp), ("vel", vp), ("aux", vp), ("links", vp), ("row_simple", vp),
+                ("f", vp * 2), ("rho", vp), ("vel", vp), ("aux", vp), ("links", vp),
                 ("status", vp), ("moving", vp), ("ct", vp), ("bnd_cells", vp), ("bnd_na", C.c_uint32),
-                ("bnd_nb", C.c_uint32)]
+                ("bnd_nb", C.c_uint32), ("bnd_f0", vp), ("bnd_slip", C.c_int32)]
 
 
 class Grains(C.Structure):
@@ -79,7 +79,7 @@ class Dem(C.Structure):
 EXPORTS = {
     "lbdem_abi_version": ([], C.c_int),
     "lbdem_last_error": ([], C.c_char_p),
-    "lbdem_build_links": ([vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp], C.c_int),
+    "lbdem_build_links": ([vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
     "lbdem_lattice_init": ([vp, C.c_int32, vp], C.c_int),
     "lbdem_psc_map": ([vp, vp, vp, vp], C.c_int),
     "lbdem_psc_step_f32": ([vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp], C.c_int),
@@ -102,7 +102,7 @@ EXPORTS = {
 _lib = None
 
 # kernels launched per call (for the launch count reported by bench.py)
-KERNELS_PER_CALL = {"lbdem_build_links": 2, "lbdem_lattice_init": 1, "lbdem_psc_map": 2,
+KERNELS_PER_CALL = {"lbdem_build_links": 1, "lbdem_lattice_init": 1, "lbdem_psc_map": 2,
                     "lbdem_psc_step_f32": 1, "lbdem_psc_step_f16": 1, "lbdem_psc_step_bf16": 1,
                     "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
                     "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2,

@@ -43,7 +43,6 @@ struct AdjArgs {
     float *bbar;                 // dL/dB per cell
     double *gbar;                // dL/dF (3)
     const uint32_t *links;
-    const uint8_t *row_simple;
     const uint32_t *key;
     const float *eps;
 };
@@ -67,8 +66,7 @@ __global__ void __launch_bounds__(256) k_psc_adjoint(const AdjArgs a) {
     const uint32_t rs = a.rs;
     const uint32_t r0 = row * rs;
     const uint32_t own = r0 + xslot((uint32_t)xc_, QB);
-    uint32_t lk = LINK_FLUID;
-    if (!a.row_simple[row]) lk = a.links[cell];
+    const uint32_t lk = a.links[cell];
     const bool act = inb && !(lk & LINK_SKIP);
 
     // forward streamed populations (deviation d = f - w) and where each came from
@@ -254,7 +252,7 @@ extern "C" int lbdem_psc_step_adjoint_f32(const lbdem_lattice *L, const lbdem_ps
                                           const float *lam_in, float *lam_out, float *bbar, double *gbar,
                                           const double *loss_dir, int32_t gather, int32_t seed, void *stream) {
     if (!L || !P || !f_prev || !bbar || !gbar || !loss_dir || (!seed && !lam_in) || (gather && !lam_out) ||
-        !L->links || !L->row_simple) {
+        !L->links) {
         set_error("psc_step_adjoint: bad arguments");
         return LBDEM_ERR_ARG;
     }
@@ -291,7 +289,6 @@ extern "C" int lbdem_psc_step_adjoint_f32(const lbdem_lattice *L, const lbdem_ps
     a.bbar = bbar;
     a.gbar = gbar;
     a.links = L->links;
-    a.row_simple = L->row_simple;
     a.key = P->key;
     a.eps = P->eps;
     int bx = ((L->nx + 31) / 32) * 32;

@@ -63,6 +63,7 @@ constexpr uint32_t LINK_DEFER = 1u << 23;    // Zou-He / exit / Ladd inlet cell,
 constexpr uint32_t LINK_PHASE_B = 1u << 24;  // deferred cell that reads its interior neighbour (exit, inlet)
 constexpr uint32_t LINK_KEEP = 1u << 25;     // interior neighbour of an exit or inlet: the step stores rho/u
 constexpr uint32_t LINK_INLET = 1u << 26;    // the cell is a Ladd velocity inlet (VEL_INLET_LADD)
+constexpr uint32_t LINK_SLIP_NB = 1u << 0;   // some neighbour is a free-slip wall (bit 0: no direction uses it)
 
 // Face of an open-boundary cell from its orientation bits, in the reference's
 // precedence LEFT, RIGHT, BOTTOM, TOP, BACK, FRONT (lbm_solver3d.py:522-527,

@@ -53,12 +53,14 @@ struct StepArgs {
     void *dst;
     void *aux;
     const uint32_t *links;
-    const uint8_t *row_simple;
     const uint32_t *moving;    // velocity-link bits per cell (VEL_LADD / VEL_INLET_LADD neighbours), or NULL
     float *rho;                // lagged density of moving-wall-adjacent cells (read, then rewritten);
                                // inlet densities; moments of LINK_KEEP cells
     float *vel;                // wall / inlet velocities (SoA planes); moments of LINK_KEEP cells
     const int32_t *ct;         // CellType (boundary pass only)
+    void *bnd_f0;              // populations of the second-pass cells, [q][t] (Ladd inlets' constant f)
+    uint32_t bnd_nb;           // second-pass cells (row length of bnd_f0)
+    int slip;                  // the lattice has free-slip cells (their mirrors read inlets' post-collision f)
     const uint32_t *key;
     const float *eps;          // smooth solid fraction per cell, or NULL (exact count in the key)
     const float4 *table;
@@ -474,8 +476,9 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
         for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ap[k * 32]);
     }
     uint32_t key = (a.key != nullptr) ? a.key[cell] : 0u;
-    uint32_t lk = LINK_FLUID;
-    if (!a.row_simple[row]) lk = a.links[cell];
+    // the link mask is read for every cell: a flag that skipped this load for
+    // plain blocks cost more (a dependent load before it) than the 4 B it saved
+    const uint32_t lk = a.links[cell];
     const bool act = inb && !(lk & (LINK_SKIP | LINK_DEFER));
     if (!act) key = 0u;
     if (GATHER && (lk & 0x7FFFEu)) {
@@ -538,8 +541,7 @@ __global__ void __launch_bounds__(256) k_stream_moments(const StepArgs a, float 
     if (x >= nx || y >= ny) return;
     const uint32_t row = (uint32_t)(z * ny + y);
     const uint32_t cell = row * (uint32_t)nx + (uint32_t)x;
-    uint32_t lk = LINK_FLUID;
-    if (!a.row_simple[row]) lk = a.links[cell];
+    const uint32_t lk = a.links[cell];
     if (lk & (LINK_SKIP | LINK_DEFER)) return;   // deferred cells: the boundary pass
     const T *src = static_cast<const T *>(a.src);
     T *dst = static_cast<T *>(a.dst);
@@ -604,8 +606,10 @@ __device__ __forceinline__ int comp(int q, int axis) { return axis == 0 ? cx(q) 
 // Post-stream populations of one cell with every neighbour rule of the
 // stream's first pass (lbm_solver3d.py:207-236; periodic wrap :308-342):
 // propagation, bounce-back, moving wall / Ladd inlet, specular free slip.
+// Directions in `unknown` (bit q) are left at zero: a wet-node rule overwrites them.
 template <typename T>
-__device__ __forceinline__ void gather_general(const StepArgs &a, int x, int y, int z, uint32_t cell, float h[Q]) {
+__device__ __forceinline__ void gather_general(const StepArgs &a, int x, int y, int z, uint32_t cell, uint32_t lk,
+                                               uint32_t unknown, float h[Q]) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t nc = a.nc;
     const T *src = static_cast<const T *>(a.src);
@@ -614,8 +618,36 @@ __device__ __forceinline__ void gather_general(const StepArgs &a, int x, int y, 
     const uint32_t own = slot(x, y, z);
     const int32_t prop = LBDEM_CT_FLUID | LBDEM_CT_VEL_ZOUHE | LBDEM_CT_VEL_EXIT | LBDEM_CT_PRE_ZOUHE;
     h[0] = Store<T>::widen(src[own]);
+    if (!(lk & LINK_SLIP_NB)) {
+        // no free-slip neighbour: the link mask holds every rule (as in the main kernel)
+        const uint32_t mv = (lk & LINK_MOVING) ? a.moving[cell] : 0u;
+#pragma unroll
+        for (int q = 1; q < Q; ++q) {
+            h[q] = 0.f;
+            if (unknown & (1u << q)) continue;
+            int xn = x - cx(q), yn = y - cy(q), zn = z - cz(q);
+            xn = xn >= nx ? 0 : (xn < 0 ? nx - 1 : xn);
+            yn = yn >= ny ? 0 : (yn < 0 ? ny - 1 : yn);
+            zn = zn >= nz ? 0 : (zn < 0 ? nz - 1 : zn);
+            if (lk & LINK_BB(q)) {
+                float v = Store<T>::widen(src[own + qinv(q) * 32]);
+                if (mv & LINK_BB(q)) {
+                    const size_t n = ((size_t)zn * ny + yn) * nx + xn;
+                    const float r = (a.links[n] & LINK_INLET) ? a.rho[n] : a.rho[cell];
+                    const float cu = cx(q) * a.vel[n] + cy(q) * a.vel[nc + n] + cz(q) * a.vel[2 * nc + n];
+                    v += 6.f * a.S * r * cu;
+                }
+                h[q] = v;
+            } else {
+                h[q] = Store<T>::widen(src[slot(xn, yn, zn) + q * 32]);
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
+        h[q] = 0.f;
+        if (unknown & (1u << q)) continue;
         int xn = x - cx(q), yn = y - cy(q), zn = z - cz(q);
         xn = xn >= nx ? 0 : (xn < 0 ? nx - 1 : xn);
         yn = yn >= ny ? 0 : (yn < 0 ? ny - 1 : yn);
@@ -660,41 +692,46 @@ __device__ __forceinline__ bool zou_he(const StepArgs &a, int32_t ct, bool press
                                        float u[3]) {
     int ax, s;
     if (!face_of(ct, ax, s)) return false;
-    float Dk = 0.f, Do = 0.f, T[3] = {0.f, 0.f, 0.f};
+    // scalars selected by the runtime axis (no runtime-indexed local arrays)
+    float Dk = 0.f, Do = 0.f, T0 = 0.f, T1 = 0.f, T2 = 0.f;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const float d = h[q] * (wq(q) * a.dec);
         const int ca = comp(q, ax);
         if (ca == 0) {
             Dk += d;
-            T[0] += (float)cx(q) * d;
-            T[1] += (float)cy(q) * d;
-            T[2] += (float)cz(q) * d;
+            T0 += (float)cx(q) * d;
+            T1 += (float)cy(q) * d;
+            T2 += (float)cz(q) * d;
         } else if (ca == -s) {
             Do += d;
         }
     }
-    float uu[3];
+    const float fs = (float)s;
+    float u0 = u[0], u1 = u[1], u2 = u[2];
+    float w0, w1, w2;   // velocity entering the unknowns
     if (pressure) {
-        u[ax] = (float)s * ((rho - 1.f) - Dk - 2.f * Do) / rho;
-        uu[0] = uu[1] = uu[2] = 0.f;
-        uu[ax] = u[ax];
+        const float un = fs * ((rho - 1.f) - Dk - 2.f * Do) / rho;
+        if (ax == 0) u0 = un; else if (ax == 1) u1 = un; else u2 = un;
+        w0 = ax == 0 ? un : 0.f;
+        w1 = ax == 1 ? un : 0.f;
+        w2 = ax == 2 ? un : 0.f;
     } else {
-        rho = (1.f + Dk + 2.f * Do) / (1.f - (float)s * u[ax]);
-        uu[0] = u[0]; uu[1] = u[1]; uu[2] = u[2];
+        const float ua = ax == 0 ? u0 : (ax == 1 ? u1 : u2);
+        rho = (1.f + Dk + 2.f * Do) / (1.f - fs * ua);
+        w0 = u0; w1 = u1; w2 = u2;
     }
-    float N[3];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) N[b] = 0.5f * T[b] - (pressure ? 0.f : rho * uu[b] * (1.f / 3.f));
+    u[0] = u0; u[1] = u1; u[2] = u2;
+    const float k3 = pressure ? 0.f : rho * (1.f / 3.f);
+    const float N0 = 0.5f * T0 - k3 * w0, N1 = 0.5f * T1 - k3 * w1, N2 = 0.5f * T2 - k3 * w2;
     const float k6 = 6.f * a.S * rho, k36 = 36.f * a.S;
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
         if (comp(q, ax) != s) continue;
-        const float cu = (float)cx(q) * uu[0] + (float)cy(q) * uu[1] + (float)cz(q) * uu[2];
-        float corr = 0.f;
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-            if (b != ax && comp(q, b) != 0) corr = (float)comp(q, b) * N[b];
+        const float cu = (float)cx(q) * w0 + (float)cy(q) * w1 + (float)cz(q) * w2;
+        // the tangential component of a diagonal unknown (zero on the axis direction)
+        const float corr = (ax != 0 ? (float)cx(q) * N0 : 0.f) + (ax != 1 ? (float)cy(q) * N1 : 0.f) +
+                           (ax != 2 ? (float)cz(q) * N2 : 0.f);
         h[q] = h[qinv(q)] + k6 * cu - k36 * corr;
     }
     return true;
@@ -730,10 +767,10 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
     int ax = 0, s = 0;
     size_t nbr = cell;
     if (face_of(ct, ax, s)) {
-        int m[3] = {x, y, z};
-        const int lim[3] = {nx, ny, nz};
-        m[ax] = min(max(m[ax] + s, 0), lim[ax] - 1);
-        nbr = ((size_t)m[2] * ny + m[1]) * nx + m[0];
+        const int mx = ax == 0 ? min(max(x + s, 0), nx - 1) : x;
+        const int my = ax == 1 ? min(max(y + s, 0), ny - 1) : y;
+        const int mz = ax == 2 ? min(max(z + s, 0), nz - 1) : z;
+        nbr = ((size_t)mz * ny + my) * nx + mx;
     }
     bool fields = false;   // (rho, u) come from the rule or the stored fields, not the moments
     bool collide_it = true;
@@ -743,10 +780,20 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
         // lives in the step's dst slot (gather) or src slot (post-stream input),
         // the post-collision populations in the other buffer.  Its density
         // follows the interior neighbour's (bc_ladd_inlet).
-        if (MODE != BND_STREAM) {
-            const T *f0 = MODE == BND_GATHER ? static_cast<const T *>(a.dst) + own : src + own;
+        // f: from the post-stream buffer in a step that reads populations in
+        // place (first step after initialize / a host read; also captured into
+        // bnd_f0), else from bnd_f0 (t - first second-pass index = row in bnd_f0)
+        const uint32_t tb = t >= a.bnd_nb ? 0u : t;
+        T *f0 = static_cast<T *>(a.bnd_f0);
+        if (MODE == BND_LOCAL) {
 #pragma unroll
-            for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(f0[q * 32]);
+            for (int q = 0; q < Q; ++q) {
+                h[q] = Store<T>::widen(src[own + q * 32]);
+                if (valid) f0[(size_t)q * a.bnd_nb + tb] = src[own + q * 32];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(f0[(size_t)q * a.bnd_nb + tb]);
         }
         if (MODE != BND_LOCAL) {
             rho = a.rho[nbr];
@@ -772,11 +819,17 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
         aux[0] = 0.f; aux[1] = u[0]; aux[2] = u[1]; aux[3] = u[2];
         fields = true;
     } else if (MODE != BND_LOCAL) {
-        gather_general<T>(a, x, y, z, cell, h);
+        uint32_t unknown = 0u;
+        if ((rule == WET_VEL_ZOUHE || rule == WET_PRE_ZOUHE) && s != 0) {
+#pragma unroll
+            for (int q = 1; q < Q; ++q)
+                if (comp(q, ax) == s) unknown |= 1u << q;
+        }
+        gather_general<T>(a, x, y, z, cell, lk, unknown, h);
         if (rule == WET_VEL_ZOUHE || rule == WET_PRE_ZOUHE) {
             const bool pressure = rule == WET_PRE_ZOUHE;
             if (zou_he(a, ct, pressure, h, rho, u) && valid) {
-                if (pressure) a.vel[(size_t)ax * nc + cell] = u[ax];
+                if (pressure) a.vel[(size_t)ax * nc + cell] = ax == 0 ? u[0] : (ax == 1 ? u[1] : u[2]);
                 else a.rho[cell] = rho;
             }
             fields = true;
@@ -803,7 +856,8 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
         }
     }
     if (MODE == BND_STREAM) {
-        if (valid && rule != WET_INLET) {   // an inlet's f already sits in dst
+        // an inlet's post-stream populations are its constant f
+        if (valid && (rule != WET_INLET || !(lk & LINK_MAP_SKIP))) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) dst[own + q * 32] = Store<T>::narrow(h[q]);
             if (rule == WET_EXIT && a.aux != nullptr) {
@@ -827,15 +881,10 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
     collide<float, SMAG, true>(
         a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { hout[q] = v; },
         [&](int k, float v) { aux[k] = v; }, [](float, float, float, float) {}, ovr);
-    if (act) {
+    // an inlet's post-collision populations are read only by free-slip mirrors
+    if (act && (rule != WET_INLET || a.slip)) {
 #pragma unroll
         for (int q = 0; q < Q; ++q) dst[own + q * 32] = Store<T>::narrow(hout[q]);
-        if (MODE == BND_GATHER && rule == WET_INLET) {
-            // the buffer read as src this step is the next step's dst: it takes f
-            T *keep = const_cast<T *>(src) + own;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) keep[q * 32] = Store<T>::narrow(h[q]);
-        }
     }
     if (act) {
         if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
@@ -933,7 +982,7 @@ __global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inle
             L |= LINK_BB(q) | LINK_MOVING;
             M |= LINK_BB(q);
         } else if ((ctn & LBDEM_CT_FREE_SLIP) && !sskip) {
-            L |= LINK_DEFER;
+            L |= LINK_DEFER | LINK_SLIP_NB;
         }
     }
     // interior neighbour of an exit / inlet face cell (the face's +s side;
@@ -953,22 +1002,6 @@ __global__ void k_links(const int32_t *ct, int nx, int ny, int nz, int skip_inle
     }
     links[c] = L;
     if (moving) moving[c] = M;
-}
-
-// row flag: every cell of the (y,z) row is an updated FLUID cell without
-// bounce-back links, so the step needs no per-cell link read there
-__global__ void k_rows(const uint32_t *links, int nx, int nrows, uint8_t *row_simple) {
-    const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    const int lane = threadIdx.x & 31;
-    if (row >= nrows) return;
-    const uint32_t bad_mask = LINK_SKIP | LINK_DEFER | LINK_KEEP | 0x7FFFEu;
-    int ok = 1;
-    for (int x = lane; x < nx; x += 32) {
-        const uint32_t L = links[(size_t)row * nx + x];
-        if ((L & bad_mask) || !(L & LINK_FLUID)) ok = 0;
-    }
-    ok = __all_sync(0xffffffffu, ok);
-    if (lane == 0) row_simple[row] = (uint8_t)ok;
 }
 
 // per-cell PSC fields from the owner keys (psclattice3d.py:45-52, 144-182)
@@ -1055,8 +1088,7 @@ __global__ void __launch_bounds__(256) k_stress(const StepArgs a, float *out) {
     if (x >= a.nx || y >= a.ny) return;
     const uint32_t row = (uint32_t)(z * a.ny + y);
     const uint32_t cell = row * (uint32_t)a.nx + (uint32_t)x;
-    uint32_t lk = LINK_FLUID;
-    if (!a.row_simple[row]) lk = a.links[cell];
+    const uint32_t lk = a.links[cell];
     if (lk & LINK_SKIP) return;
     const T *p = static_cast<const T *>(a.src) + (row * a.rs + xslot((uint32_t)x, QB));
     float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
@@ -1203,13 +1235,12 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
     a.aux = L->aux;
     a.keep_lag = L->aux != nullptr;
     a.links = L->links;
-    a.row_simple = L->row_simple;
     a.moving = L->moving;
     a.rho = L->rho;
     a.vel = L->vel;
     a.status = L->status;
-    if (!a.links || !a.row_simple || !a.status) {
-        set_error("links, row_simple and status are required");
+    if (!a.links || !a.status) {
+        set_error("links and status are required");
         return LBDEM_ERR_ARG;
     }
     if (L->smag_mode == LBDEM_SMAG_REFERENCE && !L->aux) {
@@ -1221,8 +1252,15 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
         return LBDEM_ERR_ARG;
     }
     a.ct = L->ct;
+    a.bnd_f0 = L->bnd_f0;
+    a.bnd_nb = L->bnd_nb;
+    a.slip = L->bnd_slip;
     if (L->bnd_na + L->bnd_nb > 0 && (!L->ct || !L->bnd_cells || !L->rho || !L->vel)) {
         set_error("open boundaries need ct, bnd_cells and the rho and vel fields");
+        return LBDEM_ERR_ARG;
+    }
+    if (L->bnd_nb > 0 && !L->bnd_f0) {
+        set_error("second-pass boundary cells need bnd_f0 (19 * bnd_nb elements)");
         return LBDEM_ERR_ARG;
     }
     return LBDEM_OK;
@@ -1446,16 +1484,14 @@ int lbdem_abi_version(void) { return LBDEM_ABI_VERSION; }
 const char *lbdem_last_error(void) { return g_err; }
 
 int lbdem_build_links(const int32_t *ct, int32_t nx, int32_t ny, int32_t nz, int32_t skip_inlet, uint32_t *links,
-                      uint8_t *row_simple, uint32_t *moving, void *stream) {
-    if (!ct || !links || !row_simple || nx <= 0 || ny <= 0 || nz <= 0) {
+                      uint32_t *moving, void *stream) {
+    if (!ct || !links || nx <= 0 || ny <= 0 || nz <= 0) {
         set_error("build_links: bad arguments");
         return LBDEM_ERR_ARG;
     }
     cudaStream_t st = (cudaStream_t)stream;
     const size_t nc = (size_t)nx * ny * nz;
     k_links<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(ct, nx, ny, nz, skip_inlet, links, moving);
-    const int nrows = ny * nz;
-    k_rows<<<(nrows + 7) / 8, 256, 0, st>>>(links, nx, nrows, row_simple);
     return check_launch("build_links");
 }
 

@@ -180,7 +180,8 @@ class LatticeEngine:
         self._bnd = None
         self._bnd_counts = torch.zeros(2, dtype=torch.int32, device=dev)
         self._bnd_scratch = None
-        self._rows = torch.zeros(self.Ny * self.Nz, dtype=torch.uint8, device=dev)
+        self._bnd_f0 = None
+        self._has_slip = False
         self._ct_dev = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
         self._sum_out = torch.zeros(4, dtype=torch.float64, device=dev)
@@ -223,7 +224,7 @@ class LatticeEngine:
         L.f[0], L.f[1] = N.ptr(self._f[0]), N.ptr(self._f[1])
         L.rho, L.vel = N.ptr(self._rho), N.ptr(self._vel)
         L.aux = N.ptr(self._aux)
-        L.links, L.row_simple = N.ptr(self._links), N.ptr(self._rows)
+        L.links = N.ptr(self._links)
         L.status = N.ptr(self._status)
         L.ct = N.ptr(self._ct_dev)
 
@@ -242,6 +243,7 @@ class LatticeEngine:
                              "direction (lbm_solver3d.py:230-236)")
         self._ct_dev.copy_(torch.from_numpy(from_ref(host.astype(np.int32)).reshape(-1)))
         self.has_open_boundaries = bool(np.bitwise_and(host, _OPEN).any())
+        self._has_slip = bool(slip.any())
         # moving walls and Ladd inlets: per-cell velocity-link bits, allocated on first use
         if np.bitwise_and(host, CellType.VEL_LADD | CellType.VEL_INLET_LADD).any():
             if self._moving is None:
@@ -254,8 +256,9 @@ class LatticeEngine:
     def _build_boundary_list(self):
         """Cells of the boundary pass, in lattice order (one host read of the counts)."""
         L = self._lat
+        L.bnd_slip = int(self._has_slip)
         if not self.has_open_boundaries:
-            L.bnd_cells, L.bnd_na, L.bnd_nb = None, 0, 0
+            L.bnd_cells, L.bnd_na, L.bnd_nb, L.bnd_f0 = None, 0, 0, None
             return
         if self._bnd_scratch is None:
             self._bnd_scratch = torch.zeros(2 * self.Ny * self.Nz, dtype=torch.int32, device="cuda")
@@ -272,6 +275,9 @@ class LatticeEngine:
                 break
             self._bnd = torch.zeros(na + nb, dtype=torch.int32, device="cuda")
         L.bnd_cells, L.bnd_na, L.bnd_nb = N.ptr(self._bnd), na, nb
+        if self._bnd_f0 is None or self._bnd_f0.shape[1] < max(nb, 1):
+            self._bnd_f0 = torch.zeros((19, max(nb, 1)), dtype=self._tdtype, device="cuda")
+        L.bnd_f0 = N.ptr(self._bnd_f0)
 
     def _push_rho(self, host):
         self._rho.copy_(torch.from_numpy(from_ref(host).reshape(-1).astype(np.float32)))
@@ -283,10 +289,13 @@ class LatticeEngine:
         # the Smagorinsky constant is a class attribute in the reference
         # (lbm_solver3d.py:97, read at :508); drivers may change it on the class or the instance
         self._lat.smag_cs = float(self.SmagorinskyConstant)
+        if self.CT._dirty and self._cur_kind == "fpc" and self._collided is None:
+            # the reference streams eagerly: a pending stream uses the old cell types
+            self._materialize()
         self.CT.flush()
         if self._links_dirty:
             N.call("lbdem_build_links", N.ptr(self._ct_dev), self.Nx, self.Ny, self.Nz, int(self.skip_inlet),
-                   N.ptr(self._links), N.ptr(self._rows), N.ptr(self._moving) if self._lat.moving else None,
+                   N.ptr(self._links), N.ptr(self._moving) if self._lat.moving else None,
                    N.stream_handle())
             self._build_boundary_list()
             self._links_dirty = False

@@ -40,7 +40,7 @@ def test_host_side_argument_checks():
     L = N.Lattice()
     L.nx, L.ny, L.nz = 8, 8, 8
     L.storage, L.omega0, L.scale16 = N.F32, 1.6, 1.0
-    L.links, L.row_simple, L.status = 8, 8, 8            # never dereferenced: checks come first
+    L.links, L.status = 8, 8                             # never dereferenced: checks come first
     assert lib.lbdem_psc_step_f32(C.byref(L), None, None, 0, 0, 1, None) == N.LBDEM_ERR_ARG   # src == dst
     L.smag_mode = N.SMAG_REFERENCE                       # needs the aux buffer
     assert lib.lbdem_psc_step_f32(C.byref(L), None, None, 0, 1, 1, None) == N.LBDEM_ERR_ARG

@@ -65,7 +65,7 @@ def test_noalloc_sums_reject_lattices_beyond_the_static_scratch():
     L.storage = N.F32
     L.omega0 = 1.6
     L.scale16 = 1.0
-    L.links, L.row_simple, L.status = 8, 8, 8      # never dereferenced: the size check comes first
+    L.links, L.status = 8, 8      # never dereferenced: the size check comes first
     rc = lib.lbdem_global_sums_f64_noalloc(C.byref(L), 0, 8, None)
     assert rc == N.LBDEM_ERR_ARG
     assert b"at most" in lib.lbdem_last_error()
