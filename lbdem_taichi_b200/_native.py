@@ -149,14 +149,10 @@ def _boundary_phases(arg):
 
 
 def call(name: str, *args):
-    psc = getattr(args[1], "_obj", None) if name == "lbdem_psc_map" else None
-    parity = psc.map_parity if isinstance(psc, Psc) else None
     rc = getattr(load(), name)(*args)
     _launches[0] += load().lbdem_dem_launches_last() if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
     if name in _BOUNDARY_CALLS:
         _launches[0] += _boundary_phases(args[0])
-    if parity is not None and psc.map_parity != parity:
-        _launches[0] += 1   # the map-reuse check ran
     if rc != LBDEM_OK:
         msg = load().lbdem_last_error().decode(errors="replace")
         raise LbdemError(f"{name} failed (code {rc}): {msg}")

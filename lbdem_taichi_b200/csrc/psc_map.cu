@@ -24,7 +24,8 @@ struct MapArgs {
     float4 *table;
     double *prev;
     int have_prev;
-    const uint32_t *moved;   // map reuse: any particle moved since the previous map (device word), or NULL
+    uint32_t *moved;         // map reuse: set when a particle moved since the previous map (device word), or NULL
+    uint32_t *moved_next;    // the next call's word, cleared here
     double *ff, *mf;
     int32_t *status;
 };
@@ -42,10 +43,24 @@ __device__ __forceinline__ void particle_lattice(const MapArgs &a, int g, double
 
 // Clear the cells claimed by the previous map (conservative shell), zero the
 // force accumulators, and write the FP32 particle table used by the step.
+// With map reuse (a.moved set) a particle clears its old shell only if its
+// lattice centre or mapping radius changed, and flags the change; the scatter
+// then re-claims every particle's cells if any particle moved and is skipped
+// otherwise.  That is exact: an unmoved particle's old keys are still its own
+// valid claims, and atomicMax against them gives the same winners.
 __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
     const int g = blockIdx.x;
-    const bool reuse = a.moved != nullptr && *a.moved == 0u;   // keys are exact already
-    if (a.have_prev && !reuse) {
+    bool clear = a.have_prev != 0;
+    if (a.moved != nullptr) {
+        if (g == 0 && threadIdx.x == 0) *a.moved_next = 0u;
+        double xc, yc, zc, r;
+        particle_lattice(a, g, xc, yc, zc, r);
+        const double *p = a.prev + 4 * (size_t)g;
+        const bool moved = !(xc == p[0] && yc == p[1] && zc == p[2] && r == p[3]);
+        if (moved && threadIdx.x == 0) *a.moved = 1u;
+        clear = clear && moved;
+    }
+    if (clear) {
         const double pxc = a.prev[4 * g], pyc = a.prev[4 * g + 1], pzc = a.prev[4 * g + 2];
         const double lim = a.prev[4 * g + 3] + HALF_DIAG + 1e-6;
         if (lim > 0.0) {
@@ -81,19 +96,6 @@ __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
         a.table[4 * g + 3] = make_float4((float)(a.omega[3 * g] * a.dt), (float)(a.omega[3 * g + 1] * a.dt),
                                          (float)(a.omega[3 * g + 2] * a.dt), 0.f);
     }
-}
-
-// Map reuse check: flag[0] = 1 when some particle's lattice centre or mapping
-// radius differs (bitwise) from the previous map's; flag[1] (the other call
-// parity's word) is cleared for the next call.
-__global__ void k_map_moved(const MapArgs a, uint32_t *flag, uint32_t *other) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g == 0) *other = 0u;
-    if (g >= a.n) return;
-    double xc, yc, zc, r;
-    particle_lattice(a, g, xc, yc, zc, r);
-    const double *p = a.prev + 4 * (size_t)g;
-    if (!(xc == p[0] && yc == p[1] && zc == p[2] && r == p[3])) *flag = 1u;
 }
 
 // Exact FP64 sub-cell test, in the reference's operation order
@@ -337,7 +339,7 @@ extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const 
         a.have_prev = 0;
         a.ff = G->force_fluid; a.mf = G->moment_fluid;
         a.status = L->status;
-        a.moved = nullptr;
+        a.moved = a.moved_next = nullptr;
         k_map_clear<<<G->n, 128, 0, st>>>(a);
         k_map_smooth<<<G->n, 256, 0, st>>>(a, reinterpret_cast<unsigned long long *>(scratch));
     }
@@ -374,14 +376,13 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     a.have_prev = P->have_prev;
     a.ff = G->force_fluid; a.mf = G->moment_fluid;
     a.status = L->status;
-    a.moved = nullptr;
+    a.moved = a.moved_next = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
     if (P->map_moved && P->map_reuse && P->have_prev) {
         // the previous exact map's centres are in prev: skip the remap when none changed
         const int par = P->map_parity & 1;
-        uint32_t *flag = P->map_moved + par;
-        k_map_moved<<<(G->n + 255) / 256, 256, 0, st>>>(a, flag, P->map_moved + (1 - par));
-        a.moved = flag;
+        a.moved = P->map_moved + par;
+        a.moved_next = P->map_moved + (1 - par);
         P->map_parity = 1 - par;
     }
     k_map_clear<<<G->n, 128, 0, st>>>(a);

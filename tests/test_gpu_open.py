@@ -189,5 +189,5 @@ def test_boundary_list_and_launch_count():
     lat.collide()
     lat.stream()
     lat.collide()
-    # map (reuse check + clear + scatter) + step (1) + two boundary passes, twice
-    assert N.launch_count() == 2 * (3 + 1 + 2)
+    # map (clear + scatter) + step (1) + two boundary passes, twice
+    assert N.launch_count() == 2 * (2 + 1 + 2)
