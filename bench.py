@@ -39,7 +39,7 @@ METRIC = "MLUPS & HBM-roofline % for D3Q19 PSC step, FP16-store vs FP32 at ≤1e
 BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}   # 19 reads + 19 writes of the storage type
 # DRAM read + write per cell of the step kernel, from the ncu capture of the
 # 128^3 case (see profiles/k_psc_step_128cube_full.md), scaled by the cells of a launch
-TRAFFIC_PER_CELL = {"f32": 177.4, "f16": 85.7, "bf16": 85.7}
+TRAFFIC_PER_CELL = {"f32": 175.7, "f16": 85.2, "bf16": 85.2}
 
 # Workloads (lattice units).  c2 is the headline configuration; c5 and c1 are
 # the large channel and the single settling sphere.  Parameters the workload
@@ -175,7 +175,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
