@@ -178,6 +178,14 @@ typedef struct lbdem_psc {
     uint32_t *map_moved;
     int32_t map_reuse;
     int32_t map_parity;
+    /* Periodic images (no counterpart in the reference, whose mapping never
+     * wraps, psclattice3d.py:102-108): wrap[a] = 1 maps a sphere that crosses
+     * the periodic faces of axis a also through its image shifted by
+     * period[a] lattice units (the DEM domain length / dx), and the step takes
+     * the minimum image for lever arms and solid velocities.  The exact map
+     * only; 0 everywhere reproduces the reference. */
+    int32_t wrap[3];
+    double period[3];
 } lbdem_psc;
 
 typedef struct lbdem_dem {
@@ -214,6 +222,11 @@ typedef struct lbdem_dem {
     int32_t *status;
     uint32_t *sync;        /* 2 words of caller-owned device memory for the grid barrier of the
                               single-launch sub-step kernel (reset by the library on every call) */
+    int32_t wrap_pairs;    /* 0: the reference's broad phase, which never proposes a pair across a
+                              periodic face (bpcd.py:154-194, cells not wrapped); 1: also probe the
+                              cells around a particle's periodic image when it lies within one
+                              broad-phase cell of a periodic face (needs every periodic length
+                              >= 4 cells; no counterpart in the reference) */
 } lbdem_dem;
 
 int lbdem_abi_version(void);

@@ -55,7 +55,8 @@ class Psc(C.Structure):
                 ("xmin", C.c_double), ("ymin", C.c_double), ("zmin", C.c_double),
                 ("skip_inlet", C.c_int32), ("key", vp), ("table", vp), ("prev", vp),
                 ("have_prev", C.c_int32), ("hydro_out", vp), ("eps", vp), ("map_moved", vp),
-                ("map_reuse", C.c_int32), ("map_parity", C.c_int32)]
+                ("map_reuse", C.c_int32), ("map_parity", C.c_int32), ("wrap", C.c_int32 * 3),
+                ("period", C.c_double * 3)]
 
 
 _DEM_PTRS = ("pos", "vel", "acc", "force", "quat", "omega", "omega_dot", "moment", "inertia", "mass", "radius",
@@ -73,7 +74,8 @@ class Dem(C.Structure):
                 ("wall_n", C.c_double * 18), ("wall_d", C.c_double * 6), ("wall_periodic", C.c_int32 * 6)] + \
                [(n, vp) for n in _DEM_PTRS] + \
                [("cell_cap", C.c_int32), ("cell_count", vp), ("cell_list", vp), ("acc_force", vp),
-                ("acc_moment", vp), ("parity", C.c_int32), ("status", vp), ("sync", vp)]
+                ("acc_moment", vp), ("parity", C.c_int32), ("status", vp), ("sync", vp),
+                ("wrap_pairs", C.c_int32)]
 
 
 EXPORTS = {

@@ -260,6 +260,10 @@ extern "C" int lbdem_psc_step_adjoint_f32(const lbdem_lattice *L, const lbdem_ps
         set_error("psc_step_adjoint: the adjoint covers FP32 storage with Smagorinsky off");
         return LBDEM_ERR_UNSUPPORTED;
     }
+    if (P->wrap[0] || P->wrap[1] || P->wrap[2]) {
+        set_error("psc_step_adjoint: the smooth solid fraction has no periodic images");
+        return LBDEM_ERR_UNSUPPORTED;
+    }
     if (L->moving || L->bnd_na + L->bnd_nb > 0) {
         set_error("psc_step_adjoint: the adjoint covers fixed walls only (no moving walls, inlets or open boundaries)");
         return LBDEM_ERR_UNSUPPORTED;

@@ -350,6 +350,8 @@ __device__ void wall_contact(const lbdem_dem &d, int i, const PState &P, int w, 
 // shuffles before one atomic per component.
 // One lane of the contact phase: lane k of particle i = tid / 8.  All 32 lanes
 // of the warp must call it together (shuffle reduction over groups of 8).
+// WRAP: also probe around the particle's periodic images (lbdem_dem.wrap_pairs).
+template <bool WRAP>
 __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *count, int tid) {
     const int i = tid >> 3, k = tid & 7;
     const bool act = i < d.n;
@@ -375,23 +377,47 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
         }
         const bool wall_lane = k < 6 && !d.wall_periodic[k];
         const int wact = wall_lane ? d.wcf_active[(size_t)i * 6 + k] : 0;
-        int ijk[3], dd[3];
-        ref_cell(d, P.p, ijk);
-        for (int a = 0; a < 3; ++a) {
-            const double center = (ijk[a] + 0.5) * d.cell_size + d.bp_min[a];
-            dd[a] = (P.p[a] > center) ? 1 : -1;
-        }
-        const int ox = (k == 1 || k == 5 || k == 6 || k == 7) ? dd[0] : 0;
-        const int oy = (k == 2 || k == 4 || k == 6 || k == 7) ? dd[1] : 0;
-        const int oz = (k == 3 || k == 4 || k == 5 || k == 7) ? dd[2] : 0;
-        const int c = cell_index(d, ijk[0] + ox, ijk[1] + oy, ijk[2] + oz);
-        if (c >= 0) {
-            const int n = min(count[c], d.cell_cap);
-            const int32_t *lst = d.cell_list + (size_t)c * d.cell_cap;
-            for (int t = 0; t < n; ++t) {
-                const int j = lst[t];
-                if (j > i) resolve_pair(d, i, P, n_i, hj, ha, j, Fi, Mi);
+        // the reference's probe of lane k around a position (own cell + octant)
+        auto probe = [&](const double q[3]) {
+            int ijk[3], dd[3];
+            ref_cell(d, q, ijk);
+            for (int a = 0; a < 3; ++a) {
+                const double center = (ijk[a] + 0.5) * d.cell_size + d.bp_min[a];
+                dd[a] = (q[a] > center) ? 1 : -1;
             }
+            const int ox = (k == 1 || k == 5 || k == 6 || k == 7) ? dd[0] : 0;
+            const int oy = (k == 2 || k == 4 || k == 6 || k == 7) ? dd[1] : 0;
+            const int oz = (k == 3 || k == 4 || k == 5 || k == 7) ? dd[2] : 0;
+            const int c = cell_index(d, ijk[0] + ox, ijk[1] + oy, ijk[2] + oz);
+            if (c >= 0) {
+                const int n = min(count[c], d.cell_cap);
+                const int32_t *lst = d.cell_list + (size_t)c * d.cell_cap;
+                for (int t = 0; t < n; ++t) {
+                    const int j = lst[t];
+                    if (j > i) resolve_pair(d, i, P, n_i, hj, ha, j, Fi, Mi);
+                }
+            }
+        };
+        if constexpr (!WRAP) {
+            probe(P.p);
+        } else {
+            // the particle and its periodic images when it lies within one
+            // broad-phase cell of a periodic face; the pair geometry is the
+            // minimum image either way (periodic_delta)
+            double sh[3] = {0.0, 0.0, 0.0};
+            int nimg[3] = {1, 1, 1};
+            for (int a = 0; a < 3; ++a) {
+                if (!d.periodic[a]) continue;
+                const double L = d.dom_max[a] - d.dom_min[a];
+                if (P.p[a] < d.dom_min[a] + d.cell_size) { sh[a] = L; nimg[a] = 2; }
+                else if (P.p[a] > d.dom_max[a] - d.cell_size) { sh[a] = -L; nimg[a] = 2; }
+            }
+            for (int ia = 0; ia < nimg[0]; ++ia)
+                for (int ja = 0; ja < nimg[1]; ++ja)
+                    for (int ka = 0; ka < nimg[2]; ++ka) {
+                        const double q[3] = {P.p[0] + ia * sh[0], P.p[1] + ja * sh[1], P.p[2] + ka * sh[2]};
+                        probe(q);
+                    }
         }
         if (wall_lane) {
             const int w = k;
@@ -420,8 +446,9 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
         }
 }
 
+template <bool WRAP>
 __global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArgs A) {
-    contact_lane(A.d, A.d.cell_count + (size_t)A.parity * A.ncell, blockIdx.x * blockDim.x + threadIdx.x);
+    contact_lane<WRAP>(A.d, A.d.cell_count + (size_t)A.parity * A.ncell, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // quaternion to rotation matrix (demsolver/utils.py:34-61)
@@ -594,6 +621,7 @@ __device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, in
 // barriers (barrier.cluster arrive.release / wait.acquire), which order the
 // global-memory writes of one phase before the reads of the next for every
 // thread of the cluster.  Same per-lane/per-particle code as the two kernels.
+template <bool WRAP>
 __global__ void __launch_bounds__(512) k_dem_cluster(const __grid_constant__ DemArgs A, int nsub) {
     cg::cluster_group cl = cg::this_cluster();
     const lbdem_dem &d = A.d;
@@ -603,7 +631,7 @@ __global__ void __launch_bounds__(512) k_dem_cluster(const __grid_constant__ Dem
     for (int s = 0; s < nsub; ++s) {
         const int parity = (A.parity + s) & 1;
         const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
-        for (int base = 0; base < nlanes; base += nthr) contact_lane(d, count, base + me);
+        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(d, count, base + me);
         cl.sync();
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
@@ -656,6 +684,7 @@ __device__ __forceinline__ void grid_barrier(uint32_t *sync, unsigned &gen, int3
     __syncthreads();
 }
 
+template <bool WRAP>
 __global__ void __launch_bounds__(128) k_dem_coop(const __grid_constant__ DemArgs A, int nsub) {
     const lbdem_dem &d = A.d;
     const int nthr = gridDim.x * blockDim.x;
@@ -665,7 +694,7 @@ __global__ void __launch_bounds__(128) k_dem_coop(const __grid_constant__ DemArg
     for (int s = 0; s < nsub; ++s) {
         const int parity = (A.parity + s) & 1;
         const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
-        for (int base = 0; base < nlanes; base += nthr) contact_lane(d, count, base + me);
+        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(d, count, base + me);
         grid_barrier(d.sync, gen, d.status);
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
@@ -689,6 +718,13 @@ static int check_dem(const lbdem_dem *D) {
         set_error("dem: bad broad-phase grid");
         return LBDEM_ERR_ARG;
     }
+    if (D->wrap_pairs)
+        for (int a = 0; a < 3; ++a)
+            if (D->periodic[a] && D->dom_max[a] - D->dom_min[a] < 4.0 * D->cell_size) {
+                // a pair must not be reachable both directly and through an image
+                set_error("dem: periodic images need every periodic length >= 4 broad-phase cells (axis %d)", a);
+                return LBDEM_ERR_ARG;
+            }
     return LBDEM_OK;
 }
 
@@ -733,11 +769,14 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     // (opt-in: it confines the contact phase to <= 16 SMs and measured slower
     // than two launches per sub-step spread over the whole GPU)
     const char *mode = getenv("LBDEM_DEM_KERNELS");
+    const bool wrap = D->wrap_pairs != 0;
+    auto *kcl = wrap ? k_dem_cluster<true> : k_dem_cluster<false>;
+    auto *kcoop = wrap ? k_dem_coop<true> : k_dem_coop<false>;
     if (mode && strcmp(mode, "cluster") == 0) {
         // one cluster of up to 16 CTAs x 512 threads, sized to the contact lanes
         int ncta = (int)((8ll * D->n + 511) / 512);
         ncta = ncta < 1 ? 1 : (ncta > 16 ? 16 : ncta);
-        cudaFuncSetAttribute(k_dem_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaFuncSetAttribute(kcl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         for (; ncta >= 1; ncta >>= 1) {
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(ncta, 1, 1);
@@ -752,12 +791,12 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
             cfg.attrs = attr;
             cfg.numAttrs = 1;
             int nclusters = 0;
-            if (cudaOccupancyMaxActiveClusters(&nclusters, k_dem_cluster, &cfg) != cudaSuccess || nclusters < 1) {
+            if (cudaOccupancyMaxActiveClusters(&nclusters, kcl, &cfg) != cudaSuccess || nclusters < 1) {
                 cudaGetLastError();
                 continue;
             }
             A.parity = D->parity;
-            if (cudaLaunchKernelEx(&cfg, k_dem_cluster, A, (int)nsub) == cudaSuccess) {
+            if (cudaLaunchKernelEx(&cfg, kcl, A, (int)nsub) == cudaSuccess) {
                 D->parity ^= (nsub & 1);
                 g_dem_launches = 1;
                 return check_launch("dem_substeps (cluster)");
@@ -772,7 +811,7 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dem_coop, 128, 0) == cudaSuccess &&
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kcoop, 128, 0) == cudaSuccess &&
             per_sm > 0) {
             // one resident wave must cover every contact lane: beyond that the
             // grid-stride loop serialises the phases' memory-latency chains and
@@ -784,7 +823,7 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
                 A.parity = D->parity;
                 int nsub_arg = nsub;
                 void *args[] = {&A, &nsub_arg};
-                if (cudaLaunchCooperativeKernel((void *)k_dem_coop, dim3(nb), dim3(128), args, 0, st) ==
+                if (cudaLaunchCooperativeKernel((void *)kcoop, dim3(nb), dim3(128), args, 0, st) ==
                     cudaSuccess) {
                     D->parity ^= (nsub & 1);
                     g_dem_launches = 1;
@@ -796,7 +835,8 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     }
     for (int s = 0; s < nsub; ++s) {
         A.parity = D->parity;
-        k_contacts<<<nb_con, 128, 0, st>>>(A);
+        if (wrap) k_contacts<true><<<nb_con, 128, 0, st>>>(A);
+        else k_contacts<false><<<nb_con, 128, 0, st>>>(A);
         k_integrate<<<nb_int, 128, 0, st>>>(A);
         D->parity ^= 1;
     }

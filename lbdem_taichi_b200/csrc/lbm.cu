@@ -72,6 +72,9 @@ struct StepArgs {
     uint32_t rs;               // population elements per row, nb * 19 * 32
     uint32_t ars;              // auxiliary elements per row, nb * 5 * 32
     int keep_lag;              // aux present: keep (drho, u, omega) of every collision (stress diagnostics)
+    float per_x, per_y, per_z;  // periodic-image lengths (lattice units) of the map, 0: no images
+    float iper_x, iper_y, iper_z;   // their reciprocals (0 without images)
+    int wrap_any;                   // some axis has periodic images
 };
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
@@ -132,9 +135,16 @@ struct CellForce {
     float rho;                     // density of the collision
 };
 
+// Minimum image of a lever-arm component along an axis mapped with periodic
+// images: r - P rint(r / P); with P = 1/P = 0 (no images) it returns r exactly.
+__device__ __forceinline__ float min_image(float r, float P, float iP) { return fmaf(-P, rintf(r * iP), r); }
+
 // PSC quantities of one cell owned by a particle (psclattice3d.py:144-182;
 // B from the current omega as hybridlattice.py:236-245): weight B, 3 u_s,
 // and the cell's force B (j - rho u_s) with its torque about the centre.
+// WRAP: the map has periodic images, lever arms take the minimum image (the
+// branch-free form is the identity where an axis has none).
+template <bool WRAP>
 __device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float eps_smooth, float om, float rho,
                                           float jx, float jy, float jz, int x, int y, int z, float &s3x, float &s3y,
                                           float &s3z, CellForce &cf) {
@@ -144,9 +154,14 @@ __device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float
     const float Bw = eps * taum * rcp_fast((1.f - eps) + taum);
     const float4 t0 = a.table[4 * cf.gid + 0], t1 = a.table[4 * cf.gid + 1];
     const float4 t2 = a.table[4 * cf.gid + 2], t3 = a.table[4 * cf.gid + 3];
-    const float rx = ((float)x - t0.x) - t1.x;
-    const float ry = ((float)y - t0.y) - t1.y;
-    const float rz = ((float)z - t0.z) - t1.z;
+    // integer part first (exact), then the fractional centre: image cells round as interior ones
+    float ix = (float)x - t0.x, iy = (float)y - t0.y, iz = (float)z - t0.z;
+    if constexpr (WRAP) {
+        ix = min_image(ix, a.per_x, a.iper_x);
+        iy = min_image(iy, a.per_y, a.iper_y);
+        iz = min_image(iz, a.per_z, a.iper_z);
+    }
+    const float rx = ix - t1.x, ry = iy - t1.y, rz = iz - t1.z;
     const float sx = t2.x + (t3.y * rz - t3.z * ry);
     const float sy = t2.y + (t3.z * rx - t3.x * rz);
     const float sz = t2.z + (t3.x * ry - t3.y * rx);
@@ -177,7 +192,7 @@ __device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float
 // OVR: collide with the density and velocity in ovr[4] = (rho, ux, uy, uz)
 // instead of the moments of h -- the boundary pass, where a wet-node rule set
 // them (the reference always collides with its rho / vel fields).
-template <class V, int SMAG, bool OVR = false, class Out, class AuxOut, class Macro>
+template <class V, int SMAG, bool OVR = false, bool WRAP = false, class Out, class AuxOut, class Macro>
 __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const bool act[], const int xs[], int y,
                                         int z, const V aux[5], bool psc, const uint32_t key[], const float eps[],
                                         CellForce cf[], Out &&out, AuxOut &&aux_out, Macro &&macro,
@@ -326,7 +341,7 @@ __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const b
     for (int i = 0; i < L::N; ++i) {
         if (key[i]) {
             float sx, sy, sz;
-            L::set(Bw, i, psc_cell(a, key[i], eps[i], L::get(om, i), L::get(rho, i), L::get(jx, i), L::get(jy, i),
+            L::set(Bw, i, psc_cell<WRAP>(a, key[i], eps[i], L::get(om, i), L::get(rho, i), L::get(jx, i), L::get(jy, i),
                                    L::get(jz, i), xs[i], y, z, sx, sy, sz, cf[i]));
             L::set(s3x, i, sx); L::set(s3y, i, sy); L::set(s3z, i, sz);
         }
@@ -427,7 +442,7 @@ __device__ __forceinline__ void moving_wall_terms(const StepArgs &a, uint32_t ce
     }
 }
 
-template <typename T, bool GATHER, int SMAG>
+template <typename T, bool GATHER, int SMAG, bool WRAP>
 __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -498,7 +513,7 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     const uint32_t keys[1] = {key};
     const float epss[1] = {(a.eps != nullptr && key) ? a.eps[cell] : 0.f};
     // post-collision values overwrite h[] and aux[] and are stored together
-    collide<float, SMAG>(
+    collide<float, SMAG, false, WRAP>(
         a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { h[q] = v; },
         [&](int k, float v) { aux[k] = v; },
         [&](float r, float u3x, float u3y, float u3z) {
@@ -878,7 +893,7 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
     const float epss[1] = {(a.eps != nullptr && key) ? a.eps[cell] : 0.f};
     const float ovr[4] = {rho, u[0], u[1], u[2]};
     float hout[Q];
-    collide<float, SMAG, true>(
+    collide<float, SMAG, true, true>(
         a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { hout[q] = v; },
         [&](int k, float v) { aux[k] = v; }, [](float, float, float, float) {}, ovr);
     // an inlet's post-collision populations are read only by free-slip mirrors
@@ -1031,7 +1046,15 @@ __global__ void k_decode(const StepArgs a, int smag_ref, int32_t *id, float *vol
     weight[c] = eps * taum / ((1.f - eps) + taum);
     const float4 t0 = a.table[4 * gid + 0], t1 = a.table[4 * gid + 1];
     const float4 t2 = a.table[4 * gid + 2], t3 = a.table[4 * gid + 3];
-    const float rx = ((float)x - t0.x) - t1.x, ry = ((float)y - t0.y) - t1.y, rz = ((float)z - t0.z) - t1.z;
+    // integer part first (exact), then the fractional centre: image cells round
+    // as interior ones; the minimum image only when the map has periodic images
+    float ix = (float)x - t0.x, iy = (float)y - t0.y, iz = (float)z - t0.z;
+    if (a.wrap_any) {
+        ix = min_image(ix, a.per_x, a.iper_x);
+        iy = min_image(iy, a.per_y, a.iper_y);
+        iz = min_image(iz, a.per_z, a.iper_z);
+    }
+    const float rx = ix - t1.x, ry = iy - t1.y, rz = iz - t1.z;
     velsolid[c] = t2.x + (t3.y * rz - t3.z * ry);
     velsolid[nc + c] = t2.y + (t3.z * rx - t3.x * rz);
     velsolid[2 * nc + c] = t2.z + (t3.x * ry - t3.y * rx);
@@ -1277,6 +1300,16 @@ static void launch_boundary(const lbdem_lattice *L, const StepArgs &a, cudaStrea
                                                                             L->bnd_nb);
 }
 
+static void set_periods(StepArgs &a, const lbdem_psc *P) {
+    a.per_x = P->wrap[0] ? (float)P->period[0] : 0.f;
+    a.per_y = P->wrap[1] ? (float)P->period[1] : 0.f;
+    a.per_z = P->wrap[2] ? (float)P->period[2] : 0.f;
+    a.iper_x = a.per_x > 0.f ? 1.f / a.per_x : 0.f;
+    a.iper_y = a.per_y > 0.f ? 1.f / a.per_y : 0.f;
+    a.iper_z = a.per_z > 0.f ? 1.f / a.per_z : 0.f;
+    a.wrap_any = a.per_x > 0.f || a.per_y > 0.f || a.per_z > 0.f;
+}
+
 static void step_geometry(const lbdem_lattice *L, dim3 &grid, dim3 &block, int nthreads = 256) {
     int bx = ((L->nx + 31) / 32) * 32;
     if (bx > nthreads) bx = nthreads;
@@ -1306,6 +1339,7 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
         a.key = P->key;
         a.eps = P->eps;
         a.table = (const float4 *)P->table;
+        set_periods(a, P);
         a.fscale = P->rho_unit * (P->dx * P->dx * P->dx * P->dx) / (P->dt * P->dt);
         a.tscale = a.fscale * P->dx;
         a.force_fluid = G->force_fluid;
@@ -1316,7 +1350,8 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
     step_geometry(L, grid, block, ONE_THREADS);
 #define LBDEM_STEP_CASE(G_, S_)                                        \
     do {                                                               \
-        k_psc_step<T, G_, S_><<<grid, block, 0, st>>>(a);              \
+        if (a.wrap_any) k_psc_step<T, G_, S_, true><<<grid, block, 0, st>>>(a);   \
+        else k_psc_step<T, G_, S_, false><<<grid, block, 0, st>>>(a);            \
         launch_boundary<T, S_, G_ ? BND_GATHER : BND_LOCAL>(L, a, st); \
     } while (0)
     if (gather) {
@@ -1392,6 +1427,7 @@ static int launch_decode(const lbdem_lattice *L, const lbdem_psc *P, int32_t *id
         a.key = P->key;
         a.eps = P->eps;
         a.table = (const float4 *)P->table;
+        set_periods(a, P);
     }
     const unsigned nb = (unsigned)((a.nc + 255) / 256);
     k_decode<T><<<nb, 256, 0, st>>>(a, L->smag_mode == LBDEM_SMAG_REFERENCE, id, vf, w, vs);

@@ -28,6 +28,8 @@ struct MapArgs {
     uint32_t *moved_next;    // the next call's word, cleared here
     double *ff, *mf;
     int32_t *status;
+    int wrap[3];             // periodic images along each axis (0: the reference's unwrapped mapping)
+    double period[3];        // image shift per axis, lattice units
 };
 
 constexpr double HALF_DIAG = 0.8660254037844386;  // 0.5 * sqrt(3.0), psclattice3d.py:111
@@ -41,6 +43,17 @@ __device__ __forceinline__ void particle_lattice(const MapArgs &a, int g, double
     r = (a.radius[g] - 0.5 * a.dx) / a.dx;
 }
 
+// Image shifts of a sphere centre c with reach `reach` along `axis`: 0, plus
+// one periodic image when the sphere crosses a periodic face (wrap mode).
+__device__ __forceinline__ int image_shifts(const MapArgs &a, int axis, double c, double reach, int n, double sh[2]) {
+    sh[0] = 0.0;
+    sh[1] = 0.0;
+    if (!a.wrap[axis]) return 1;
+    if (c - reach < 0.0) { sh[1] = a.period[axis]; return 2; }
+    if (c + reach > (double)(n - 1)) { sh[1] = -a.period[axis]; return 2; }
+    return 1;
+}
+
 // Clear the cells claimed by the previous map (conservative shell), zero the
 // force accumulators, and write the FP32 particle table used by the step.
 // With map reuse (a.moved set) a particle clears its old shell only if its
@@ -48,6 +61,9 @@ __device__ __forceinline__ void particle_lattice(const MapArgs &a, int g, double
 // then re-claims every particle's cells if any particle moved and is skipped
 // otherwise.  That is exact: an unmoved particle's old keys are still its own
 // valid claims, and atomicMax against them gives the same winners.
+// WRAP: the map has periodic images (a.wrap); without them the image loops
+// compile to the single original sphere.
+template <bool WRAP>
 __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
     const int g = blockIdx.x;
     bool clear = a.have_prev != 0;
@@ -60,9 +76,20 @@ __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
         if (moved && threadIdx.x == 0) *a.moved = 1u;
         clear = clear && moved;
     }
-    if (clear) {
-        const double pxc = a.prev[4 * g], pyc = a.prev[4 * g + 1], pzc = a.prev[4 * g + 2];
-        const double lim = a.prev[4 * g + 3] + HALF_DIAG + 1e-6;
+    const double lim = a.prev[4 * g + 3] + HALF_DIAG + 1e-6;
+    double shx[2], shy[2], shz[2];
+    shx[0] = shy[0] = shz[0] = 0.0;
+    int nix = clear ? 1 : 0, niy = 1, niz = 1;
+    if constexpr (WRAP) {
+        if (clear) {
+            nix = image_shifts(a, 0, a.prev[4 * g], lim, a.nx, shx);
+            niy = image_shifts(a, 1, a.prev[4 * g + 1], lim, a.ny, shy);
+            niz = image_shifts(a, 2, a.prev[4 * g + 2], lim, a.nz, shz);
+        }
+    }
+    for (int im = 0; im < nix * niy * niz; ++im) {
+        const double pxc = a.prev[4 * g] + shx[im % nix], pyc = a.prev[4 * g + 1] + shy[(im / nix) % niy];
+        const double pzc = a.prev[4 * g + 2] + shz[im / (nix * niy)];
         if (lim > 0.0) {
             const int x0 = max(0, (int)floor(pxc - lim)), x1 = min(a.nx - 1, (int)ceil(pxc + lim));
             const int y0 = max(0, (int)floor(pyc - lim)), y1 = min(a.ny - 1, (int)ceil(pyc + lim));
@@ -122,133 +149,146 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
 //     for these offsets), so counts are bit-exact.
 constexpr int MAP_CHUNK = 2048;
 
+template <bool WRAP>
 __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32; w = global cell index
     __shared__ int s_amb[MAP_CHUNK];      // partial cells needing the exact recount (index into s_off)
     __shared__ int s_n, s_na;
     if (a.moved != nullptr && *a.moved == 0u) return;   // reuse: nothing moved, keys unchanged
     const int g = blockIdx.x;
-    double xc, yc, zc, r;
-    particle_lattice(a, g, xc, yc, zc, r);
+    double xc0, yc0, zc0, r;
+    particle_lattice(a, g, xc0, yc0, zc0, r);
     if (threadIdx.x == 0) {
-        a.prev[4 * g] = xc; a.prev[4 * g + 1] = yc; a.prev[4 * g + 2] = zc; a.prev[4 * g + 3] = r;
+        a.prev[4 * g] = xc0; a.prev[4 * g + 1] = yc0; a.prev[4 * g + 2] = zc0; a.prev[4 * g + 3] = r;
     }
     const double t_out = r + HALF_DIAG, t_in = r - HALF_DIAG;
     if (!(t_out > 0.0)) return;
-    const int x0 = max(0, (int)floor(xc - t_out)), x1 = min(a.nx - 1, (int)ceil(xc + t_out));
-    const int y0 = max(0, (int)floor(yc - t_out)), y1 = min(a.ny - 1, (int)ceil(yc + t_out));
-    const int z0 = max(0, (int)floor(zc - t_out)), z1 = min(a.nz - 1, (int)ceil(zc + t_out));
-    const int ex = x1 - x0 + 1, ey = y1 - y0 + 1, ez = z1 - z0 + 1;
-    if (ex <= 0 || ey <= 0 || ez <= 0) return;
-    const uint32_t gbits = 0xFFFFFFu - (uint32_t)g;
-    const float out2 = (float)(t_out * t_out), marg_o = (float)(1e-4 * (1.0 + t_out * t_out));
-    const float in2 = t_in > 0.0 ? (float)(t_in * t_in) : -1.f, marg_i = (float)(1e-4 * (1.0 + t_in * t_in));
-    const double rr = r > 0.0 ? r * r : 0.0;
-    const float band = (float)(1e-4 * (1.0 + rr));
-    const float lo = (float)rr - band, hi = (float)rr + band;
-    const unsigned tot = (unsigned)ex * (unsigned)ey * (unsigned)ez;
-    // this thread's first cell, then advance by blockDim cells with carries
-    const unsigned bd = blockDim.x;
-    const int adx = (int)(bd % (unsigned)ex), ady = (int)((bd / (unsigned)ex) % (unsigned)ey);
-    const int adz = (int)(bd / ((unsigned)ex * (unsigned)ey));
-    int ix = (int)(threadIdx.x % (unsigned)ex), jy = (int)((threadIdx.x / (unsigned)ex) % (unsigned)ey);
-    int kz = (int)(threadIdx.x / ((unsigned)ex * (unsigned)ey));
-    for (unsigned base = 0; base < tot; base += MAP_CHUNK) {
-        if (threadIdx.x == 0) s_n = s_na = 0;
-        __syncthreads();
-        const unsigned lim = min(tot, base + MAP_CHUNK);
-        for (unsigned t = base + threadIdx.x; t < lim; t += bd) {
-            const int i = x0 + ix, j = y0 + jy, k = z0 + kz;
-            ix += adx; jy += ady; kz += adz;
-            if (ix >= ex) { ix -= ex; ++jy; }
-            if (jy >= ey) { jy -= ey; ++kz; }
-            const float fx = (float)(xc - (double)i), fy = (float)(yc - (double)j), fz = (float)(zc - (double)k);
-            const float d2 = (fx * fx + fy * fy) + fz * fz;
-            if (d2 > out2 + marg_o) continue;                 // certainly dist >= t_out
-            const unsigned c = ((unsigned)k * (unsigned)a.ny + (unsigned)j) * (unsigned)a.nx + (unsigned)i;
-            if (a.links[c] & LINK_MAP_SKIP) continue;
-            int full;
-            if (d2 < in2 - marg_i) {
-                full = 1;                                     // certainly dist <= t_in
-            } else if (d2 < out2 - marg_o && d2 > in2 + marg_i) {
-                full = 0;                                     // certainly partial
-            } else {
-                const double ddx = xc - i, ddy = yc - j, ddz = zc - k;
-                const double dist = sqrt((ddx * ddx + ddy * ddy) + ddz * ddz);
-                if (dist >= t_out) continue;
-                full = dist <= t_in;
+    // the sphere, and in wrap mode its periodic images (block-uniform loop)
+    double shx[2], shy[2], shz[2];
+    shx[0] = shy[0] = shz[0] = 0.0;
+    int nix = 1, niy = 1, niz = 1;
+    if constexpr (WRAP) {
+        nix = image_shifts(a, 0, xc0, t_out, a.nx, shx);
+        niy = image_shifts(a, 1, yc0, t_out, a.ny, shy);
+        niz = image_shifts(a, 2, zc0, t_out, a.nz, shz);
+    }
+    for (int im = 0; im < nix * niy * niz; ++im) {
+        const double xc = xc0 + shx[im % nix], yc = yc0 + shy[(im / nix) % niy], zc = zc0 + shz[im / (nix * niy)];
+        const int x0 = max(0, (int)floor(xc - t_out)), x1 = min(a.nx - 1, (int)ceil(xc + t_out));
+        const int y0 = max(0, (int)floor(yc - t_out)), y1 = min(a.ny - 1, (int)ceil(yc + t_out));
+        const int z0 = max(0, (int)floor(zc - t_out)), z1 = min(a.nz - 1, (int)ceil(zc + t_out));
+        const int ex = x1 - x0 + 1, ey = y1 - y0 + 1, ez = z1 - z0 + 1;
+        if (ex <= 0 || ey <= 0 || ez <= 0) continue;
+        const uint32_t gbits = 0xFFFFFFu - (uint32_t)g;
+        const float out2 = (float)(t_out * t_out), marg_o = (float)(1e-4 * (1.0 + t_out * t_out));
+        const float in2 = t_in > 0.0 ? (float)(t_in * t_in) : -1.f, marg_i = (float)(1e-4 * (1.0 + t_in * t_in));
+        const double rr = r > 0.0 ? r * r : 0.0;
+        const float band = (float)(1e-4 * (1.0 + rr));
+        const float lo = (float)rr - band, hi = (float)rr + band;
+        const unsigned tot = (unsigned)ex * (unsigned)ey * (unsigned)ez;
+        // this thread's first cell, then advance by blockDim cells with carries
+        const unsigned bd = blockDim.x;
+        const int adx = (int)(bd % (unsigned)ex), ady = (int)((bd / (unsigned)ex) % (unsigned)ey);
+        const int adz = (int)(bd / ((unsigned)ex * (unsigned)ey));
+        int ix = (int)(threadIdx.x % (unsigned)ex), jy = (int)((threadIdx.x / (unsigned)ex) % (unsigned)ey);
+        int kz = (int)(threadIdx.x / ((unsigned)ex * (unsigned)ey));
+        for (unsigned base = 0; base < tot; base += MAP_CHUNK) {
+            if (threadIdx.x == 0) s_n = s_na = 0;
+            __syncthreads();
+            const unsigned lim = min(tot, base + MAP_CHUNK);
+            for (unsigned t = base + threadIdx.x; t < lim; t += bd) {
+                const int i = x0 + ix, j = y0 + jy, k = z0 + kz;
+                ix += adx; jy += ady; kz += adz;
+                if (ix >= ex) { ix -= ex; ++jy; }
+                if (jy >= ey) { jy -= ey; ++kz; }
+                const float fx = (float)(xc - (double)i), fy = (float)(yc - (double)j), fz = (float)(zc - (double)k);
+                const float d2 = (fx * fx + fy * fy) + fz * fz;
+                if (d2 > out2 + marg_o) continue;                 // certainly dist >= t_out
+                const unsigned c = ((unsigned)k * (unsigned)a.ny + (unsigned)j) * (unsigned)a.nx + (unsigned)i;
+                if (a.links[c] & LINK_MAP_SKIP) continue;
+                int full;
+                if (d2 < in2 - marg_i) {
+                    full = 1;                                     // certainly dist <= t_in
+                } else if (d2 < out2 - marg_o && d2 > in2 + marg_i) {
+                    full = 0;                                     // certainly partial
+                } else {
+                    const double ddx = xc - i, ddy = yc - j, ddz = zc - k;
+                    const double dist = sqrt((ddx * ddx + ddy * ddy) + ddz * ddz);
+                    if (dist >= t_out) continue;
+                    full = dist <= t_in;
+                }
+                if (full) {
+                    atomicMax(a.key + c, KEY_FULL | gbits);
+                } else if (r > 0.0) {
+                    const int slot = atomicAdd(&s_n, 1);
+                    s_off[slot] = make_float4(fx, fy, fz, __uint_as_float(c));
+                }
             }
-            if (full) {
-                atomicMax(a.key + c, KEY_FULL | gbits);
-            } else if (r > 0.0) {
-                const int slot = atomicAdd(&s_n, 1);
-                s_off[slot] = make_float4(fx, fy, fz, __uint_as_float(c));
+            __syncthreads();
+            const int n = s_n;
+            // 2a. one thread per partial cell: 25 columns x 5 sub-points from the
+            // squared per-axis offsets (-fmad=false: each product and sum rounded
+            // as in the per-point expression).  Cells with a sub-point inside the
+            // rounding band go to a second list for an exact warp recount.
+            for (int e = threadIdx.x; e < n; e += bd) {
+                const float4 o = s_off[e];
+                float ox2[5], oy2[5], oz2[5];
+    #pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    const float sh = 0.4f - 0.2f * (float)m;
+                    const float ox = o.x + sh, oy = o.y + sh, oz = o.z + sh;
+                    ox2[m] = ox * ox;
+                    oy2[m] = oy * oy;
+                    oz2[m] = oz * oz;
+                }
+                int cnt = 0, amb = 0;
+    #pragma unroll
+                for (int ia = 0; ia < 5; ++ia)
+    #pragma unroll
+                    for (int ja = 0; ja < 5; ++ja) {
+                        const float sxy = ox2[ia] + oy2[ja];
+    #pragma unroll
+                        for (int kk = 0; kk < 5; ++kk) {
+                            const float sd = sxy + oz2[kk];
+                            cnt += sd < lo;
+                            amb |= (sd >= lo) & (sd <= hi);
+                        }
+                    }
+                if (amb) {
+                    s_amb[atomicAdd(&s_na, 1)] = e;
+                } else if (cnt > 0) {   // eps = 0 never beats the empty cell (strict >)
+                    atomicMax(a.key + __float_as_uint(o.w), ((uint32_t)cnt << 24) | gbits);
+                }
             }
-        }
-        __syncthreads();
-        const int n = s_n;
-        // 2a. one thread per partial cell: 25 columns x 5 sub-points from the
-        // squared per-axis offsets (-fmad=false: each product and sum rounded
-        // as in the per-point expression).  Cells with a sub-point inside the
-        // rounding band go to a second list for an exact warp recount.
-        for (int e = threadIdx.x; e < n; e += bd) {
-            const float4 o = s_off[e];
-            float ox2[5], oy2[5], oz2[5];
-#pragma unroll
-            for (int m = 0; m < 5; ++m) {
-                const float sh = 0.4f - 0.2f * (float)m;
-                const float ox = o.x + sh, oy = o.y + sh, oz = o.z + sh;
-                ox2[m] = ox * ox;
-                oy2[m] = oy * oy;
-                oz2[m] = oz * oz;
-            }
-            int cnt = 0, amb = 0;
-#pragma unroll
-            for (int ia = 0; ia < 5; ++ia)
-#pragma unroll
-                for (int ja = 0; ja < 5; ++ja) {
-                    const float sxy = ox2[ia] + oy2[ja];
-#pragma unroll
+            __syncthreads();
+            // 2b. cells with near-surface sub-points: one warp per cell, lane
+            // (ii, jj) < 25 tests its column of five; points inside the band are
+            // re-tested with the reference's exact FP64 expression
+            const int na = s_na;
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+            const int ii = lane / 5, jj = lane % 5;
+            const float oxl = 0.4f - 0.2f * (float)ii, oyl = 0.4f - 0.2f * (float)jj;
+            for (int e2 = warp; e2 < na; e2 += nwarp) {
+                const float4 o = s_off[s_amb[e2]];
+                const unsigned c = __float_as_uint(o.w);
+                int cnt = 0;
+                if (lane < 25) {
+                    const int i = (int)(c % (unsigned)a.nx), j = (int)((c / (unsigned)a.nx) % (unsigned)a.ny);
+                    const int k = (int)(c / ((unsigned)a.nx * (unsigned)a.ny));
+                    const float ox = o.x + oxl, oy = o.y + oyl;
+                    const float sxy = ox * ox + oy * oy;
                     for (int kk = 0; kk < 5; ++kk) {
-                        const float sd = sxy + oz2[kk];
-                        cnt += sd < lo;
-                        amb |= (sd >= lo) & (sd <= hi);
+                        const float oz = o.z + (0.4f - 0.2f * (float)kk);
+                        const float sd = sxy + oz * oz;
+                        if (sd < lo) ++cnt;
+                        else if (sd <= hi) cnt += subcell_inside_exact(xc, yc, zc, i, j, k, ii, jj, kk, r);
                     }
                 }
-            if (amb) {
-                s_amb[atomicAdd(&s_na, 1)] = e;
-            } else if (cnt > 0) {   // eps = 0 never beats the empty cell (strict >)
-                atomicMax(a.key + __float_as_uint(o.w), ((uint32_t)cnt << 24) | gbits);
+                cnt = __reduce_add_sync(0xffffffffu, cnt);
+                if (lane == 0 && cnt > 0) atomicMax(a.key + c, ((uint32_t)cnt << 24) | gbits);
             }
+            __syncthreads();
         }
-        __syncthreads();
-        // 2b. cells with near-surface sub-points: one warp per cell, lane
-        // (ii, jj) < 25 tests its column of five; points inside the band are
-        // re-tested with the reference's exact FP64 expression
-        const int na = s_na;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-        const int ii = lane / 5, jj = lane % 5;
-        const float oxl = 0.4f - 0.2f * (float)ii, oyl = 0.4f - 0.2f * (float)jj;
-        for (int e2 = warp; e2 < na; e2 += nwarp) {
-            const float4 o = s_off[s_amb[e2]];
-            const unsigned c = __float_as_uint(o.w);
-            int cnt = 0;
-            if (lane < 25) {
-                const int i = (int)(c % (unsigned)a.nx), j = (int)((c / (unsigned)a.nx) % (unsigned)a.ny);
-                const int k = (int)(c / ((unsigned)a.nx * (unsigned)a.ny));
-                const float ox = o.x + oxl, oy = o.y + oyl;
-                const float sxy = ox * ox + oy * oy;
-                for (int kk = 0; kk < 5; ++kk) {
-                    const float oz = o.z + (0.4f - 0.2f * (float)kk);
-                    const float sd = sxy + oz * oz;
-                    if (sd < lo) ++cnt;
-                    else if (sd <= hi) cnt += subcell_inside_exact(xc, yc, zc, i, j, k, ii, jj, kk, r);
-                }
-            }
-            cnt = __reduce_add_sync(0xffffffffu, cnt);
-            if (lane == 0 && cnt > 0) atomicMax(a.key + c, ((uint32_t)cnt << 24) | gbits);
-        }
-        __syncthreads();
     }
 }
 
@@ -316,6 +356,10 @@ extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const 
         set_error("psc_map_smooth: bad arguments (key, eps, table, links and scratch are required)");
         return LBDEM_ERR_ARG;
     }
+    if (P->wrap[0] || P->wrap[1] || P->wrap[2]) {
+        set_error("psc_map_smooth: the smooth solid fraction has no periodic images");
+        return LBDEM_ERR_UNSUPPORTED;
+    }
     if (G->n > 0xFFFFFF) {
         set_error("psc_map_smooth: %d particles exceed the 2^24-1 owner-key range", G->n);
         return LBDEM_ERR_ARG;
@@ -340,7 +384,9 @@ extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const 
         a.ff = G->force_fluid; a.mf = G->moment_fluid;
         a.status = L->status;
         a.moved = a.moved_next = nullptr;
-        k_map_clear<<<G->n, 128, 0, st>>>(a);
+        a.wrap[0] = a.wrap[1] = a.wrap[2] = 0;   // the smooth map has no periodic images
+        a.period[0] = a.period[1] = a.period[2] = 0.0;
+        k_map_clear<false><<<G->n, 128, 0, st>>>(a);
         k_map_smooth<<<G->n, 256, 0, st>>>(a, reinterpret_cast<unsigned long long *>(scratch));
     }
     k_map_smooth_decode<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(
@@ -377,6 +423,14 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     a.ff = G->force_fluid; a.mf = G->moment_fluid;
     a.status = L->status;
     a.moved = a.moved_next = nullptr;
+    for (int t = 0; t < 3; ++t) {
+        a.wrap[t] = P->wrap[t] != 0;
+        a.period[t] = P->period[t];
+        if (a.wrap[t] && !(P->period[t] >= 1.0)) {
+            set_error("psc_map: periodic images need a positive period (axis %d)", t);
+            return LBDEM_ERR_ARG;
+        }
+    }
     cudaStream_t st = (cudaStream_t)stream;
     if (P->map_moved && P->map_reuse && P->have_prev) {
         // the previous exact map's centres are in prev: skip the remap when none changed
@@ -385,8 +439,13 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
         a.moved_next = P->map_moved + (1 - par);
         P->map_parity = 1 - par;
     }
-    k_map_clear<<<G->n, 128, 0, st>>>(a);
-    k_map_scatter<<<G->n, 256, 0, st>>>(a);
+    if (a.wrap[0] || a.wrap[1] || a.wrap[2]) {
+        k_map_clear<true><<<G->n, 128, 0, st>>>(a);
+        k_map_scatter<true><<<G->n, 256, 0, st>>>(a);
+    } else {
+        k_map_clear<false><<<G->n, 128, 0, st>>>(a);
+        k_map_scatter<false><<<G->n, 256, 0, st>>>(a);
+    }
     P->have_prev = 1;
     return check_launch("psc_map");
 }

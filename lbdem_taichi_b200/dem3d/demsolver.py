@@ -111,7 +111,18 @@ class GrainField:
 
 
 class DEMSolver:
-    def __init__(self, config: DEMSolverConfig):
+    """``compat="reference"`` (default) reproduces the reference: the broad
+    phase never proposes a pair across a periodic face and PSC lattices built
+    on this solver map a sphere without its periodic images (bpcd.py:154-194,
+    psclattice3d.py:102-108).  ``compat="wrapped"`` adds the periodic images in
+    both (contacts across periodic faces; spheres that cross them are mapped on
+    both sides, with minimum-image lever arms); every periodic length must span
+    at least four broad-phase cells (4 x 4 r_max)."""
+
+    def __init__(self, config: DEMSolverConfig, *, compat: str = "reference"):
+        if compat not in ("reference", "wrapped"):
+            raise ValueError('compat must be "reference" or "wrapped"')
+        self.compat = compat
         self.config = config
         self.contact_model = None
         self.n = 0
@@ -255,6 +266,7 @@ class DEMSolver:
         d.wall_n[:] = [float(v) for nrm in cfg.wall_normals for v in nrm]
         d.wall_d[:] = [float(v) for v in cfg.wall_distances]
         d.wall_periodic[:] = [int(b == cfg.BOUNDARY_TYPE_PERIODIC) for b in cfg.boundaryType]
+        d.wrap_pairs = int(self.compat == "wrapped")
         self._set_materials(density)
         for name, ten in (("pos", t["position"]), ("vel", t["velocity"]), ("acc", t["acceleration"]),
                           ("force", t["force"]), ("quat", t["quaternion"]), ("omega", t["omega"]),

@@ -67,6 +67,16 @@ class PSCLattice3D(LatticeEngine):
         p.map_moved = N.ptr(self._map_moved)
         p.map_reuse, p.map_parity = 0, 0
         self._mapped_epoch = -1
+        # periodic images of the DEM solver's "wrapped" mode: image shift = domain length / dx
+        if getattr(demslover, "compat", "reference") == "wrapped":
+            if solid_fraction == "smooth":
+                raise ValueError('the smooth solid fraction has no periodic images (DEMSolver compat="wrapped")')
+            dom = demslover.config.domain
+            lens = (dom.xmax - dom.xmin, dom.ymax - dom.ymin, dom.zmax - dom.zmin)
+            for a in range(3):
+                per = demslover.config.boundaryType[2 * a] == demslover.config.BOUNDARY_TYPE_PERIODIC
+                p.wrap[a] = int(per)
+                p.period[a] = float(lens[a] / dx) if per else 0.0
         if solid_fraction == "smooth":
             self._eps = torch.zeros(nc, dtype=torch.float32, device=dev)
             self._map_scratch = torch.zeros(nc, dtype=torch.int64, device=dev)

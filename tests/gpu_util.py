@@ -9,13 +9,13 @@ from lbdem_taichi_b200.dem3d.demsolver import DEMSolver
 
 
 def make_dem(domain, dt, gravity, contact, radius, mass, pos, vel, omega=None, periodic=(False, False, False),
-             E=1e5, nu=0.3, wall_E=1e5, wall_nu=0.3, max_coord=16, model="hertz", freeze=None):
+             E=1e5, nu=0.3, wall_E=1e5, wall_nu=0.3, max_coord=16, model="hertz", freeze=None, compat="reference"):
     cfg = DEMSolverConfig(domain=DomainBounds(*[float(v) for v in domain]), dt=dt, gravity=Vector3(*gravity),
                           contact_model=contact)
     cfg.set_particle_properties(elastic_modulus=E, poisson_ratio=nu, max_coordinate_number=max_coord)
     cfg.set_wall_properties(elastic_modulus=wall_E, poisson_ratio=wall_nu)
     cfg.set_periodic_boundaries(*periodic)
-    dem = DEMSolver(cfg)
+    dem = DEMSolver(cfg, compat=compat)
     dmin = Vector3(domain[0], domain[2], domain[4])
     dmax = Vector3(domain[1], domain[3], domain[5])
     dem.init_particle_arrays(radius, mass, pos, vel, dmin, dmax)
