@@ -106,6 +106,14 @@ __device__ __forceinline__ float sqrt_fast(float x) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
 
+// Packed FP32 pairs (B200 f32x2 FMA / add): two independent FP32 operations per
+// issued instruction, each lane rounded exactly as its scalar form.  The
+// collision runs its per-direction-pair arithmetic two pairs at a time.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
 template <class V> struct Lanes;
 template <> struct Lanes<float> {
     static constexpr int N = 1;
@@ -316,14 +324,34 @@ __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const b
         const V ks = om * SR;
         const V Vx = vfma(ks, u3x, rg3x), Vy = vfma(ks, u3y, rg3y), Vz = vfma(ks, u3z, rg3z);
         out(0, vfma(omc, h[0], vfma(k2, nU, k0)));
+        if constexpr (L::N == 1) {
+            // pairs (0,1) (2,3) (4,5) (6,7) packed, pair 8 scalar
+            const float2 k2_ = f2(k2, k2), k0_ = f2(k0, k0), nU_ = f2(nU, nU), omc_ = f2(omc, omc);
 #pragma unroll
-        for (int p = 0; p < 9; ++p) {
-            const int q = 2 * p + 1;
-            const V v = cdot(q, u3x, u3y, u3z);
-            const V cv = cdot(q, Vx, Vy, Vz);
+            for (int p = 0; p < 8; p += 2) {
+                const int q = 2 * p + 1, r = q + 2;
+                const float2 v = f2(cdot(q, u3x, u3y, u3z), cdot(r, u3x, u3y, u3z));
+                const float2 cv = f2(cdot(q, Vx, Vy, Vz), cdot(r, Vx, Vy, Vz));
+                const float2 e = fma2(k2_, fma2(v, v, nU_), k0_);
+                const float2 hp = fma2(omc_, f2(h[q], h[r]), add2(e, cv));
+                const float2 hm = fma2(omc_, f2(h[q + 1], h[r + 1]), sub2(e, cv));
+                out(q, hp.x); out(q + 1, hm.x); out(r, hp.y); out(r + 1, hm.y);
+            }
+            const V v = cdot(17, u3x, u3y, u3z);
+            const V cv = cdot(17, Vx, Vy, Vz);
             const V e = vfma(k2, vfma(v, v, nU), k0);
-            out(q, vfma(omc, h[q], e + cv));
-            out(q + 1, vfma(omc, h[q + 1], e - cv));
+            out(17, vfma(omc, h[17], e + cv));
+            out(18, vfma(omc, h[18], e - cv));
+        } else {
+#pragma unroll
+            for (int p = 0; p < 9; ++p) {
+                const int q = 2 * p + 1;
+                const V v = cdot(q, u3x, u3y, u3z);
+                const V cv = cdot(q, Vx, Vy, Vz);
+                const V e = vfma(k2, vfma(v, v, nU), k0);
+                out(q, vfma(omc, h[q], e + cv));
+                out(q + 1, vfma(omc, h[q + 1], e - cv));
+            }
         }
         return;
     }
