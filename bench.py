@@ -7,7 +7,13 @@ Gaussian velocities (sigma 1e-3); density ratio 2.0; Hertz-Mindlin contacts
 (E=1e5, nu=0.3, restitution 0.9, friction 0.3); uniform body force 1e-6 (x) on
 fluid and particles; tau=0.6 with Smagorinsky Cs=0.1 (reference lagged form);
 DEM sub-cycled 10x per lattice step.  A step = map particles -> fused PSC
-collide-stream with force reduction -> 10 DEM sub-steps.
+collide-stream with force reduction -> 10 DEM sub-steps.  `value` times the
+product's PSCLattice3D.run(), which pipelines the steps where that is faster
+(the x-blocks no particle can reach are stepped while the DEM and the next map
+run on a second stream; identical results; `pipelined` says which form ran);
+`sequential` and `phases_ms` time the plain collide/stream/DEM loop, and the
+roofline is the fused step kernel's.  --no-pipeline times the plain loop as
+`value`.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16]
     python bench.py --workload c5        # 512x512x256 channel, 20000 spheres, LES
@@ -272,6 +278,28 @@ def run_gpu(args):
     barrier()
     # with a flush the step time is the sum of the per-step events (map to end of DEM)
     ms = t0.elapsed_time(t1) if flush is None else sum(a.elapsed_time(c) for a, _, c in ev_phase)
+    ms_seq = ms
+    # ---- the product's run(): the sequential loop above, pipelined (the blocks
+    # no particle can reach are stepped while the DEM and the next map run on a
+    # second stream).  Needs inputs larger than L2 (no flush between steps).
+    pipelined = flush is None and not args.no_pipeline
+    if pipelined:
+        lat.run(40, SUB)          # run()'s automatic choice is measured here, outside the timed region
+        pipelined = bool(lat._pipeline_choice)
+        torch.cuda.synchronize()
+        Nat.reset_launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        with Clocks(local) as clk:
+            t0.record(st)
+            cpu0 = time.perf_counter()
+            lat.run(args.steps, SUB)
+            t1.record(st)
+            cpu_launch_ms = (time.perf_counter() - cpu0) * 1e3 / args.steps
+            torch.cuda.synchronize()
+        launches = Nat.launch_count()
+        barrier()
+        ms = t0.elapsed_time(t1)
     ms_t = torch.tensor([ms], device="cuda")
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -340,6 +368,10 @@ def run_gpu(args):
         "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 2 * NP * 3 * 8,
                 "d2h_bytes_per_step": 4 * NP * 3 * 8},
         "gpu_launches": launches,
+        "pipelined": pipelined,
+        "pipeline_probe_ms": [round(v, 4) for v in lat._pipeline_probe] if lat._pipeline_probe else None,
+        "sequential": {"value": round(world * cells * args.steps / (ms_seq * 1e-3) / 1e6, 2),
+                       "ms_per_step": round(ms_seq / args.steps, 4)},
         "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4), f"dem_{SUB}_substeps": round(dem_ms, 4),
                       "host_launch_per_step": round(cpu_launch_ms, 4)},
         "clocks": clocks,
@@ -535,6 +567,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-pipeline", action="store_true", help="time the sequential loop (collide, stream, DEM)")
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--size", type=int, default=0, help="cube edge override; only for small profiling cases")
     ap.add_argument("--particles", type=int, default=0, help="particle count override; only for profiling")

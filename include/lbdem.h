@@ -81,6 +81,8 @@ extern "C" {
 #define LBDEM_ST_GID_OVERFLOW 32u    /* more than 2^24-1 particles in the PSC map */
 #define LBDEM_ST_CELL_OVERFLOW 64u   /* a broad-phase cell holds more than cell_cap particles */
 #define LBDEM_ST_WAIT_TIMEOUT 128u   /* a bounded wait for an asynchronous copy gave up */
+#define LBDEM_ST_PIPELINE_MARGIN 256u /* a particle moved farther in one step than the margin a
+                                         pipelined step assumed (lbdem_psc_near_blocks) */
 
 /* storage forms */
 #define LBDEM_F32 0
@@ -186,6 +188,12 @@ typedef struct lbdem_psc {
      * only; 0 everywhere reproduces the reference. */
     int32_t wrap[3];
     double period[3];
+    /* Pipelined stepping (lbdem_psc_near_blocks / lbdem_psc_step_phase): the
+     * DEM's periodic axes, and the largest distance (lattice units) a particle
+     * may move between two maps; the map flags LBDEM_ST_PIPELINE_MARGIN when a
+     * particle moved farther (minimum image on periodic axes).  0 = no check. */
+    int32_t periodic[3];
+    double disp_limit;
 } lbdem_psc;
 
 typedef struct lbdem_dem {
@@ -261,6 +269,33 @@ int lbdem_psc_step_f16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
                        int32_t dst, int32_t gather, void *stream);
 int lbdem_psc_step_bf16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
                         int32_t dst, int32_t gather, void *stream);
+
+/* Pipelined stepping (no counterpart in the reference: a scheduling of the
+ * same step).  The fused step of a coupled lattice only needs the particle map
+ * in the x-blocks (32 cells of a row) that some particle can reach; all other
+ * blocks can be streamed and collided while the DEM sub-steps and the next
+ * map still run on another stream.
+ *
+ * lbdem_psc_near_blocks: mask[(z*Ny + y)*NB + x/32] = 1 for every x-block
+ * holding a cell within (mapping reach + margin) of a particle's current
+ * centre, or of its periodic image along P->periodic axes (mask: Ny*Nz*NB
+ * bytes of scratch); then the list `blocks` (Ny*Nz*NB uint32) holds the
+ * counts[0] far blocks (ascending) from its start and the counts[1] near
+ * blocks (ascending) packed at its end.  counts: device uint32 array of
+ * 2 + 2 * ceil(Ny*Nz*NB / 1024) words (the tail is scratch).
+ *
+ * lbdem_psc_step_phase: one gathered step (gather = 1) restricted to
+ *   phase 1: the far blocks, as pure fluid (no keys read, no force);
+ *   phase 2: the near blocks, with the map and force reduction, then the
+ *            boundary pass.
+ * Phase 1 and phase 2 together equal lbdem_psc_step_* when no particle moved
+ * farther than the margin between the lists and the map (checked by
+ * lbdem_psc_map when P->disp_limit > 0).  Periodic images (P->wrap) are not
+ * supported here (LBDEM_ERR_UNSUPPORTED). */
+int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, double margin,
+                          uint8_t *mask, uint32_t *blocks, uint32_t *counts, void *stream);
+int lbdem_psc_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
+                         int32_t dst, int32_t phase, const uint32_t *blocks, const uint32_t *counts, void *stream);
 
 /* Stream the post-collision populations of f[src] into f[dst] and write
  * rho/vel of FLUID cells (the reference's stream(), no collision). */

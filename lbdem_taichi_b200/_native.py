@@ -16,6 +16,7 @@ LBDEM_ERR_ARG, LBDEM_ERR_LAUNCH, LBDEM_ERR_UNSUPPORTED = 1, 2, 3
 ST_NAN, ST_RHO, ST_VELMAX = 1, 2, 4
 ST_CONTACT_OVERFLOW, ST_GRID_OVERFLOW, ST_GID_OVERFLOW, ST_CELL_OVERFLOW = 8, 16, 32, 64
 ST_WAIT_TIMEOUT = 128
+ST_PIPELINE_MARGIN = 256
 ABI_VERSION = 2        # LBDEM_ABI_VERSION of include/lbdem.h
 F32, F16, BF16 = 0, 1, 2
 SMAG_OFF, SMAG_REFERENCE, SMAG_LOCAL = 0, 1, 2
@@ -31,6 +32,7 @@ STATUS_TEXT = {
     ST_GID_OVERFLOW: "too many particles for the PSC owner key",
     ST_CELL_OVERFLOW: "a broad-phase cell holds more particles than its list capacity",
     ST_WAIT_TIMEOUT: "a bounded wait for an asynchronous copy gave up",
+    ST_PIPELINE_MARGIN: "a particle moved farther in one step than the pipelined run's margin",
 }
 
 vp = C.c_void_p
@@ -56,7 +58,7 @@ class Psc(C.Structure):
                 ("skip_inlet", C.c_int32), ("key", vp), ("table", vp), ("prev", vp),
                 ("have_prev", C.c_int32), ("hydro_out", vp), ("eps", vp), ("map_moved", vp),
                 ("map_reuse", C.c_int32), ("map_parity", C.c_int32), ("wrap", C.c_int32 * 3),
-                ("period", C.c_double * 3)]
+                ("period", C.c_double * 3), ("periodic", C.c_int32 * 3), ("disp_limit", C.c_double)]
 
 
 _DEM_PTRS = ("pos", "vel", "acc", "force", "quat", "omega", "omega_dot", "moment", "inertia", "mass", "radius",
@@ -99,6 +101,8 @@ EXPORTS = {
     "lbdem_psc_step_adjoint_f32": ([vp, vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp], C.c_int),
     "lbdem_psc_force_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
     "lbdem_boundary_cells": ([vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_uint32, vp, vp, vp], C.c_int),
+    "lbdem_psc_near_blocks": ([vp, vp, vp, C.c_double, vp, vp, vp, vp], C.c_int),
+    "lbdem_psc_step_phase": ([vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
 }
 
 _lib = None
@@ -109,7 +113,7 @@ KERNELS_PER_CALL = {"lbdem_build_links": 1, "lbdem_lattice_init": 1, "lbdem_psc_
                     "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
                     "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2,
                     "lbdem_psc_map_smooth": 3, "lbdem_stress": 1, "lbdem_psc_step_adjoint_f32": 1, "lbdem_psc_force_adjoint": 1,
-                    "lbdem_boundary_cells": 3}
+                    "lbdem_boundary_cells": 3, "lbdem_psc_near_blocks": 4, "lbdem_psc_step_phase": 1}
 # calls followed by the boundary pass: one more kernel per non-empty phase
 _BOUNDARY_CALLS = ("lbdem_psc_step_f32", "lbdem_psc_step_f16", "lbdem_psc_step_bf16", "lbdem_stream_moments")
 _launches = [0]
@@ -153,7 +157,7 @@ def _boundary_phases(arg):
 def call(name: str, *args):
     rc = getattr(load(), name)(*args)
     _launches[0] += load().lbdem_dem_launches_last() if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
-    if name in _BOUNDARY_CALLS:
+    if name in _BOUNDARY_CALLS or (name == "lbdem_psc_step_phase" and args[5] == 2):
         _launches[0] += _boundary_phases(args[0])
     if rc != LBDEM_OK:
         msg = load().lbdem_last_error().decode(errors="replace")

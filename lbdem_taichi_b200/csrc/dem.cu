@@ -833,11 +833,15 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
         }
         cudaGetLastError();
     }
+    // two launches per sub-step, in 64-thread blocks: each block's registers
+    // (~10 K) fit in the room one retiring block of the fused step frees, so
+    // the sub-steps can interleave with a step running on another stream
+    const int nb_con64 = (int)((8ll * D->n + 63) / 64), nb_int64 = 2 * nb_int;
     for (int s = 0; s < nsub; ++s) {
         A.parity = D->parity;
-        if (wrap) k_contacts<true><<<nb_con, 128, 0, st>>>(A);
-        else k_contacts<false><<<nb_con, 128, 0, st>>>(A);
-        k_integrate<<<nb_int, 128, 0, st>>>(A);
+        if (wrap) k_contacts<true><<<nb_con64, 64, 0, st>>>(A);
+        else k_contacts<false><<<nb_con64, 64, 0, st>>>(A);
+        k_integrate<<<nb_int64, 64, 0, st>>>(A);
         D->parity ^= 1;
     }
     g_dem_launches = 2 * nsub;

@@ -75,6 +75,10 @@ struct StepArgs {
     float per_x, per_y, per_z;  // periodic-image lengths (lattice units) of the map, 0: no images
     float iper_x, iper_y, iper_z;   // their reciprocals (0 without images)
     int wrap_any;                   // some axis has periodic images
+    const uint32_t *blist;          // pipelined step: x-block ids (row * nb + x/32) of this phase
+    const uint32_t *bcount;         // their number (device)
+    int bfrom_end;                  // the list is read from the end of blist (near blocks)
+    uint32_t nblocks;               // rows * nb
 };
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
@@ -470,12 +474,26 @@ __device__ __forceinline__ void moving_wall_terms(const StepArgs &a, uint32_t ce
     }
 }
 
-template <typename T, bool GATHER, int SMAG, bool WRAP>
+// LISTED (pipelined stepping): one-dimensional blocks whose warps take the
+// x-blocks of a compact list (blist / bcount), so every warp of a CTA has
+// work; otherwise the grid covers the lattice.  A warp is one x-block.
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool LISTED = false>
 __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
+    int x, y, z;
+    if constexpr (LISTED) {
+        const uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (w >= *a.bcount) return;   // warp-uniform
+        const uint32_t id = a.blist[a.bfrom_end ? a.nblocks - *a.bcount + w : w];
+        const uint32_t r = id / a.nb;
+        x = (int)((id - r * a.nb) * 32u + (threadIdx.x & 31u));
+        y = (int)(r % (uint32_t)ny);
+        z = (int)(r / (uint32_t)ny);
+    } else {
+        x = blockIdx.x * blockDim.x + threadIdx.x;
+        y = blockIdx.y * blockDim.y + threadIdx.y;
+        z = blockIdx.z;
+    }
     const bool inb = (x < nx) && (y < ny);
     const int xc_ = inb ? x : 0, yc_ = inb ? y : 0;
     const uint32_t row = (uint32_t)(z * ny + yc_);
@@ -1395,6 +1413,65 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
     return check_launch("psc_step");
 }
 
+// Pipelined stepping: phase 1 = far blocks as pure fluid (keys ignored, no
+// force), phase 2 = near blocks with the map, then the boundary pass.
+template <typename T>
+static int launch_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int src, int dst,
+                             int phase, const uint32_t *blocks, const uint32_t *counts, cudaStream_t st) {
+    if (phase != 1 && phase != 2) {
+        set_error("psc_step_phase: phase must be 1 or 2");
+        return LBDEM_ERR_ARG;
+    }
+    if (!blocks || !counts || (phase == 2 && !(P && G && G->n > 0))) {
+        set_error("psc_step_phase: needs the block lists (and for phase 2 the particles)");
+        return LBDEM_ERR_ARG;
+    }
+    if (P && (P->wrap[0] || P->wrap[1] || P->wrap[2])) {
+        set_error("psc_step_phase: periodic images are not supported in pipelined stepping");
+        return LBDEM_ERR_UNSUPPORTED;
+    }
+    StepArgs a;
+    int rc = fill_args(L, a);
+    if (rc) return rc;
+    if (src < 0 || src > 1 || dst < 0 || dst > 1 || src == dst) {
+        set_error("src/dst must be 0/1 and distinct");
+        return LBDEM_ERR_ARG;
+    }
+    a.src = L->f[src];
+    a.dst = L->f[dst];
+    a.blist = blocks;
+    a.bcount = counts + (phase == 2 ? 1 : 0);
+    a.bfrom_end = phase == 2;
+    a.nblocks = a.nb * (uint32_t)L->ny * (uint32_t)L->nz;
+    if (phase == 2) {
+        if (!P->key || !P->table || !G->force_fluid || !G->moment_fluid) {
+            set_error("PSC step needs key, table and force accumulators");
+            return LBDEM_ERR_ARG;
+        }
+        a.key = P->key;
+        a.eps = P->eps;
+        a.table = (const float4 *)P->table;
+        set_periods(a, P);
+        a.fscale = P->rho_unit * (P->dx * P->dx * P->dx * P->dx) / (P->dt * P->dt);
+        a.tscale = a.fscale * P->dx;
+        a.force_fluid = G->force_fluid;
+        a.moment_fluid = G->moment_fluid;
+        a.hydro_out = P->hydro_out;
+    }
+    // the list length is on the device: cover every block; CTAs past it leave at once
+    const dim3 block(ONE_THREADS, 1, 1), grid((a.nblocks + ONE_THREADS / 32 - 1) / (ONE_THREADS / 32), 1, 1);
+#define LBDEM_PHASE_CASE(S_)                                                              \
+    do {                                                                                  \
+        k_psc_step<T, true, S_, false, true><<<grid, block, 0, st>>>(a);                  \
+        if (phase == 2) launch_boundary<T, S_, BND_GATHER>(L, a, st);                     \
+    } while (0)
+    if (L->smag_mode == LBDEM_SMAG_OFF) LBDEM_PHASE_CASE(LBDEM_SMAG_OFF);
+    else if (L->smag_mode == LBDEM_SMAG_REFERENCE) LBDEM_PHASE_CASE(LBDEM_SMAG_REFERENCE);
+    else LBDEM_PHASE_CASE(LBDEM_SMAG_LOCAL);
+#undef LBDEM_PHASE_CASE
+    return check_launch("psc_step_phase");
+}
+
 template <typename T>
 static int launch_stream_moments(const lbdem_lattice *L, int src, int dst, cudaStream_t st) {
     StepArgs a;
@@ -1605,6 +1682,19 @@ int lbdem_psc_step_bf16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_
                         int32_t gather, void *stream) {
     if (!L || L->storage != LBDEM_BF16) { set_error("psc_step_bf16: storage mismatch"); return LBDEM_ERR_ARG; }
     return launch_step<__nv_bfloat16>(L, P, G, src, dst, gather, (cudaStream_t)stream);
+}
+
+int lbdem_psc_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
+                         int32_t dst, int32_t phase, const uint32_t *blocks, const uint32_t *counts, void *stream) {
+    if (!L) return LBDEM_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (L->storage) {
+        case LBDEM_F32: return launch_step_phase<float>(L, P, G, src, dst, phase, blocks, counts, st);
+        case LBDEM_F16: return launch_step_phase<__half>(L, P, G, src, dst, phase, blocks, counts, st);
+        case LBDEM_BF16: return launch_step_phase<__nv_bfloat16>(L, P, G, src, dst, phase, blocks, counts, st);
+    }
+    set_error("unknown storage form %d", L->storage);
+    return LBDEM_ERR_ARG;
 }
 
 int lbdem_stream_moments(const lbdem_lattice *L, int32_t src, int32_t dst, void *stream) {

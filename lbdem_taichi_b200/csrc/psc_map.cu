@@ -10,6 +10,7 @@
 // pre-classification with a proven margin decides the clear cases, so the 5^3
 // sub-sample counts match the reference bit for bit at FP32 speed.
 #include <math.h>
+#include <string.h>
 
 #include "common.cuh"
 
@@ -30,6 +31,8 @@ struct MapArgs {
     int32_t *status;
     int wrap[3];             // periodic images along each axis (0: the reference's unwrapped mapping)
     double period[3];        // image shift per axis, lattice units
+    int periodic[3];         // DEM periodic axes (pipelined stepping: near-block images, displacement check)
+    double disp_limit;       // largest allowed centre displacement between two maps (0: no check)
 };
 
 constexpr double HALF_DIAG = 0.8660254037844386;  // 0.5 * sqrt(3.0), psclattice3d.py:111
@@ -67,6 +70,16 @@ template <bool WRAP>
 __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
     const int g = blockIdx.x;
     bool clear = a.have_prev != 0;
+    if (a.disp_limit > 0.0 && a.have_prev && threadIdx.x == 0) {
+        // pipelined stepping: the near-block mask assumed at most disp_limit
+        double xc, yc, zc, r;
+        particle_lattice(a, g, xc, yc, zc, r);
+        double d[3] = {xc - a.prev[4 * g], yc - a.prev[4 * g + 1], zc - a.prev[4 * g + 2]};
+        for (int t = 0; t < 3; ++t)
+            if (a.periodic[t] && a.period[t] > 0.0) d[t] -= a.period[t] * rint(d[t] / a.period[t]);
+        if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] > a.disp_limit * a.disp_limit)
+            atomicOr(a.status, (int)LBDEM_ST_PIPELINE_MARGIN);
+    }
     if (a.moved != nullptr) {
         if (g == 0 && threadIdx.x == 0) *a.moved_next = 0u;
         double xc, yc, zc, r;
@@ -293,6 +306,55 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
 }
 
 
+// Near-block mask for pipelined stepping: every x-block (32 cells of a row)
+// holding a cell within the particle's mapping reach plus `margin` of its
+// lattice centre (per row: the chord of that ball), and
+// of the centre's periodic image when the sphere's reach crosses a periodic
+// face (a particle that crosses the face reappears there).  One block per
+// particle; the stores are idempotent.
+__global__ void __launch_bounds__(128) k_near_blocks(const MapArgs a, double margin, uint8_t *near) {
+    const int g = blockIdx.x;
+    double xc0, yc0, zc0, r;
+    particle_lattice(a, g, xc0, yc0, zc0, r);
+    const double reach = r + HALF_DIAG + margin;
+    if (!(reach > 0.0)) return;
+    const int nb = (a.nx + 31) / 32;
+    const int n3[3] = {a.nx, a.ny, a.nz};
+    const double c3[3] = {xc0, yc0, zc0};
+    double sh[3][2];
+    int ni[3];
+    for (int t = 0; t < 3; ++t) {
+        sh[t][0] = sh[t][1] = 0.0;
+        ni[t] = 1;
+        if (a.periodic[t] && a.period[t] > 0.0) {
+            if (c3[t] - reach < 0.0) { sh[t][1] = a.period[t]; ni[t] = 2; }
+            else if (c3[t] + reach > (double)(n3[t] - 1)) { sh[t][1] = -a.period[t]; ni[t] = 2; }
+        }
+    }
+    for (int im = 0; im < ni[0] * ni[1] * ni[2]; ++im) {
+        const double xc = xc0 + sh[0][im % ni[0]], yc = yc0 + sh[1][(im / ni[0]) % ni[1]];
+        const double zc = zc0 + sh[2][im / (ni[0] * ni[1])];
+        const int x0 = max(0, (int)floor(xc - reach)), x1 = min(a.nx - 1, (int)ceil(xc + reach));
+        const int y0 = max(0, (int)floor(yc - reach)), y1 = min(a.ny - 1, (int)ceil(yc + reach));
+        const int z0 = max(0, (int)floor(zc - reach)), z1 = min(a.nz - 1, (int)ceil(zc + reach));
+        if (x1 < x0 || y1 < y0 || z1 < z0) continue;
+        // one thread per (y, z) row of the box: the row's chord of the reach ball
+        const int ey = y1 - y0 + 1;
+        const unsigned tot = (unsigned)ey * (unsigned)(z1 - z0 + 1);
+        for (unsigned t = threadIdx.x; t < tot; t += blockDim.x) {
+            const int y = y0 + (int)(t % (unsigned)ey), z = z0 + (int)(t / (unsigned)ey);
+            const double dy = (double)y - yc, dz = (double)z - zc;
+            const double w2 = reach * reach - dy * dy - dz * dz;
+            if (w2 < 0.0) continue;
+            const double w = sqrt(w2);
+            const int xa = max(0, (int)floor(xc - w)), xb = min(a.nx - 1, (int)ceil(xc + w));
+            if (xb < xa) continue;
+            uint8_t *rowp = near + ((size_t)z * a.ny + y) * nb;
+            for (int b = xa >> 5; b <= (xb >> 5); ++b) rowp[b] = 1;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Smooth solid fraction (differentiable stand-in for the 5^3 count): the same
 // effective radius r = R/dx - 1/2 (psclattice3d.py:105), a C1 ramp of one
@@ -384,6 +446,8 @@ extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const 
         a.ff = G->force_fluid; a.mf = G->moment_fluid;
         a.status = L->status;
         a.moved = a.moved_next = nullptr;
+        a.disp_limit = 0.0;
+        a.periodic[0] = a.periodic[1] = a.periodic[2] = 0;
         a.wrap[0] = a.wrap[1] = a.wrap[2] = 0;   // the smooth map has no periodic images
         a.period[0] = a.period[1] = a.period[2] = 0.0;
         k_map_clear<false><<<G->n, 128, 0, st>>>(a);
@@ -426,11 +490,13 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     for (int t = 0; t < 3; ++t) {
         a.wrap[t] = P->wrap[t] != 0;
         a.period[t] = P->period[t];
+        a.periodic[t] = P->periodic[t] != 0;
         if (a.wrap[t] && !(P->period[t] >= 1.0)) {
             set_error("psc_map: periodic images need a positive period (axis %d)", t);
             return LBDEM_ERR_ARG;
         }
     }
+    a.disp_limit = P->disp_limit;
     cudaStream_t st = (cudaStream_t)stream;
     if (P->map_moved && P->map_reuse && P->have_prev) {
         // the previous exact map's centres are in prev: skip the remap when none changed
@@ -448,4 +514,116 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     }
     P->have_prev = 1;
     return check_launch("psc_map");
+}
+
+// Ordered block lists (ascending ids, so each phase walks memory in order):
+// far blocks from the front of `blocks`, near blocks packed at its end.
+// Chunks of 1024 block ids: per-chunk counts, one scan over the chunks, then
+// each chunk writes its ids at its offsets (warp ballots + a CTA prefix).
+constexpr int LIST_CHUNK = 1024;
+
+__global__ void __launch_bounds__(LIST_CHUNK) k_list_count(const uint8_t *mask, uint32_t nblocks, uint32_t *chunk_n) {
+    const uint32_t id = blockIdx.x * LIST_CHUNK + threadIdx.x;
+    const int nearb = id < nblocks && mask[id] != 0;
+    const int n_near = __syncthreads_count(nearb);
+    if (threadIdx.x == 0) {
+        const uint32_t valid = min((uint32_t)LIST_CHUNK, nblocks - blockIdx.x * LIST_CHUNK);
+        chunk_n[2 * blockIdx.x] = valid - (uint32_t)n_near;
+        chunk_n[2 * blockIdx.x + 1] = (uint32_t)n_near;
+    }
+}
+
+// exclusive scan of the (far, near) chunk counts in place; totals to counts[0..1]
+__global__ void __launch_bounds__(1024) k_list_scan(uint32_t *chunk_n, uint32_t nchunks, uint32_t *counts) {
+    __shared__ uint32_t sf[1024], sn[1024];
+    const int t = threadIdx.x;
+    uint32_t cf = 0, cn = 0;
+    for (uint32_t base = 0; base < nchunks; base += 1024) {
+        const uint32_t i = base + t;
+        const uint32_t vf = i < nchunks ? chunk_n[2 * i] : 0u, vn = i < nchunks ? chunk_n[2 * i + 1] : 0u;
+        sf[t] = vf;
+        sn[t] = vn;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            const uint32_t af = t >= o ? sf[t - o] : 0u, an = t >= o ? sn[t - o] : 0u;
+            __syncthreads();
+            sf[t] += af;
+            sn[t] += an;
+            __syncthreads();
+        }
+        if (i < nchunks) {
+            chunk_n[2 * i] = cf + sf[t] - vf;
+            chunk_n[2 * i + 1] = cn + sn[t] - vn;
+        }
+        const uint32_t tf = sf[1023], tn = sn[1023];
+        __syncthreads();
+        cf += tf;
+        cn += tn;
+    }
+    if (t == 0) {
+        counts[0] = cf;
+        counts[1] = cn;
+    }
+}
+
+__global__ void __launch_bounds__(LIST_CHUNK) k_list_fill(const uint8_t *mask, uint32_t nblocks, const uint32_t *chunk_n,
+                                                          const uint32_t *counts, uint32_t *blocks) {
+    __shared__ uint32_t wf[LIST_CHUNK / 32], wn[LIST_CHUNK / 32];
+    const uint32_t id = blockIdx.x * LIST_CHUNK + threadIdx.x;
+    const bool in = id < nblocks;
+    const bool nearb = in && mask[id] != 0, farb = in && !nearb;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, below = (1u << lane) - 1u;
+    const unsigned mf = __ballot_sync(0xffffffffu, farb), mn = __ballot_sync(0xffffffffu, nearb);
+    if (lane == 0) {
+        wf[warp] = (uint32_t)__popc(mf);
+        wn[warp] = (uint32_t)__popc(mn);
+    }
+    __syncthreads();
+    uint32_t pf = 0, pn = 0;
+    for (unsigned w = 0; w < warp; ++w) {
+        pf += wf[w];
+        pn += wn[w];
+    }
+    if (farb) blocks[chunk_n[2 * blockIdx.x] + pf + __popc(mf & below)] = id;
+    if (nearb) blocks[nblocks - counts[1] + chunk_n[2 * blockIdx.x + 1] + pn + __popc(mn & below)] = id;
+}
+
+extern "C" int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G,
+                                     double margin, uint8_t *near, uint32_t *blocks, uint32_t *counts,
+                                     void *stream) {
+    using namespace lbdem;
+    if (!L || !P || !G || !near || !blocks || !counts || L->nx <= 0 || L->ny <= 0 || L->nz <= 0 ||
+        !(margin >= 0.0)) {
+        set_error("psc_near_blocks: bad arguments");
+        return LBDEM_ERR_ARG;
+    }
+    if (!(P->dx > 0.0)) {
+        set_error("psc_near_blocks: dx must be positive");
+        return LBDEM_ERR_ARG;
+    }
+    const size_t nb = ((size_t)L->nx + 31) / 32;
+    const size_t nblocks = nb * (size_t)L->ny * L->nz;
+    if (nblocks >= (1ull << 32)) {
+        set_error("psc_near_blocks: too many x-blocks");
+        return LBDEM_ERR_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(near, 0, nblocks, st) != cudaSuccess) return check_launch("near_blocks");
+    MapArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
+    a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;
+    a.pos = G->pos; a.radius = G->radius;
+    for (int t = 0; t < 3; ++t) {
+        a.periodic[t] = P->periodic[t] != 0;
+        a.period[t] = P->period[t];
+    }
+    if (G->n > 0) k_near_blocks<<<G->n, 128, 0, st>>>(a, margin, near);
+    // ordered lists; the chunk counts live in the tail of counts (2 + 2 * chunks words)
+    const uint32_t nchunks = (uint32_t)((nblocks + LIST_CHUNK - 1) / LIST_CHUNK);
+    uint32_t *chunk_n = counts + 2;
+    k_list_count<<<nchunks, LIST_CHUNK, 0, st>>>(near, (uint32_t)nblocks, chunk_n);
+    k_list_scan<<<1, 1024, 0, st>>>(chunk_n, nchunks, counts);
+    k_list_fill<<<nchunks, LIST_CHUNK, 0, st>>>(near, (uint32_t)nblocks, chunk_n, counts, blocks);
+    return check_launch("near_blocks");
 }

@@ -67,16 +67,25 @@ class PSCLattice3D(LatticeEngine):
         p.map_moved = N.ptr(self._map_moved)
         p.map_reuse, p.map_parity = 0, 0
         self._mapped_epoch = -1
-        # periodic images of the DEM solver's "wrapped" mode: image shift = domain length / dx
-        if getattr(demslover, "compat", "reference") == "wrapped":
-            if solid_fraction == "smooth":
-                raise ValueError('the smooth solid fraction has no periodic images (DEMSolver compat="wrapped")')
-            dom = demslover.config.domain
-            lens = (dom.xmax - dom.xmin, dom.ymax - dom.ymin, dom.zmax - dom.zmin)
-            for a in range(3):
-                per = demslover.config.boundaryType[2 * a] == demslover.config.BOUNDARY_TYPE_PERIODIC
-                p.wrap[a] = int(per)
-                p.period[a] = float(lens[a] / dx) if per else 0.0
+        # periodic axes of the DEM domain (image shift = domain length / dx): used by the
+        # pipelined run, and for periodic images in the DEM solver's "wrapped" mode
+        self.wrapped = getattr(demslover, "compat", "reference") == "wrapped"
+        if self.wrapped and solid_fraction == "smooth":
+            raise ValueError('the smooth solid fraction has no periodic images (DEMSolver compat="wrapped")')
+        dom = demslover.config.domain
+        lens = (dom.xmax - dom.xmin, dom.ymax - dom.ymin, dom.zmax - dom.zmin)
+        for a in range(3):
+            per = demslover.config.boundaryType[2 * a] == demslover.config.BOUNDARY_TYPE_PERIODIC
+            p.periodic[a] = int(per)
+            p.period[a] = float(lens[a] / dx) if per else 0.0
+            p.wrap[a] = int(per and self.wrapped)
+        p.disp_limit = 0.0
+        # pipelined run(): near-block mask, side stream for the DEM and the next map
+        self.pipeline_margin = 0.25
+        self._pipeline_choice = None      # run(pipeline="auto"): measured on the first long run
+        self._pipeline_probe = None       # (sequential, pipelined) ms per step of that measurement
+        self._near = None
+        self._side = None
         if solid_fraction == "smooth":
             self._eps = torch.zeros(nc, dtype=torch.float32, device=dev)
             self._map_scratch = torch.zeros(nc, dtype=torch.int64, device=dev)
@@ -169,6 +178,98 @@ class PSCLattice3D(LatticeEngine):
         self.stream()
         self.dem.run_substeps(sub_cycles)
 
-    def run(self, n_steps: int, sub_cycles: int = 1):
-        for _ in range(int(n_steps)):
-            self.step(sub_cycles)
+    def run(self, n_steps: int, sub_cycles: int = 1, pipeline="auto"):
+        """n_steps coupled steps (step() n times).  Pipelined, the step's
+        x-blocks that no particle can reach -- at most ``pipeline_margin``
+        lattice units of motion per step, 0.25 by default -- are streamed and
+        collided on the GPU while the DEM sub-steps and the next map still run
+        on a second stream; the blocks near particles follow once the map is
+        ready.  Every cell is computed once from the same inputs, so the result
+        is the sequential loop's (force sums may differ in the last FP64 bits:
+        they are added atomically).  A particle that moves farther than the
+        margin in one step raises a lattice fault at the next check_status().
+
+        ``pipeline``: True, False, or "auto" (default): the first call of at
+        least 32 steps times twelve sequential and twelve pipelined steps and
+        keeps the faster form for this lattice (the pipeline pays where the DEM
+        and the map are a large part of the step and particles leave much of
+        the lattice free).  Lattices without particles, with the smooth solid
+        fraction or with periodic images always run sequentially."""
+        n = int(n_steps)
+        if n <= 0:
+            return
+        eligible = self.dem.n > 0 and self.solid_fraction == "exact" and not self.wrapped
+        if pipeline == "auto":
+            if not eligible:
+                pipeline = False
+            elif self._pipeline_choice is None and n >= 32:
+                def timed(fn):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    fn()
+                    e1.record()
+                    e1.synchronize()
+                    return e0.elapsed_time(e1)
+                # untimed first: the first launches of the pipelined kernels load their code
+                self._run_pipelined(2, sub_cycles)
+                t_seq = timed(lambda: [self.step(sub_cycles) for _ in range(12)]) / 12
+                t_pipe = timed(lambda: self._run_pipelined(12, sub_cycles)) / 12
+                self._pipeline_choice = t_pipe < t_seq
+                self._pipeline_probe = (t_seq, t_pipe)
+                n -= 26
+                pipeline = self._pipeline_choice
+            else:
+                pipeline = bool(self._pipeline_choice)
+        if not pipeline or not eligible or n < 2:
+            for _ in range(n):
+                self.step(sub_cycles)
+            return
+        self._run_pipelined(n, sub_cycles)
+
+    def _run_pipelined(self, n: int, sub_cycles: int):
+        S = torch.cuda.current_stream()
+        if self._side is None:
+            self._side = torch.cuda.Stream(priority=-1)
+            nblk = self.Ny * self.Nz * self._nb
+            self._near = torch.zeros(nblk, dtype=torch.uint8, device="cuda")
+            self._blocks = torch.zeros(nblk, dtype=torch.int32, device="cuda")
+            self._bcounts = torch.zeros(2 + 2 * ((nblk + 1023) // 1024), dtype=torch.int32, device="cuda")
+        D = self._side
+        lat, psc, grains = C.byref(self._lat), C.byref(self._psc), C.byref(self._grains)
+        d = self.dem._d
+        sync = d.sync
+        d.sync = None                      # DEM as plain launches: they can share the GPU with the step
+        self._psc.disp_limit = float(self.pipeline_margin)
+        try:
+            self.collide()                 # step 0: map and full fused step
+            self.stream()
+            for k in range(n):
+                last = k == n - 1
+                if not last:
+                    # blocks a particle can reach before the DEM moves it (positions of step k)
+                    N.call("lbdem_psc_near_blocks", lat, psc, grains, float(self.pipeline_margin),
+                           N.ptr(self._near), N.ptr(self._blocks), N.ptr(self._bcounts), S.cuda_stream)
+                ev = torch.cuda.Event()
+                ev.record(S)
+                with torch.cuda.stream(D):
+                    D.wait_event(ev)
+                    self.dem.run_substeps(sub_cycles)
+                    if not last:
+                        self.grains2lattice()      # map of step k+1
+                    done = torch.cuda.Event()
+                    done.record(D)
+                if last:
+                    S.wait_event(done)
+                    break
+                src = self._cur
+                blk = (N.ptr(self._blocks), N.ptr(self._bcounts))
+                N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 1, *blk, S.cuda_stream)
+                S.wait_event(done)
+                if self._hydro is not None:
+                    self._hydro.zero_()
+                N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 2, *blk, S.cuda_stream)
+                self._cur, self._cur_kind, self._collided = 1 - src, "fpc", None
+        finally:
+            d.sync = sync
+            self._psc.disp_limit = 0.0
+        self._invalidate_views()
