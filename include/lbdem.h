@@ -281,8 +281,10 @@ int lbdem_psc_step_bf16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_
  * centre, or of its periodic image along P->periodic axes (mask: Ny*Nz*NB
  * bytes of scratch); then the list `blocks` (Ny*Nz*NB uint32) holds the
  * counts[0] far blocks (ascending) from its start and the counts[1] near
- * blocks (ascending) packed at its end.  counts: device uint32 array of
- * 2 + 2 * ceil(Ny*Nz*NB / 1024) words (the tail is scratch).
+ * blocks (ascending) packed at its end, each entry z << 20 | y << 8 | x/32.
+ * counts: device uint32 array of 2 + 2 * ceil(Ny*Nz*NB / 1024) words (the
+ * tail is scratch).  Lattices beyond Nx = 8192, Ny = 4096 or Nz = 4096 get
+ * LBDEM_ERR_UNSUPPORTED.
  *
  * lbdem_psc_step_phase: one gathered step (gather = 1) restricted to
  *   phase 1: the far blocks, as pure fluid (no keys read, no force);

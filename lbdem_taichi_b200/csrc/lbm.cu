@@ -484,11 +484,11 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     if constexpr (LISTED) {
         const uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
         if (w >= *a.bcount) return;   // warp-uniform
-        const uint32_t id = a.blist[a.bfrom_end ? a.nblocks - *a.bcount + w : w];
-        const uint32_t r = id / a.nb;
-        x = (int)((id - r * a.nb) * 32u + (threadIdx.x & 31u));
-        y = (int)(r % (uint32_t)ny);
-        z = (int)(r / (uint32_t)ny);
+        // entry: z | y | x-block (bits 20-31 | 8-19 | 0-7)
+        const uint32_t e = a.blist[a.bfrom_end ? a.nblocks - *a.bcount + w : w];
+        x = (int)((e & 0xFFu) * 32u + (threadIdx.x & 31u));
+        y = (int)((e >> 8) & 0xFFFu);
+        z = (int)(e >> 20);
     } else {
         x = blockIdx.x * blockDim.x + threadIdx.x;
         y = blockIdx.y * blockDim.y + threadIdx.y;

@@ -566,8 +566,10 @@ __global__ void __launch_bounds__(1024) k_list_scan(uint32_t *chunk_n, uint32_t 
     }
 }
 
-__global__ void __launch_bounds__(LIST_CHUNK) k_list_fill(const uint8_t *mask, uint32_t nblocks, const uint32_t *chunk_n,
-                                                          const uint32_t *counts, uint32_t *blocks) {
+// list entry: z (bits 20-31) | y (bits 8-19) | x-block (bits 0-7), so the step decodes it with shifts
+__global__ void __launch_bounds__(LIST_CHUNK) k_list_fill(const uint8_t *mask, uint32_t nblocks, uint32_t nb, uint32_t ny,
+                                                          const uint32_t *chunk_n, const uint32_t *counts,
+                                                          uint32_t *blocks) {
     __shared__ uint32_t wf[LIST_CHUNK / 32], wn[LIST_CHUNK / 32];
     const uint32_t id = blockIdx.x * LIST_CHUNK + threadIdx.x;
     const bool in = id < nblocks;
@@ -584,8 +586,9 @@ __global__ void __launch_bounds__(LIST_CHUNK) k_list_fill(const uint8_t *mask, u
         pf += wf[w];
         pn += wn[w];
     }
-    if (farb) blocks[chunk_n[2 * blockIdx.x] + pf + __popc(mf & below)] = id;
-    if (nearb) blocks[nblocks - counts[1] + chunk_n[2 * blockIdx.x + 1] + pn + __popc(mn & below)] = id;
+    const uint32_t row = id / nb, code = ((row / ny) << 20) | ((row % ny) << 8) | (id - row * nb);
+    if (farb) blocks[chunk_n[2 * blockIdx.x] + pf + __popc(mf & below)] = code;
+    if (nearb) blocks[nblocks - counts[1] + chunk_n[2 * blockIdx.x + 1] + pn + __popc(mn & below)] = code;
 }
 
 extern "C" int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G,
@@ -607,6 +610,10 @@ extern "C" int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P,
         set_error("psc_near_blocks: too many x-blocks");
         return LBDEM_ERR_ARG;
     }
+    if (nb > 256 || L->ny > 4096 || L->nz > 4096) {
+        set_error("psc_near_blocks: block lists cover Nx <= 8192, Ny <= 4096, Nz <= 4096");
+        return LBDEM_ERR_UNSUPPORTED;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     if (cudaMemsetAsync(near, 0, nblocks, st) != cudaSuccess) return check_launch("near_blocks");
     MapArgs a;
@@ -624,6 +631,7 @@ extern "C" int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P,
     uint32_t *chunk_n = counts + 2;
     k_list_count<<<nchunks, LIST_CHUNK, 0, st>>>(near, (uint32_t)nblocks, chunk_n);
     k_list_scan<<<1, 1024, 0, st>>>(chunk_n, nchunks, counts);
-    k_list_fill<<<nchunks, LIST_CHUNK, 0, st>>>(near, (uint32_t)nblocks, chunk_n, counts, blocks);
+    k_list_fill<<<nchunks, LIST_CHUNK, 0, st>>>(near, (uint32_t)nblocks, (uint32_t)nb, (uint32_t)L->ny, chunk_n, counts,
+                                                blocks);
     return check_launch("near_blocks");
 }

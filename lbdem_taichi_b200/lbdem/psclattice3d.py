@@ -194,11 +194,14 @@ class PSCLattice3D(LatticeEngine):
         keeps the faster form for this lattice (the pipeline pays where the DEM
         and the map are a large part of the step and particles leave much of
         the lattice free).  Lattices without particles, with the smooth solid
-        fraction or with periodic images always run sequentially."""
+        fraction, with periodic images or beyond 8192 x 4096 x 4096 cells always
+        run sequentially."""
         n = int(n_steps)
         if n <= 0:
             return
-        eligible = self.dem.n > 0 and self.solid_fraction == "exact" and not self.wrapped
+        # block-list entries pack z, y and the x-block into 12 + 12 + 8 bits
+        eligible = (self.dem.n > 0 and self.solid_fraction == "exact" and not self.wrapped
+                    and self.Nx <= 8192 and self.Ny <= 4096 and self.Nz <= 4096)
         if pipeline == "auto":
             if not eligible:
                 pipeline = False

@@ -69,6 +69,13 @@ def test_host_side_argument_checks():
     # the list builder validates its arguments before any launch
     assert lib.lbdem_boundary_cells(None, 8, 8, 8, None, 0, 8, 8, None) == N.LBDEM_ERR_ARG
     assert lib.lbdem_boundary_cells(8, 8, 8, 8, None, 16, 8, 8, None) == N.LBDEM_ERR_ARG   # capacity, no array
+    # block-list entries hold z, y and the x-block in 12 + 12 + 8 bits
+    G = N.Grains()
+    P.dx = 1.0
+    L.nx, L.ny, L.nz = 64, 5000, 8
+    assert lib.lbdem_psc_near_blocks(C.byref(L), C.byref(P), C.byref(G), 0.25, 8, 8, 8, None) == \
+        N.LBDEM_ERR_UNSUPPORTED
+    assert b"Ny <= 4096" in lib.lbdem_last_error()
 
 
 @pytest.mark.skipif(subprocess.run(["which", "gcc"], capture_output=True).returncode != 0, reason="no gcc")
