@@ -235,23 +235,30 @@ class PSCLattice3D(LatticeEngine):
             self._side = torch.cuda.Stream(priority=-1)
             nblk = self.Ny * self.Nz * self._nb
             self._near = torch.zeros(nblk, dtype=torch.uint8, device="cuda")
-            self._blocks = torch.zeros(nblk, dtype=torch.int32, device="cuda")
-            self._bcounts = torch.zeros(2 + 2 * ((nblk + 1023) // 1024), dtype=torch.int32, device="cuda")
+            # two block lists: the side stream builds the next step's while this step's is in use
+            self._blocks = [torch.zeros(nblk, dtype=torch.int32, device="cuda") for _ in range(2)]
+            self._bcounts = [torch.zeros(2 + 2 * ((nblk + 1023) // 1024), dtype=torch.int32, device="cuda")
+                             for _ in range(2)]
         D = self._side
         lat, psc, grains = C.byref(self._lat), C.byref(self._psc), C.byref(self._grains)
         d = self.dem._d
         sync = d.sync
         d.sync = None                      # DEM as plain launches: they can share the GPU with the step
         self._psc.disp_limit = float(self.pipeline_margin)
+
+        def near_blocks(buf, stream):
+            # blocks a particle can reach before the DEM moves it (current positions)
+            N.call("lbdem_psc_near_blocks", lat, psc, grains, float(self.pipeline_margin), N.ptr(self._near),
+                   N.ptr(self._blocks[buf]), N.ptr(self._bcounts[buf]), stream.cuda_stream)
+
         try:
             self.collide()                 # step 0: map and full fused step
             self.stream()
+            near_blocks(0, S)
+            lists = None                   # event: the next step's lists are built (side stream)
             for k in range(n):
                 last = k == n - 1
-                if not last:
-                    # blocks a particle can reach before the DEM moves it (positions of step k)
-                    N.call("lbdem_psc_near_blocks", lat, psc, grains, float(self.pipeline_margin),
-                           N.ptr(self._near), N.ptr(self._blocks), N.ptr(self._bcounts), S.cuda_stream)
+                buf = k & 1
                 ev = torch.cuda.Event()
                 ev.record(S)
                 with torch.cuda.stream(D):
@@ -259,15 +266,22 @@ class PSCLattice3D(LatticeEngine):
                     self.dem.run_substeps(sub_cycles)
                     if not last:
                         self.grains2lattice()      # map of step k+1
-                    done = torch.cuda.Event()
-                    done.record(D)
+                    mapped = torch.cuda.Event()
+                    mapped.record(D)
+                    if k < n - 2:
+                        near_blocks(1 - buf, D)    # the next iteration's lists, from the positions of this map
+                        nxt = torch.cuda.Event()
+                        nxt.record(D)
                 if last:
-                    S.wait_event(done)
+                    S.wait_event(mapped)
                     break
+                if lists is not None:
+                    S.wait_event(lists)
+                lists = nxt if k < n - 2 else None
                 src = self._cur
-                blk = (N.ptr(self._blocks), N.ptr(self._bcounts))
+                blk = (N.ptr(self._blocks[buf]), N.ptr(self._bcounts[buf]))
                 N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 1, *blk, S.cuda_stream)
-                S.wait_event(done)
+                S.wait_event(mapped)
                 if self._hydro is not None:
                     self._hydro.zero_()
                 N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 2, *blk, S.cuda_stream)
