@@ -767,12 +767,16 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     const int nb_con = (int)((8ll * D->n + 127) / 128);
     // "cluster": all sub-steps in one launch of a single thread-block cluster
     // (opt-in: it confines the contact phase to <= 16 SMs and measured slower
-    // than two launches per sub-step spread over the whole GPU)
+    // than two launches per sub-step spread over the whole GPU).  It is the
+    // default when one 512-thread block holds every contact lane (n <= 64):
+    // block barriers instead of grid barriers (one sphere: 90 us for 10
+    // sub-steps against 107 us cooperative).
     const char *mode = getenv("LBDEM_DEM_KERNELS");
     const bool wrap = D->wrap_pairs != 0;
     auto *kcl = wrap ? k_dem_cluster<true> : k_dem_cluster<false>;
     auto *kcoop = wrap ? k_dem_coop<true> : k_dem_coop<false>;
-    if (mode && strcmp(mode, "cluster") == 0) {
+    const bool one_block = !mode && D->sync && 8ll * D->n <= 512;
+    if ((mode && strcmp(mode, "cluster") == 0) || one_block) {
         // one cluster of up to 16 CTAs x 512 threads, sized to the contact lanes
         int ncta = (int)((8ll * D->n + 511) / 512);
         ncta = ncta < 1 ? 1 : (ncta > 16 ? 16 : ncta);

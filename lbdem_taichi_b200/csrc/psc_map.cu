@@ -148,7 +148,9 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
     return sqrt((ox * ox + oy * oy) + oz * oz) < r;
 }
 
-// One block per particle, two phases per chunk of its bounding box:
+// One block per particle -- or, with few particles, gridDim.y blocks sharing
+// its bounding box in contiguous ranges of cells, so that a lone sphere does
+// not map on one SM -- two phases per chunk of the box:
 //  1. each thread classifies one cell -- outside / fully covered / partial
 //     (psclattice3d.py:108-113).  FP32 with a safety margin decides the clear
 //     cases; the exact FP64 comparisons run only for cells near a threshold.
@@ -161,6 +163,7 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
 //     with the reference's exact FP64 expression (|s32 - s64| < 2e-5 (1 + r^2)
 //     for these offsets), so counts are bit-exact.
 constexpr int MAP_CHUNK = 2048;
+constexpr int MAP_SPLIT_BELOW = 592;   // 148 SMs x 4 blocks
 
 template <bool WRAP>
 __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
     const int g = blockIdx.x;
     double xc0, yc0, zc0, r;
     particle_lattice(a, g, xc0, yc0, zc0, r);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && blockIdx.y == 0) {
         a.prev[4 * g] = xc0; a.prev[4 * g + 1] = yc0; a.prev[4 * g + 2] = zc0; a.prev[4 * g + 3] = r;
     }
     const double t_out = r + HALF_DIAG, t_in = r - HALF_DIAG;
@@ -199,16 +202,21 @@ __global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
         const float band = (float)(1e-4 * (1.0 + rr));
         const float lo = (float)rr - band, hi = (float)rr + band;
         const unsigned tot = (unsigned)ex * (unsigned)ey * (unsigned)ez;
+        // this block's range of the box's cells
+        const unsigned per = (tot + gridDim.y - 1) / gridDim.y;
+        const unsigned beg = min(tot, blockIdx.y * per), end = min(tot, beg + per);
         // this thread's first cell, then advance by blockDim cells with carries
+        // (every chunk but the last is a whole number of blockDim steps)
         const unsigned bd = blockDim.x;
         const int adx = (int)(bd % (unsigned)ex), ady = (int)((bd / (unsigned)ex) % (unsigned)ey);
         const int adz = (int)(bd / ((unsigned)ex * (unsigned)ey));
-        int ix = (int)(threadIdx.x % (unsigned)ex), jy = (int)((threadIdx.x / (unsigned)ex) % (unsigned)ey);
-        int kz = (int)(threadIdx.x / ((unsigned)ex * (unsigned)ey));
-        for (unsigned base = 0; base < tot; base += MAP_CHUNK) {
+        const unsigned t0 = beg + threadIdx.x;
+        int ix = (int)(t0 % (unsigned)ex), jy = (int)((t0 / (unsigned)ex) % (unsigned)ey);
+        int kz = (int)(t0 / ((unsigned)ex * (unsigned)ey));
+        for (unsigned base = beg; base < end; base += MAP_CHUNK) {
             if (threadIdx.x == 0) s_n = s_na = 0;
             __syncthreads();
-            const unsigned lim = min(tot, base + MAP_CHUNK);
+            const unsigned lim = min(end, base + MAP_CHUNK);
             for (unsigned t = base + threadIdx.x; t < lim; t += bd) {
                 const int i = x0 + ix, j = y0 + jy, k = z0 + kz;
                 ix += adx; jy += ady; kz += adz;
@@ -505,12 +513,14 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
         a.moved_next = P->map_moved + (1 - par);
         P->map_parity = 1 - par;
     }
+    // fewer particles than about four blocks per SM: split each box over several blocks
+    const dim3 sgrid((unsigned)G->n, (unsigned)(G->n >= MAP_SPLIT_BELOW ? 1 : min(16, (MAP_SPLIT_BELOW + G->n - 1) / G->n)));
     if (a.wrap[0] || a.wrap[1] || a.wrap[2]) {
         k_map_clear<true><<<G->n, 128, 0, st>>>(a);
-        k_map_scatter<true><<<G->n, 256, 0, st>>>(a);
+        k_map_scatter<true><<<sgrid, 256, 0, st>>>(a);
     } else {
         k_map_clear<false><<<G->n, 128, 0, st>>>(a);
-        k_map_scatter<false><<<G->n, 256, 0, st>>>(a);
+        k_map_scatter<false><<<sgrid, 256, 0, st>>>(a);
     }
     P->have_prev = 1;
     return check_launch("psc_map");

@@ -337,3 +337,31 @@ def test_dem_single_launch_kernels_match_split_kernels(mode, monkeypatch):
     assert set(res[0][0]) == set(res[1][0]) and len(res[0][0]) > 100
     assert np.abs(res[0][1] - res[1][1]).max() < 1e-11
     assert relmax(res[0][2], res[1][2]) < 1e-8
+
+
+def test_dem_few_particles_one_block_matches_split_kernels(monkeypatch):
+    """With at most 64 particles the default single launch is one block
+    (block barriers between the phases): same contact sets and states as two
+    launches per sub-step."""
+    rng = np.random.default_rng(14)
+    g = np.stack(np.meshgrid(np.arange(3), np.arange(3), np.arange(3), indexing="ij"), -1).reshape(-1, 3)
+    pos = 4.5 + g * 3.95 + rng.uniform(-0.05, 0.05, g.shape)
+    n = len(pos)
+    rad = 2.0 + rng.uniform(-0.02, 0.02, n)
+    vel = rng.normal(0, 0.02, (n, 3))
+    mass = 2.0 * 4.0 / 3.0 * np.pi * rad ** 3
+    res = []
+    for m in (None, "split"):
+        if m is None:
+            monkeypatch.delenv("LBDEM_DEM_KERNELS", raising=False)
+        else:
+            monkeypatch.setenv("LBDEM_DEM_KERNELS", m)
+        dem = make_dem((0.0, 20.0, 0.0, 20.0, 0.0, 16.0), 0.05, (0, 0, -1e-3), _hertz(), rad, mass, pos, vel,
+                       periodic=(True, True, False), max_coord=24, E=1e3, wall_E=1e3)
+        dem.run_substeps(17)
+        dem.check_status()
+        res.append((dem.active_contacts(), dem.gf.position.to_numpy(), dem.gf.omega.to_numpy()))
+    monkeypatch.delenv("LBDEM_DEM_KERNELS", raising=False)
+    assert set(res[0][0]) == set(res[1][0]) and len(res[0][0]) > 20
+    assert np.abs(res[0][1] - res[1][1]).max() < 1e-11
+    assert relmax(res[0][2], res[1][2]) < 1e-8
