@@ -775,7 +775,8 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     const bool wrap = D->wrap_pairs != 0;
     auto *kcl = wrap ? k_dem_cluster<true> : k_dem_cluster<false>;
     auto *kcoop = wrap ? k_dem_coop<true> : k_dem_coop<false>;
-    const bool one_block = !mode && D->sync && 8ll * D->n <= 512;
+    // (one block on one SM also runs beside a step on another stream)
+    const bool one_block = !mode && 8ll * D->n <= 512;
     if ((mode && strcmp(mode, "cluster") == 0) || one_block) {
         // one cluster of up to 16 CTAs x 512 threads, sized to the contact lanes
         int ncta = (int)((8ll * D->n + 511) / 512);

@@ -243,7 +243,7 @@ class PSCLattice3D(LatticeEngine):
         lat, psc, grains = C.byref(self._lat), C.byref(self._psc), C.byref(self._grains)
         d = self.dem._d
         sync = d.sync
-        d.sync = None                      # DEM as plain launches: they can share the GPU with the step
+        d.sync = None                      # no grid-wide DEM launch: its blocks share the GPU with the step
         self._psc.disp_limit = float(self.pipeline_margin)
 
         def near_blocks(buf, stream):
