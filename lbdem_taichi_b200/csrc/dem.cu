@@ -640,6 +640,26 @@ __global__ void __launch_bounds__(512) k_dem_cluster(const __grid_constant__ Dem
     }
 }
 
+// All sub-steps in one 128-thread block (at most 16 particles): the phases are
+// separated by __syncthreads, which orders the block's global-memory writes of
+// one phase before the reads of the next; the same per-lane/per-particle code
+// without the cluster form's register cap (512 threads), so nothing spills.
+template <bool WRAP>
+__global__ void __launch_bounds__(128) k_dem_block(const __grid_constant__ DemArgs A, int nsub) {
+    const lbdem_dem &d = A.d;
+    const int nthr = (int)blockDim.x, me = (int)threadIdx.x;
+    const int nlanes = 8 * d.n;
+    for (int s = 0; s < nsub; ++s) {
+        const int parity = (A.parity + s) & 1;
+        const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
+        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(d, count, base + me);
+        __syncthreads();
+        int32_t *used = d.cell_count + (size_t)parity * A.ncell;
+        for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
+        for (int i = me; i < d.n; i += nthr) integrate_particle(d, A.ncell, parity, i);
+        __syncthreads();
+    }
+}
 
 // ---------------------------------------------------------------------------
 // All sub-steps of one call in ONE cooperative launch (the default): every
@@ -777,6 +797,14 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     auto *kcoop = wrap ? k_dem_coop<true> : k_dem_coop<false>;
     // (one block on one SM also runs beside a step on another stream)
     const bool one_block = !mode && 8ll * D->n <= 512;
+    if (one_block && 8ll * D->n <= 128) {
+        A.parity = D->parity;
+        if (wrap) k_dem_block<true><<<1, 128, 0, st>>>(A, (int)nsub);
+        else k_dem_block<false><<<1, 128, 0, st>>>(A, (int)nsub);
+        D->parity ^= (nsub & 1);
+        g_dem_launches = 1;
+        return check_launch("dem_substeps (one block)");
+    }
     if ((mode && strcmp(mode, "cluster") == 0) || one_block) {
         // one cluster of up to 16 CTAs x 512 threads, sized to the contact lanes
         int ncta = (int)((8ll * D->n + 511) / 512);
