@@ -165,8 +165,10 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
 constexpr int MAP_CHUNK = 2048;
 constexpr int MAP_SPLIT_BELOW = 592;   // 148 SMs x 4 blocks
 
+// Five 256-thread blocks per SM (46 registers, 40 KB of shared memory each);
+// the image form keeps four (it would spill at five).
 template <bool WRAP>
-__global__ void __launch_bounds__(256) k_map_scatter(const MapArgs a) {
+__global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs a) {
     __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32; w = global cell index
     __shared__ int s_amb[MAP_CHUNK];      // partial cells needing the exact recount (index into s_off)
     __shared__ int s_n, s_na;
@@ -515,6 +517,13 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     }
     // fewer particles than about four blocks per SM: split each box over several blocks
     const dim3 sgrid((unsigned)G->n, (unsigned)(G->n >= MAP_SPLIT_BELOW ? 1 : min(16, (MAP_SPLIT_BELOW + G->n - 1) / G->n)));
+    static const bool carveout = [] {
+        // room for five scatter blocks' shared memory on every SM
+        cudaFuncSetAttribute(k_map_scatter<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        return true;
+    }();
+    (void)carveout;
     if (a.wrap[0] || a.wrap[1] || a.wrap[2]) {
         k_map_clear<true><<<G->n, 128, 0, st>>>(a);
         k_map_scatter<true><<<sgrid, 256, 0, st>>>(a);
