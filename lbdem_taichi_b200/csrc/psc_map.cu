@@ -517,13 +517,6 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     }
     // fewer particles than about four blocks per SM: split each box over several blocks
     const dim3 sgrid((unsigned)G->n, (unsigned)(G->n >= MAP_SPLIT_BELOW ? 1 : min(16, (MAP_SPLIT_BELOW + G->n - 1) / G->n)));
-    static const bool carveout = [] {
-        // room for five scatter blocks' shared memory on every SM
-        cudaFuncSetAttribute(k_map_scatter<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-        return true;
-    }();
-    (void)carveout;
     if (a.wrap[0] || a.wrap[1] || a.wrap[2]) {
         k_map_clear<true><<<G->n, 128, 0, st>>>(a);
         k_map_scatter<true><<<sgrid, 256, 0, st>>>(a);
