@@ -453,10 +453,14 @@ def run_reference(args):
     cells = NX * NY * nz_slab
     v = cells * args.steps_ref / dt / 1e6
     sample = f"{NX}x{NY}x{nz_slab} slab of the workload with all {NP} particles per step"
-    out = {"metric": METRIC, "value": round(v, 4), "unit": "MLUPS", "impl": "reference", "n_gpus": 0,
-           "steps": args.steps_ref, "warmup": args.warmup_ref, "ms_per_step": round(dt * 1e3 / args.steps_ref, 2),
+    # the GPU arm's config; the reference computes in FP64 on the host cores (no GPU)
+    out = {"metric": METRIC, "value": round(v, 4), "unit": "MLUPS", "impl": "reference", "n_gpus": args.gpus,
+           "device": "cpu", "steps": args.steps_ref, "warmup": args.warmup_ref,
+           "ms_per_step": round(dt * 1e3 / args.steps_ref, 2),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": W["desc"] + f" (per-step sample: {sample})"},
+           "config": {"workload": W["desc"], "name": W["key"], "lattice": [NX, NY, NZ], "particles": NP,
+                      "dem_subcycles": SUB, "storage": "f64", "sample": f"per step: {sample}",
+                      "parallelism": f"{os.cpu_count()} host threads"},
            "cpu_baseline": {"value": round(v, 4), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                             "sample": sample},
            "e2e": {"value": round(v, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
