@@ -216,6 +216,24 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The slowest rank's value of x (a time in ms).  Every rank calls it, in
+    the same order, for every reduced quantity."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(world, cells, steps, ms):
+    """Whole-job MLUPS of `world` replicas that each updated `cells` cells
+    `steps` times, timed by the slowest rank (ms)."""
+    return world * cells * steps / (ms * 1e-3) / 1e6
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -300,10 +318,8 @@ def run_gpu(args):
         launches = Nat.launch_count()
         barrier()
         ms = t0.elapsed_time(t1)
-    ms_t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
+    ms = max_over_ranks(ms, world)
+    ms_seq = max_over_ranks(ms_seq, world)
     kern_ms = statistics.mean(a.elapsed_time(b) for a, b in ev_step)
     lbm_ms = statistics.mean(a.elapsed_time(b) for a, b, _ in ev_phase)
     dem_ms = statistics.mean(b.elapsed_time(c) for _, b, c in ev_phase)
@@ -340,13 +356,10 @@ def run_gpu(args):
     e1.record(st)
     torch.cuda.synchronize()
     e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - tw0) * 1e3)
-    e2e_t = torch.tensor([e2e_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(e2e_t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world)
 
-    value = world * cells * args.steps / (ms * 1e-3) / 1e6
-    e2e_value = world * cells * e_steps / (e2e_ms * 1e-3) / 1e6
+    value = job_mlups(world, cells, args.steps, ms)
+    e2e_value = job_mlups(world, cells, e_steps, e2e_ms)
     peak, peak_kind = peaks()
     bpc = BYTES_PER_CELL[args.storage]
     l2_note = (f"inputs larger than L2 (populations {pop_gb:.2f} GB); no flush" if flush is None else
@@ -370,7 +383,7 @@ def run_gpu(args):
         "gpu_launches": launches,
         "pipelined": pipelined,
         "pipeline_probe_ms": [round(v, 4) for v in lat._pipeline_probe] if lat._pipeline_probe else None,
-        "sequential": {"value": round(world * cells * args.steps / (ms_seq * 1e-3) / 1e6, 2),
+        "sequential": {"value": round(job_mlups(world, cells, args.steps, ms_seq), 2),
                        "ms_per_step": round(ms_seq / args.steps, 4)},
         "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4), f"dem_{SUB}_substeps": round(dem_ms, 4),
                       "host_launch_per_step": round(cpu_launch_ms, 4)},
