@@ -250,9 +250,12 @@ __global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs
             __syncthreads();
             const int n = s_n;
             // 2a. one thread per partial cell: 25 columns x 5 sub-points from the
-            // squared per-axis offsets (-fmad=false: each product and sum rounded
-            // as in the per-point expression).  Cells with a sub-point inside the
-            // rounding band go to a second list for an exact warp recount.
+            // squared per-axis offsets (-fmad=false).  Per column (x, y) the five
+            // z terms are compared with lo - s_xy and hi - s_xy (their rounding is
+            // far inside the band), so a point counts when its squared distance is
+            // certainly below r^2 and the cell is ambiguous when a point lies
+            // between the two thresholds (the two counts differ); ambiguous cells
+            // go to a second list for an exact warp recount.
             for (int e = threadIdx.x; e < n; e += bd) {
                 const float4 o = s_off[e];
                 float ox2[5], oy2[5], oz2[5];
@@ -264,20 +267,20 @@ __global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs
                     oy2[m] = oy * oy;
                     oz2[m] = oz * oz;
                 }
-                int cnt = 0, amb = 0;
+                int cnt = 0, cnt_hi = 0;
     #pragma unroll
                 for (int ia = 0; ia < 5; ++ia)
     #pragma unroll
                     for (int ja = 0; ja < 5; ++ja) {
                         const float sxy = ox2[ia] + oy2[ja];
+                        const float tl = lo - sxy, th = hi - sxy;
     #pragma unroll
                         for (int kk = 0; kk < 5; ++kk) {
-                            const float sd = sxy + oz2[kk];
-                            cnt += sd < lo;
-                            amb |= (sd >= lo) & (sd <= hi);
+                            cnt += oz2[kk] < tl;
+                            cnt_hi += oz2[kk] <= th;
                         }
                     }
-                if (amb) {
+                if (cnt_hi != cnt) {
                     s_amb[atomicAdd(&s_na, 1)] = e;
                 } else if (cnt > 0) {   // eps = 0 never beats the empty cell (strict >)
                     atomicMax(a.key + __float_as_uint(o.w), ((uint32_t)cnt << 24) | gbits);
