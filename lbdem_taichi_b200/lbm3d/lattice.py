@@ -41,6 +41,14 @@ C_Q = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 
 QINV = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17])
 
 
+def _mirror_table(axis):
+    """Index of the direction with c's `axis` component negated (the
+    free-slip reflection tables qsyx / qsyy / qsyz, lbm_solver3d.py:50-57)."""
+    flip = C_Q.copy()
+    flip[:, axis] *= -1
+    return np.array([int(np.flatnonzero((C_Q == v).all(axis=1))[0]) for v in flip], dtype=np.int32)
+
+
 def to_ref(a):
     """device order (..., z, y, x) -> reference order (x, y, z, ...)."""
     a = np.asarray(a)
@@ -137,6 +145,7 @@ class LatticeEngine:
     c = C_Q
     w = W
     qinv = QINV
+    qsyx, qsyy, qsyz = _mirror_table(0), _mirror_table(1), _mirror_table(2)
     cssq = 1.0 / 3.0
     velmax = (2.0 / 3.0) ** 0.5
     SmagorinskyConstant = 0.1
