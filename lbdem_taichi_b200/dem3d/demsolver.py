@@ -18,6 +18,7 @@ import torch
 
 from .. import _native as N
 from .demconfig import DEMSolverConfig, HertzContactConfig, LinearContactConfig
+from .p4io import read_p4p, write_p4c, write_p4p
 
 DEV = "cuda"
 
@@ -133,33 +134,9 @@ class DEMSolver:
         """Read a p4p file (demsolver.py:130-309: single-space separated,
         1-based IDs) and allocate the device state."""
         N.require_cuda()
-        with open(file_name, encoding="UTF-8") as fp:
-            fp.readline()
-            n = int(fp.readline().removesuffix("\n").split(" ")[1])
-            fp.readline()
-            rows = []
-            for _ in range(n):
-                line = fp.readline()
-                if line == "":
-                    break
-                rows.append(line.split(" "))
-        ID = np.zeros(n, np.int64)
-        group = np.zeros(n, np.int64)
-        radius = np.zeros(n)
-        mass = np.zeros(n)
-        pos = np.zeros((n, 3))
-        vel = np.zeros((n, 3))
-        density = 0.0
-        for tok in rows:
-            i = int(tok[0]) - 1
-            ID[i] = int(tok[0])
-            group[i] = int(tok[1])
-            radius[i] = float(tok[2])
-            mass[i] = float(tok[3])
-            pos[i] = [float(tok[4]), float(tok[5]), float(tok[6])]
-            vel[i] = [float(tok[7]), float(tok[8]), float(tok[9])]
-            density = 3 * mass[i] / (4 * math.pi * radius[i] ** 3)
-        self._allocate(ID, group, radius, mass, pos, vel, density, domain_min, domain_max)
+        p = read_p4p(file_name)
+        self._allocate(p["ID"], p["group"], p["radius"], p["mass"], p["pos"], p["vel"], p["density"], domain_min,
+                       domain_max)
 
     def init_particle_arrays(self, radius, mass, pos, vel, domain_min, domain_max, ID=None, group=None):
         """Same as init_particle_fields, from arrays instead of a p4p file."""
@@ -412,21 +389,12 @@ class DEMSolver:
     def save_single(self, p4pfile, p4cfile, t: float):
         """Append one p4p/p4c frame (demsolver.py:59-128 format)."""
         tk1 = time.time()
-        n = self.n
-        p4pfile.write("TIMESTEP  PARTICLES\n")
-        p4pfile.write(f"{t} {n}\n")
-        p4pfile.write("ID  GROUP  RAD  MASS  PX  PY  PZ  VX  VY  VZ\n")
         g = self.gf
         ID = g.ID.to_numpy()
-        pos, vel = g.position.to_numpy(), g.velocity.to_numpy()
-        data = np.column_stack([ID, g.groupID.to_numpy(), g.radius.to_numpy(), g.mass.to_numpy(),
-                                pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2]])
-        np.savetxt(p4pfile, data, fmt="%d %d %.6e %.6e %.6e %.6e %.6e %.6e %.6e %.6e")
+        write_p4p(p4pfile, t, ID, g.groupID.to_numpy(), g.radius.to_numpy(), g.mass.to_numpy(),
+                  g.position.to_numpy(), g.velocity.to_numpy())
+        # contact rows by (P1, P2): the reference's slot order follows the
+        # order of atomic appends, which no run fixes
         con = self.active_contacts()
-        p4cfile.write("TIMESTEP  CONTACTS\n")
-        p4cfile.write(f"{t} {len(con)}\n")
-        p4cfile.write("P1  P2  CX  CY  CZ  FX  FY  FZ\n")
-        if con:
-            rows = [[ID[i], ID[j], *p, *f] for (i, j), (p, f, _) in sorted(con.items())]
-            np.savetxt(p4cfile, np.array(rows), fmt="%d %d %.6e %.6e %.6e %.6e %.6e %.6e")
+        write_p4c(p4cfile, t, [[ID[i], ID[j], *p, *f] for (i, j), (p, f, _) in sorted(con.items())])
         print(f"save time cost = {time.time() - tk1:.3f}s")

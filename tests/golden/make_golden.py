@@ -588,12 +588,39 @@ def scen_open_smag():
          nsteps=np.int64(4), **init, **out)
 
 
+def scen_p4io():
+    """DEMSolver.save_single (demsolver.py:59-128) after 20 sub-steps of the
+    DEM scenario: the text of one p4p and one p4c frame and the arrays it was
+    written from (the active contacts in the reference's slot order)."""
+    import io
+    rng = np.random.default_rng(21)
+    pos, rad, vel, omg = _dem_particles(rng)
+    domain = (0.0, 40.0, 0.0, 30.0, 0.0, 30.0)
+    dem = make_dem(domain, 0.05, (0.0, 0.0, -2e-3),
+                   HertzContactConfig(pp_friction=0.3, pw_friction=0.4, pp_restitution=0.9, pw_restitution=0.8),
+                   rad, 2.0, pos, vel, omega=omg, periodic=(True, False, False), E=1e3, nu=0.3, wall_E=2e3,
+                   wall_nu=0.25, model="hertz")
+    for _ in range(20):
+        dem.run_simulation()
+    p4p, p4c = io.StringIO(), io.StringIO()
+    t = 1.25
+    dem.save_single(p4p, p4c, t)
+    cf = dem.cf
+    act = cf.isActive.to_numpy().astype(bool)
+    gf = dem.gf
+    save("p4io", p4p=np.array(p4p.getvalue()), p4c=np.array(p4c.getvalue()), t=np.float64(t),
+         ID=gf.ID.to_numpy(), group=gf.groupID.to_numpy(), radius=gf.radius.to_numpy(), mass=gf.mass.to_numpy(),
+         position=gf.position.to_numpy(), velocity=gf.velocity.to_numpy(), ci=cf.i.to_numpy()[act],
+         cj=cf.j.to_numpy()[act], cpos=cf.position.to_numpy()[act], cforce=cf.force_a.to_numpy()[act])
+
+
 SCENARIOS = {
     "bgk_smag": scen_bgk_smag, "forced": scen_forced, "psc": scen_psc, "hybrid": scen_hybrid,
     "dem_hertz": scen_dem_hertz, "dem_linear": scen_dem_linear, "coupled": scen_coupled,
     "couette_ladd": scen_couette_ladd, "open_x": scen_open_x, "open_y": scen_open_y, "open_z": scen_open_z,
     "open_xr": scen_open_xr, "open_exit_x": scen_open_exit_x, "open_exit_z": scen_open_exit_z,
     "open_yr": scen_open_yr, "open_zb": scen_open_zb, "open_slip": scen_open_slip, "open_smag": scen_open_smag,
+    "p4io": scen_p4io,
 }
 
 if __name__ == "__main__":
