@@ -150,12 +150,12 @@ class DEMSolverConfig:
     def summary(self) -> str:
         m = self.contact_model
         s = (f"\nDEM Solver Configuration:\n========================\n"
-             f"Domain: [{self.domain.xmin}, {self.domain.xmax}] x [{self.domain.ymin}, {self.domain.ymax}] x "
+             f"Domain: [{self.domain.xmin}, {self.domain.xmax}] \u00d7 [{self.domain.ymin}, {self.domain.ymax}] \u00d7 "
              f"[{self.domain.zmin}, {self.domain.zmax}]\nTime step: {self.dt} s\n"
-             f"Gravity: ({self.gravity.x}, {self.gravity.y}, {self.gravity.z}) m/s^2\n\n"
+             f"Gravity: ({self.gravity.x}, {self.gravity.y}, {self.gravity.z}) m/s\u00b2\n\n"
              f"Particle Properties:\n- Elastic modulus: {self.particle_props.elastic_modulus} Pa\n"
-             f"- Poisson ratio: {self.particle_props.poisson_ratio}\n- Density: {self.particle_props.density} kg/m^3\n\n"
-             f"Wall Properties:\n- Density: {self.wall_props.density} kg/m^3\n"
+             f"- Poisson ratio: {self.particle_props.poisson_ratio}\n- Density: {self.particle_props.density} kg/m\u00b3\n\n"
+             f"Wall Properties:\n- Density: {self.wall_props.density} kg/m\u00b3\n"
              f"- Elastic modulus: {self.wall_props.elastic_modulus} Pa\n"
              f"- Poisson ratio: {self.wall_props.poisson_ratio}\n\nContact Model: {m.get_model_name().upper()}\n")
         if isinstance(m, LinearContactConfig):

@@ -614,13 +614,65 @@ def scen_p4io():
          cj=cf.j.to_numpy()[act], cpos=cf.position.to_numpy()[act], cforce=cf.force_a.to_numpy()[act])
 
 
+def scen_host_api():
+    """Host-side helpers drivers use (lbmutils.py:14-63, demconfig.py,
+    types.py, contact_model.py): UnitConverter conversions, the configuration
+    state after the setters, summary() text, and which inputs raise."""
+    from src.lbm3d.lbmutils import UnitConverter
+    uc = UnitConverter(2e-3, 1e-4, 1000.0)
+    names = [m for m in dir(UnitConverter) if m.startswith(("getLb", "getPhys"))]
+    conv = np.array([[getattr(uc, m)(v) for v in (0.5, 3.0)] for m in names])
+    cfg = DEMSolverConfig(domain=DomainBounds(0.0, 1.0, 0.0, 2.0, -1.0, 3.0), dt=1e-4,
+                          gravity=Vector3(0.0, 0.0, -9.81),
+                          contact_model=HertzContactConfig(pp_friction=0.3, pw_friction=0.4, pp_restitution=0.9,
+                                                           pw_restitution=0.8))
+    cfg.set_particle_properties(elastic_modulus=1e6, poisson_ratio=0.25, density=2650.0, max_coordinate_number=12)
+    cfg.set_wall_properties(density=2500.0, elastic_modulus=2e6, poisson_ratio=0.3)
+    cfg.set_periodic_boundaries(True, False, True)
+    cfg.update_contact_model(pp_friction=0.5)
+    lin = DEMSolverConfig(domain=DomainBounds(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), dt=2e-4, gravity=Vector3(0.0, -1.0, 0.0),
+                          contact_model=LinearContactConfig(stiffness_normal=1e5, stiffness_tangential=5e4,
+                                                            damping_normal=0.1, damping_tangential=0.05,
+                                                            pp_friction=0.2, pw_friction=0.3))
+
+    def raises(fn):
+        try:
+            fn()
+        except ValueError:
+            return True
+        return False
+
+    bad = np.array([
+        raises(lambda: DomainBounds(1.0, 0.0, 0.0, 1.0, 0.0, 1.0)),
+        raises(lambda: DEMSolverConfig(DomainBounds(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), 0.0, Vector3(0.0, 0.0, 0.0),
+                                       HertzContactConfig(0.3, 0.3, 0.9, 0.9))),
+        raises(lambda: cfg.set_particle_properties(bogus=1.0)),
+        raises(lambda: cfg.set_wall_properties(bogus=1.0)),
+        raises(lambda: cfg.update_contact_model(bogus=1.0)),
+        raises(lambda: HertzContactConfig(1.5, 0.3, 0.9, 0.9).validate()),
+        raises(lambda: HertzContactConfig(0.3, 0.3, 1.2, 0.9).validate()),
+        raises(lambda: LinearContactConfig(-1.0, 1.0, 0.1, 0.1, 0.3, 0.3).validate()),
+        raises(lambda: LinearContactConfig(1.0, 1.0, -0.1, 0.1, 0.3, 0.3).validate()),
+        raises(lambda: LinearContactConfig(1.0, 1.0, 0.1, 0.1, 0.3, 1.3).validate()),
+    ])
+    pp, wp = cfg.particle_props, cfg.wall_props
+    save("host_api", conv_names=np.array(names), conv=conv, boundary_type=np.array(cfg.boundaryType),
+         wall_normals=np.array([np.asarray(v, float) for v in cfg.wall_normals]),
+         wall_distances=np.array(cfg.wall_distances, float), domain_min=np.asarray(cfg.domain_min, float),
+         domain_max=np.asarray(cfg.domain_max, float),
+         particle_props=np.array([pp.elastic_modulus, pp.poisson_ratio, pp.density, pp.max_coordinate_number], float),
+         wall_props=np.array([wp.density, wp.elastic_modulus, wp.poisson_ratio], float),
+         pp_friction=np.float64(cfg.contact_model.pp_friction), summary_hertz=np.array(cfg.summary()),
+         summary_linear=np.array(lin.summary()), raises=bad)
+
+
 SCENARIOS = {
     "bgk_smag": scen_bgk_smag, "forced": scen_forced, "psc": scen_psc, "hybrid": scen_hybrid,
     "dem_hertz": scen_dem_hertz, "dem_linear": scen_dem_linear, "coupled": scen_coupled,
     "couette_ladd": scen_couette_ladd, "open_x": scen_open_x, "open_y": scen_open_y, "open_z": scen_open_z,
     "open_xr": scen_open_xr, "open_exit_x": scen_open_exit_x, "open_exit_z": scen_open_exit_z,
     "open_yr": scen_open_yr, "open_zb": scen_open_zb, "open_slip": scen_open_slip, "open_smag": scen_open_smag,
-    "p4io": scen_p4io,
+    "p4io": scen_p4io, "host_api": scen_host_api,
 }
 
 if __name__ == "__main__":
