@@ -32,7 +32,7 @@ import torch
 from .. import _native as N
 from ..dem3d.demsolver import DEMSolver
 from ..lbm3d.lattice import LatticeEngine, LatticeField, to_ref
-from ..lbm3d.lbmutils import CellType
+from ..lbm3d.lbmutils import CellType  # noqa: F401  (in the module namespace, as the reference module has it)
 
 
 class PSCLattice3D(LatticeEngine):
