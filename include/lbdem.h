@@ -354,6 +354,15 @@ int lbdem_dem_bin(lbdem_dem *D, void *stream);
 /* Kernels launched by the calling thread's last lbdem_dem_substeps (1 for the
  * single-launch form, 2 per sub-step for the split form); for launch counts. */
 int lbdem_dem_launches_last(void);
+/* nsub DEM sub-steps on the stream, in one of these forms (same contact sets
+ * and states; only the order of the atomic force sums differs):
+ *   n <= 16:  one 128-thread block, block barriers between the phases;
+ *   n <= 64:  one 512-thread block (cluster launch), block barriers;
+ *   larger, with D->sync (2 words of device memory) and all contact lanes
+ *            in one resident wave: one cooperative launch, bounded grid
+ *            barriers (LBDEM_ST_WAIT_TIMEOUT if one gives up);
+ *   otherwise two launches per sub-step (contacts, integration) in 64-thread
+ *            blocks, which also share the GPU with a step on another stream. */
 int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream);
 
 /* FP64 totals over the updated (non-skipped) cells of population buffer
