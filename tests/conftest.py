@@ -12,6 +12,14 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built sm_100a library")
 
 
+def pytest_sessionstart(session):
+    # a fresh tree: build the sm_100a library once (nvcc cross-compiles
+    # without a GPU); a prebuilt library is used as it is
+    from lbdem_taichi_b200 import build as B
+    if not os.path.exists(B.LIB):
+        B.build()
+
+
 def _has_cuda():
     try:
         import torch
