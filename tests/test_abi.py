@@ -103,3 +103,21 @@ def test_ctypes_descriptors_match_the_header():
         assert got[(cname, "size")] == C.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_binding_raises_with_the_library_message():
+    """A non-zero return code becomes LbdemError carrying the function name,
+    the code and the library's last error (no device work is attempted: the
+    argument checks come first)."""
+    from lbdem_taichi_b200 import _native as N
+    L = N.Lattice()
+    L.nx, L.ny, L.nz = 8, 8, 8
+    L.storage, L.omega0, L.scale16 = N.F32, 1.6, 1.0
+    L.links, L.status = 8, 8
+    with pytest.raises(N.LbdemError) as ei:
+        N.call("lbdem_psc_step_f32", C.byref(L), None, None, 0, 0, 1, None)   # src == dst
+    msg = str(ei.value)
+    assert "lbdem_psc_step_f32" in msg and f"code {N.LBDEM_ERR_ARG}" in msg
+    assert "distinct" in msg
+    with pytest.raises(N.LbdemError, match="dem: bad descriptor"):
+        N.call("lbdem_dem_substeps", None, 1, None)
