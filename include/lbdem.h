@@ -380,13 +380,16 @@ int lbdem_global_sums_f64(const lbdem_lattice *L, int32_t buf, double *out, doub
  * ABI with buffers lent by another component, or a process whose GPU memory is
  * fully reserved by a framework's caching allocator.  No counterpart in the
  * reference.  The block partials live in a library-owned device array of
- * 4 * 4096 doubles (32 KB, held by every GPU that loads the library until the
- * process exits), which covers lattices of up to 2^28 cells; larger lattices
- * return LBDEM_ERR_ARG.  The first call on a device looks up that array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  Every call shares the array: calls that may overlap on the GPU
- * (different streams without ordering) race; each call overwrites every
- * partial it reads, so no clearing is needed between calls. */
+ * 4 * 2048 doubles (64 KB, held by every GPU that loads the library until the
+ * process exits), which covers lattices of up to 2^26 = 67,108,864 cells
+ * (512 x 512 x 256); larger lattices return LBDEM_ERR_ARG before any device
+ * work.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture; the
+ * address is kept for the life of the process, so a device that the caller
+ * resets (cudaDeviceReset) must not be given to this function again.  Every
+ * call shares the array: calls that may overlap on the GPU (different streams
+ * without ordering) race; each call overwrites every partial it reads, so no
+ * clearing is needed between calls. */
 int lbdem_global_sums_f64_noalloc(const lbdem_lattice *L, int32_t buf, double *out, void *stream);
 
 #ifdef __cplusplus

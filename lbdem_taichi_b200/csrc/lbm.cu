@@ -1558,16 +1558,24 @@ static int launch_sums(const lbdem_lattice *L, int buf, double *out, double *par
 // Allocation-free FP64 totals: the block partials live in a file-scope device
 // array instead of caller scratch.  One block per NOALLOC_CELLS_PER_BLOCK
 // cells, at most NOALLOC_MAX_BLOCKS blocks, so lattices of up to
-// 4096 * 65536 = 2^28 cells are covered (32 KB of device memory, held by every
-// GPU that loads the library until the process exits).
+// 2048 * 32768 = 2^26 = 67,108,864 cells (512 x 512 x 256) are covered; the
+// array is 4 * 2048 doubles = 64 KB of device memory, held by every GPU that
+// loads the library until the process exits.  Larger lattices are refused
+// before any device work (the 32-bit element offsets of fill_args allow up to
+// about 2.26e8 cells, so this limit is the one that binds).
 // ---------------------------------------------------------------------------
-constexpr int NOALLOC_MAX_BLOCKS = 4096;
-constexpr size_t NOALLOC_CELLS_PER_BLOCK = 65536;
+constexpr int NOALLOC_MAX_BLOCKS = 2048;
+constexpr size_t NOALLOC_CELLS_PER_BLOCK = 32768;
+static_assert((size_t)NOALLOC_MAX_BLOCKS * NOALLOC_CELLS_PER_BLOCK < (1ull << 32) / Q,
+              "the allocation-free limit must bind before the 32-bit offset limit of fill_args");
 static __device__ __align__(256) double g_noalloc_partials[4 * NOALLOC_MAX_BLOCKS];
 
-// Device address of g_noalloc_partials for the current device, looked up once
-// per device (the host-side symbol is only a stand-in and must never be passed
-// to a kernel).
+// Device address of g_noalloc_partials for the current device, looked up on
+// the first call on each device (the host-side symbol is only a stand-in and
+// must never be passed to a kernel).  The cached address belongs to the
+// device's primary context: after cudaDeviceReset on that device it is stale,
+// so a caller that resets a device must not call the allocation-free sums on
+// it again in the same process.
 static double *noalloc_partials_address() {
     static std::mutex mu;
     static double *addr[256] = {};
@@ -1601,7 +1609,7 @@ static int launch_sums_noalloc(const lbdem_lattice *L, int buf, double *out, cud
     const size_t nb = (a.nc + NOALLOC_CELLS_PER_BLOCK - 1) / NOALLOC_CELLS_PER_BLOCK;
     if (nb > (size_t)NOALLOC_MAX_BLOCKS) {
         set_error("global_sums_f64_noalloc: lattice has %zu cells; the allocation-free sums cover at most %zu "
-                  "cells (use lbdem_global_sums_f64 with caller scratch)",
+                  "cells (64 KB static scratch; use lbdem_global_sums_f64 with caller scratch)",
                   a.nc, (size_t)NOALLOC_MAX_BLOCKS * NOALLOC_CELLS_PER_BLOCK);
         return LBDEM_ERR_ARG;
     }
