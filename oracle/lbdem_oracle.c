@@ -131,50 +131,128 @@ static void solid_vel(const orc_lat *L, const orc_grains *G, long c, int i, int 
  * sub-sample count).  The weighting factor B is computed in orc_collide from
  * the relaxation frequency in force at collision time (hybridlattice.py:236-245,
  * which equals psclattice3d.py:144-155 whenever omega is not updated). */
-void orc_grains2lattice(orc_lat *L, const orc_grains *G) {
-    long nc = (long)L->nx * L->ny * L->nz;
+/* The body of the reference's per-cell grain loop (psclattice3d.py:100-138)
+ * for one grain g; returns 1 when the loop breaks (full cover). */
+static inline int map_visit(orc_lat *L, const orc_grains *G, long c, int i, int j, int k, int g) {
     const double half_diag = 0.5 * sqrt(3.0);
+    double xc = (G->pos[3 * g + 0] - L->xmin + 0.5 * L->dx) / L->dx;
+    double yc = (G->pos[3 * g + 1] - L->ymin + 0.5 * L->dx) / L->dx;
+    double zc = (G->pos[3 * g + 2] - L->zmin + 0.5 * L->dx) / L->dx;
+    double r = (G->radius[g] - 0.5 * L->dx) / L->dx;
+    double dxv = xc - i, dyv = yc - j, dzv = zc - k;
+    double dist = sqrt(dxv * dxv + dyv * dyv + dzv * dzv);
+    if (dist >= r + half_diag) return 0;
+    if (dist <= r - half_diag) {
+        L->id[c] = g;
+        L->volfrac[c] = 1.0;
+        solid_vel(L, G, c, i, j, k, g, xc, yc, zc);
+        return 1;
+    }
+    int cnt = 0;
+    for (int ii = 0; ii < 5; ii++)
+        for (int jj = 0; jj < 5; jj++)
+            for (int kk = 0; kk < 5; kk++) {
+                double sx = xc - ((double)i - 0.4 + 0.2 * ii);
+                double sy = yc - ((double)j - 0.4 + 0.2 * jj);
+                double sz = zc - ((double)k - 0.4 + 0.2 * kk);
+                if (sqrt(sx * sx + sy * sy + sz * sz) < r) cnt++;
+            }
+    double eps = cnt / 125.0;
+    if (eps > L->volfrac[c]) {
+        L->id[c] = g;
+        L->volfrac[c] = eps;
+        solid_vel(L, G, c, i, j, k, g, xc, yc, zc);
+    }
+    return 0;
+}
+
+static inline void map_reset(orc_lat *L, long c) {
+    L->id[c] = -1;
+    L->volfrac[c] = 0.0;
+    L->weight[c] = 0.0;
+    L->velsolid[3 * c] = L->velsolid[3 * c + 1] = L->velsolid[3 * c + 2] = 0.0;
+}
+
+/* The reference's form: every cell visits every grain in id order. */
+void orc_grains2lattice_all(orc_lat *L, const orc_grains *G) {
+    long nc = (long)L->nx * L->ny * L->nz;
 #pragma omp parallel for schedule(dynamic, 64)
     for (long c = 0; c < nc; c++) {
         int i = (int)(c / ((long)L->ny * L->nz));
         int j = (int)((c / L->nz) % L->ny);
         int k = (int)(c % L->nz);
-        L->id[c] = -1;
-        L->volfrac[c] = 0.0;
-        L->weight[c] = 0.0;
-        L->velsolid[3 * c] = L->velsolid[3 * c + 1] = L->velsolid[3 * c + 2] = 0.0;
+        map_reset(L, c);
         if (skip_cell(L, L->ct[c])) continue;
-        for (int g = 0; g < G->n; g++) {
-            double xc = (G->pos[3 * g + 0] - L->xmin + 0.5 * L->dx) / L->dx;
-            double yc = (G->pos[3 * g + 1] - L->ymin + 0.5 * L->dx) / L->dx;
-            double zc = (G->pos[3 * g + 2] - L->zmin + 0.5 * L->dx) / L->dx;
-            double r = (G->radius[g] - 0.5 * L->dx) / L->dx;
-            double dxv = xc - i, dyv = yc - j, dzv = zc - k;
-            double dist = sqrt(dxv * dxv + dyv * dyv + dzv * dzv);
-            if (dist >= r + half_diag) continue;
-            if (dist <= r - half_diag) {
-                L->id[c] = g;
-                L->volfrac[c] = 1.0;
-                solid_vel(L, G, c, i, j, k, g, xc, yc, zc);
-                break;
-            }
-            int cnt = 0;
-            for (int ii = 0; ii < 5; ii++)
-                for (int jj = 0; jj < 5; jj++)
-                    for (int kk = 0; kk < 5; kk++) {
-                        double sx = xc - ((double)i - 0.4 + 0.2 * ii);
-                        double sy = yc - ((double)j - 0.4 + 0.2 * jj);
-                        double sz = zc - ((double)k - 0.4 + 0.2 * kk);
-                        if (sqrt(sx * sx + sy * sy + sz * sz) < r) cnt++;
-                    }
-            double eps = cnt / 125.0;
-            if (eps > L->volfrac[c]) {
-                L->id[c] = g;
-                L->volfrac[c] = eps;
-                solid_vel(L, G, c, i, j, k, g, xc, yc, zc);
-            }
-        }
+        for (int g = 0; g < G->n; g++)
+            if (map_visit(L, G, c, i, j, k, g)) break;
     }
+}
+
+/* Same result as orc_grains2lattice_all at a cost that does not grow with
+ * cells x grains: each cell visits, in id order, only the grains listed for
+ * its 8^3-cell bin.  A grain is listed for every bin that meets the box
+ * [c - reach - 1, c + reach + 1] around its lattice centre c, reach = r +
+ * sqrt(3)/2; every cell outside that box has dist >= reach, which is exactly
+ * the reference's skip test (psclattice3d.py:110), so the grains left out are
+ * the ones whose visit would `continue` -- the visits that remain, their order
+ * and the break are unchanged.  A grain with reach <= 0 or a non-finite centre
+ * is skipped by the reference for every cell (and changes no cell) and is
+ * listed nowhere; an infinite reach lists the grain everywhere. */
+#define MAP_BIN 8
+void orc_grains2lattice(orc_lat *L, const orc_grains *G) {
+    const int bx = (L->nx + MAP_BIN - 1) / MAP_BIN, by = (L->ny + MAP_BIN - 1) / MAP_BIN,
+              bz = (L->nz + MAP_BIN - 1) / MAP_BIN;
+    const long nbin = (long)bx * by * bz;
+    const double half_diag = 0.5 * sqrt(3.0);
+    long *start = (long *)calloc((size_t)nbin + 1, sizeof(long));
+    int *lo = (int *)malloc(sizeof(int) * 6 * (size_t)(G->n > 0 ? G->n : 1));
+    for (int g = 0; g < G->n; g++) {
+        double c3[3] = {(G->pos[3 * g + 0] - L->xmin + 0.5 * L->dx) / L->dx,
+                        (G->pos[3 * g + 1] - L->ymin + 0.5 * L->dx) / L->dx,
+                        (G->pos[3 * g + 2] - L->zmin + 0.5 * L->dx) / L->dx};
+        double reach = (G->radius[g] - 0.5 * L->dx) / L->dx + half_diag;
+        const int nn[3] = {L->nx, L->ny, L->nz};
+        int *b = lo + 6 * g;
+        int empty = !(reach > 0.0) || !isfinite(c3[0]) || !isfinite(c3[1]) || !isfinite(c3[2]);
+        for (int a = 0; a < 3 && !empty; a++) {
+            double l = floor(c3[a] - reach) - 1.0, h = ceil(c3[a] + reach) + 1.0;
+            if (h < 0.0 || l > (double)(nn[a] - 1)) { empty = 1; break; }
+            int il = l < 0.0 ? 0 : (int)l, ih = h > (double)(nn[a] - 1) ? nn[a] - 1 : (int)h;
+            b[2 * a] = il / MAP_BIN;
+            b[2 * a + 1] = ih / MAP_BIN;
+        }
+        if (empty) { b[0] = 1; b[1] = 0; continue; }
+        for (int x = b[0]; x <= b[1]; x++)
+            for (int y = b[2]; y <= b[3]; y++)
+                for (int z = b[4]; z <= b[5]; z++) start[((long)x * by + y) * bz + z + 1]++;
+    }
+    for (long t = 0; t < nbin; t++) start[t + 1] += start[t];
+    int *list = (int *)malloc(sizeof(int) * (size_t)(start[nbin] > 0 ? start[nbin] : 1));
+    long *fill = (long *)malloc(sizeof(long) * (size_t)nbin);
+    memcpy(fill, start, sizeof(long) * (size_t)nbin);
+    for (int g = 0; g < G->n; g++) {   /* ascending g: every list is in id order */
+        const int *b = lo + 6 * g;
+        if (b[0] > b[1]) continue;
+        for (int x = b[0]; x <= b[1]; x++)
+            for (int y = b[2]; y <= b[3]; y++)
+                for (int z = b[4]; z <= b[5]; z++) list[fill[((long)x * by + y) * bz + z]++] = g;
+    }
+    long nc = (long)L->nx * L->ny * L->nz;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long c = 0; c < nc; c++) {
+        int i = (int)(c / ((long)L->ny * L->nz));
+        int j = (int)((c / L->nz) % L->ny);
+        int k = (int)(c % L->nz);
+        map_reset(L, c);
+        if (skip_cell(L, L->ct[c])) continue;
+        long t = ((long)(i / MAP_BIN) * by + j / MAP_BIN) * bz + k / MAP_BIN;
+        for (long e = start[t]; e < start[t + 1]; e++)
+            if (map_visit(L, G, c, i, j, k, list[e])) break;
+    }
+    free(fill);
+    free(list);
+    free(lo);
+    free(start);
 }
 
 /* psclattice3d.py:187-261 (PSC), hybridlattice.py:450-503 (PSC after

@@ -42,6 +42,7 @@ def lib():
         for fn in ("orc_initialize", "orc_collide", "orc_stream"):
             getattr(_lib, fn).argtypes = [C.c_void_p]
         _lib.orc_grains2lattice.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.orc_grains2lattice_all.argtypes = [C.c_void_p, C.c_void_p]
         _lib.orc_lattice2grains.argtypes = [C.c_void_p, C.c_void_p]
         _lib.orc_global_sums.argtypes = [C.c_void_p, C.c_void_p]
         _lib.orc_dem_run_simulation.argtypes = [C.c_void_p]
@@ -131,7 +132,13 @@ class OracleLattice:
         lib().orc_stream(self._bind())
 
     def grains2lattice(self, g: "OracleGrains"):
+        """psclattice3d.py:84-182, each cell visiting only the grains listed
+        for its bin (identical to ``grains2lattice_all``)."""
         lib().orc_grains2lattice(self._bind(), g._bind())
+
+    def grains2lattice_all(self, g: "OracleGrains"):
+        """psclattice3d.py:84-182 as written: every cell visits every grain."""
+        lib().orc_grains2lattice_all(self._bind(), g._bind())
 
     def lattice2grains(self, g: "OracleGrains"):
         lib().orc_lattice2grains(self._bind(), g._bind())
