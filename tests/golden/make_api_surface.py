@@ -5,7 +5,7 @@ its source with `ast` -- nothing of the reference is executed -- into
 tests/golden/api_surface.json, which tests/test_api_surface.py checks this
 package against.
 
-    python tests/golden/make_api_surface.py [/root/reference]
+    python tests/golden/make_api_surface.py <reference checkout>     (or LBDEM_REFERENCE=<checkout>)
 """
 import ast
 import glob
@@ -14,7 +14,10 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LBDEM_REFERENCE")
+if not REF or not os.path.isdir(os.path.join(REF, "src")):
+    sys.exit(f"usage: python {os.path.relpath(__file__)} <reference checkout> (or set LBDEM_REFERENCE); "
+             "the checkout must hold the reference's src/ package")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "api_surface.json")
 
 CLASSES = ("PSCLattice3D", "BasicLattice3D", "ForcedLattice3D", "DEMSolver", "DEMSolverConfig", "DomainBounds",

@@ -1,9 +1,9 @@
 """Generate golden fixtures by running the reference's OWN Python source
-(dasfadwqd/LBDEM-Taichi, read from /root/reference) under the NumPy Taichi
+(dasfadwqd/LBDEM-Taichi, from a checkout given on the command line) under the NumPy Taichi
 stand-in in ``tishim.py``.
 
 Usage (in a container that has the reference checkout):
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py <reference checkout>     (or LBDEM_REFERENCE=<checkout>)
 
 Every scenario writes ``tests/golden/<name>.npz``.  Inputs are seeded; all
 arrays keep the reference's own shapes ((Nx, Ny, Nz[, k]) for lattice fields,
@@ -34,7 +34,10 @@ import tishim  # noqa: E402
 
 ti = tishim.install()
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LBDEM_REFERENCE")
+if not REF or not os.path.isdir(os.path.join(REF, "src")):
+    sys.exit(f"usage: python {os.path.relpath(__file__)} <reference checkout> (or set LBDEM_REFERENCE); "
+             "the checkout must hold the reference's src/ package")
 sys.path.insert(0, REF)
 
 from src.lbm3d.lbm_solver3d import BasicLattice3D  # noqa: E402

@@ -1,17 +1,22 @@
-"""The bench's synthetic dense-suspension workload (256^3, 2000 spheres,
-d ~ U[8, 12], seeded random sequential addition with a 1 lu gap, velocities
-N(0, 1e-3), particle density 2.0) is what its description says, and the same
-on every call."""
+"""The synthetic dense-suspension case (256^3, 2000 spheres, d ~ U[8, 12],
+seeded random sequential addition with a 1 lu gap, velocities N(0, 1e-3),
+particle density 2.0) is what its description says, and the same on every
+call; the full-size FP64 record starts from exactly these inputs."""
+import os
+
 import numpy as np
 from scipy.spatial import cKDTree
 
-import bench
+from lbdem_taichi_b200 import cases
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def test_dense_suspension_inputs():
-    assert bench.W["key"] == "c2" and (bench.NX, bench.NY, bench.NZ) == (256, 256, 256)
-    pos, rad, vel, mass = bench.workload()
-    n = bench.NP
+    c = cases.case("c2")
+    assert c["shape"] == (256, 256, 256)
+    pos, rad, vel, mass = cases.particles(c)
+    n = c["n"]
     assert n == 2000 and pos.shape == (n, 3) and rad.shape == (n,) and vel.shape == (n, 3)
     assert rad.min() >= 4.0 and rad.max() <= 6.0 and rad.std() > 0.5
     assert (pos >= 0.0).all() and (pos <= 256.0).all()
@@ -27,7 +32,17 @@ def test_dense_suspension_inputs():
 
 
 def test_workload_is_seeded():
-    a = bench.workload()
-    b = bench.workload()
+    a = cases.particles(cases.case("c2"))
+    b = cases.particles(cases.case("c2"))
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
+
+
+def test_fp64_records_start_from_the_cases_inputs():
+    for name in ("c2", "c1"):
+        rec = np.load(os.path.join(GOLDEN, f"{name}_fp64.npz"))
+        pos, rad, vel, mass = cases.particles(cases.case(name), int(rec["seed"]))
+        np.testing.assert_array_equal(rec["pos0"], pos)
+        np.testing.assert_array_equal(rec["rad"], rad)
+        np.testing.assert_array_equal(rec["vel0"], vel)
+        np.testing.assert_array_equal(rec["mass"], mass)
