@@ -1,56 +1,104 @@
-"""The headline workload at its full size (256^3, 2000 spheres d~U[8,12],
-Hertz, body force 1e-6, tau 0.6, lagged Smagorinsky 0.1, 10 DEM sub-steps per
-step): properties that do not need the FP64 oracle, which cannot run at this
-size (its map probes every particle for every cell).
+"""Full-size cases against their FP64 oracle records.
 
-  * 16-bit storage: over 30 coupled steps the total drag per particle stays
-    within the metric's 1e-3 of the FP32 run (sum over particles of |dF_x| <=
-    1e-3 sum |F_x|; FP32 itself is held to the FP64 oracle at 1e-5 by the
-    smaller tests); BF16 within 2e-2;
-  * FP64 mass of the updated cells is conserved by the fused step to 1e-9
-    relative (periodic box, no open boundaries).
+The records (tests/golden/c2_fp64.npz, c1_fp64.npz; tests/golden/
+make_fullsize.py) are the FP64 C restatement of the reference path run on the
+same seeded inputs: the dense suspension at 256^3 with 2000 spheres over 1000
+coupled steps, and the single settling sphere over 2000 steps.
+
+Dense suspension, per storage form, errors per step against FP64 (the drag is
+the one each step's collision gives; tolerances below):
+  total drag     |sum_i F_i - sum_i F64_i| / |sum_i F64_i|, every step
+  particle drag  sum_i |F_i - F64_i| / sum_i |F64_i|, at 109 recorded steps
+  velocity       ||u - u64|| / ||u64|| over the plane z = 128 at steps 100,
+                 500, 1000
+  positions      max_i |x_i - x64_i| (lattice units) every 100 steps
+FP16 storage holds the metric's 1e-3 on the total drag over the whole run.
+BF16 storage does not reach that tolerance: its 8-bit mantissa gives a
+relative precision of 2^-9 per stored deviation, and it is held to the bound
+written below instead.
+
+Settling sphere (FP32): force and position every step.
+
+With LBDEM_PRECISION_REPORT=<path> the per-step errors are written there as
+JSON.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-N = 256
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# (total drag every step, particle drag, velocity plane, position in lu)
+TOL = {"f32": (1e-4, 1e-3, 1e-4, 1e-3),
+       "f16": (1e-3, 1e-2, 2e-3, 1e-2),
+       "bf16": (2e-2, 1e-1, 3e-2, 1e-1)}
+
+_reports = {}
 
 
-def _c2(storage):
+def _report(name, data):
+    path = os.environ.get("LBDEM_PRECISION_REPORT")
+    if not path:
+        return
+    _reports[name] = data
+    with open(path, "w") as fh:
+        json.dump(_reports, fh)
+
+
+@pytest.fixture(scope="module")
+def c2_ref():
     import bench
-    bench.W = dict(bench.WORKLOADS["c2"], key="c2")
-    bench.NX = bench.NY = bench.NZ = N
-    bench.NP, bench.SUB, bench.TAU, bench.CS = 2000, 10, 0.6, 0.1
-    pos, rad, vel, mass = bench.workload()
-    return bench.build_gpu(storage, pos, rad, vel, mass)
+    return bench.load_record(os.path.join(GOLDEN, "c2_fp64.npz"))
 
 
-def _run(storage, steps):
-    lat, dem = _c2(storage)
-    drag = []
-    for _ in range(steps):
-        lat.collide()
-        lat.stream()
-        drag.append(dem.gf.force_fluid.to_numpy()[:, 0].copy())
-        dem.run_substeps(10)
-    lat.check_status()
-    dem.check_status()
-    return lat, np.array(drag)
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_dense_suspension_against_fp64(storage, c2_ref):
+    import bench
+    from lbdem_taichi_b200 import cases
+    ref = c2_ref
+    c = cases.case("c2")
+    rec = bench.record_run(c, storage, (ref["pos0"], ref["rad"], ref["vel0"], ref["mass"]), int(ref["steps"]),
+                           list(ref["drag_steps"]), list(ref["state_steps"]), list(ref["plane_steps"]),
+                           int(ref["plane_axis"]), int(ref["plane_index"]))
+    e = bench.drag_errors(rec, ref)
+    _report(f"c2_{storage}", {k: [float(x) for x in v] for k, v in e.items()})
+    t_tot, t_part, t_plane, t_pos = TOL[storage]
+    worst = int(np.argmax(e["total"]))
+    assert e["total"].max() <= t_tot, f"total drag error {e['total'].max():.3e} at step {worst + 1}"
+    assert e["particle"].max() <= t_part, e["particle"].max()
+    assert e["plane"].max() <= t_plane, e["plane"]
+    assert e["position"].max() <= t_pos, e["position"]
 
 
-@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("bf16", 2e-2)])
-def test_16bit_drag_matches_fp32_at_full_size(storage, tol):
-    _, d32 = _run("f32", 30)
-    _, d16 = _run(storage, 30)
-    for s in (9, 19, 29):
-        err = np.abs(d16[s] - d32[s]).sum() / np.abs(d32[s]).sum()
-        assert err <= tol, (storage, s, err)
+def test_settling_sphere_against_fp64():
+    import bench
+    from lbdem_taichi_b200 import cases
+    ref = bench.load_record(os.path.join(GOLDEN, "c1_fp64.npz"))
+    c = cases.case("c1")
+    steps = int(ref["steps"])
+    rec = bench.record_run(c, "f32", (ref["pos0"], ref["rad"], ref["vel0"], ref["mass"]), steps,
+                           list(ref["drag_steps"]), list(ref["state_steps"]), list(ref["plane_steps"]),
+                           int(ref["plane_axis"]), int(ref["plane_index"]))
+    F, F64 = rec["drag"][:, 0], ref["drag"][:, 0].astype(np.float64)
+    # relative to the step's force, floored at 1 % of the largest (the sphere starts at rest in fluid at rest)
+    mag = np.linalg.norm(F64, axis=1)
+    ferr = np.linalg.norm(F - F64, axis=1) / np.maximum(mag, 1e-2 * mag.max())
+    perr = np.abs(rec["pos"][:, 0] - ref["pos"][:, 0]).max(axis=1)
+    _report("c1_f32", {"force": [float(x) for x in ferr], "position": [float(x) for x in perr]})
+    # the sphere settles: about 7 lu down over the run, near its terminal speed at the end
+    assert ref["pos"][-1, 0, 2] < ref["pos0"][0, 2] - 5.0
+    assert ferr.max() <= 1e-4, (ferr.max(), int(np.argmax(ferr)) + 1)
+    assert perr.max() <= 1e-5, perr.max()
 
 
 def test_mass_conservation_at_full_size():
-    lat, _ = _c2("f32")
+    from lbdem_taichi_b200 import cases
+    c = cases.case("c2")
+    lat, _ = cases.build(c, "f32", *cases.particles(c))
     m0 = lat.global_sums()[0]
     for _ in range(20):
         lat.collide()
