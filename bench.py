@@ -1,19 +1,24 @@
 """Benchmark of the resolved LBM-DEM (PSC) time step.
 
-Default workload (dense suspension, seeded synthetic input): 256^3 D3Q19
-lattice, periodic in x, y and z; 2000 spheres with diameters uniform in
-[8, 12] lattice units placed by random sequential addition (1 lu gap);
-Gaussian velocities (sigma 1e-3); density ratio 2.0; Hertz-Mindlin contacts
-(E=1e5, nu=0.3, restitution 0.9, friction 0.3); uniform body force 1e-6 (x) on
-fluid and particles; tau=0.6 with Smagorinsky Cs=0.1 (reference lagged form);
-DEM sub-cycled 10x per lattice step.  A step = map particles -> fused PSC
-collide-stream with force reduction -> 10 DEM sub-steps.  `value` times the
-product's PSCLattice3D.run(), which pipelines the steps where that is faster
-(the x-blocks no particle can reach are stepped while the DEM and the next map
-run on a second stream; identical results; `pipelined` says which form ran);
-`sequential` and `phases_ms` time the plain collide/stream/DEM loop, and the
-roofline is the fused step kernel's.  --no-pipeline times the plain loop as
-`value`.
+Default workload (dense suspension, seeded synthetic input; ``cases.py``):
+256^3 D3Q19 lattice, periodic in x, y and z; 2000 spheres with diameters
+uniform in [8, 12] lattice units placed by random sequential addition (1 lu
+gap); Gaussian velocities (sigma 1e-3); density ratio 2.0; Hertz-Mindlin
+contacts (E=1e5, nu=0.3, restitution 0.9, friction 0.3); uniform body force
+1e-6 (x) on fluid and particles; tau=0.6 with Smagorinsky Cs=0.1 (reference
+lagged form); DEM sub-cycled 10x per lattice step.  A step = map particles ->
+fused PSC collide-stream with force reduction -> 10 DEM sub-steps.
+
+`value` times the product's PSCLattice3D.run(), which pipelines the steps where
+that is faster (the x-blocks no particle can reach are stepped while the DEM
+and the next map run on a second stream; identical results; `pipelined` says
+which form ran); `sequential` and `phases_ms` time the plain collide/stream/DEM
+loop, and the roofline is the fused step kernel's.  --no-pipeline times the
+plain loop as `value`.  `storage_forms` repeats the measurement for FP32, FP16
+and BF16 population storage in the same process (the metric's two arms side by
+side) with each form's speed-ups over FP32 and, for the full-size dense
+suspension, its per-step drag error against the FP64 record of the same run
+(tests/golden/c2_fp64.npz, written by tests/golden/make_fullsize.py).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16]
     python bench.py --workload c5        # 512x512x256 channel, 20000 spheres, LES
@@ -35,53 +40,24 @@ import subprocess
 import sys
 import tempfile
 import time
+from contextlib import contextmanager
 
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "MLUPS & HBM-roofline % for D3Q19 PSC step, FP16-store vs FP32 at ≤1e-3 drag err"
-BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}   # 19 reads + 19 writes of the storage type
-# DRAM read + write per cell of the step kernel, from the ncu capture of the
-# 128^3 case (see profiles/k_psc_step_128cube_full.md), scaled by the cells of a launch
-TRAFFIC_PER_CELL = {"f32": 175.7, "f16": 85.2, "bf16": 85.2}
+from lbdem_taichi_b200 import cases  # noqa: E402
 
-# Workloads (lattice units).  c2 is the headline configuration; c5 and c1 are
-# the large channel and the single settling sphere.  Parameters the workload
-# descriptions leave open are fixed here and used identically by the oracle.
-WORKLOADS = {
-    "c2": dict(desc="dense suspension 256^3 periodic, 2000 spheres d~U[8,12], Hertz e=0.9, body force 1e-6, "
-                    "tau=0.6, Smagorinsky Cs=0.1 (lagged), 10 DEM sub-steps",
-               shape=(256, 256, 256), n=2000, dmin=8.0, dmax=12.0, gap=1.0, walls_z=False, tau=0.6, cs=0.1,
-               fluid_force=(1e-6, 0.0, 0.0), gravity=(1e-6, 0.0, 0.0), rho_p=2.0, vel_sigma=1e-3, sub=10),
-    "c5": dict(desc="large channel 512x512x256, periodic x/y, no-slip walls at z=0,255, 20000 spheres "
-                    "d~U[6,10], Hertz e=0.9, body force 1e-6, tau=0.51, Smagorinsky Cs=0.12 (lagged), "
-                    "10 DEM sub-steps",
-               shape=(512, 512, 256), n=20000, dmin=6.0, dmax=10.0, gap=0.5, walls_z=True, tau=0.51, cs=0.12,
-               fluid_force=(1e-6, 0.0, 0.0), gravity=(1e-6, 0.0, 0.0), rho_p=2.0, vel_sigma=1e-3, sub=10),
-    "c1": dict(desc="single sphere d=12 settling in 64x64x128, periodic x/y, no-slip walls at z=0,127, density "
-                    "ratio 2.5, gravity 1e-5 (-z, buoyancy-reduced on the particle), tau=0.6, Smagorinsky Cs=0.1 "
-                    "(lagged), Hertz with the bottom wall, 10 DEM sub-steps",
-               shape=(64, 64, 128), n=1, dmin=12.0, dmax=12.0, gap=0.0, walls_z=True, tau=0.6, cs=0.1,
-               fluid_force=None, gravity=(0.0, 0.0, -1e-5 * (1.0 - 1.0 / 2.5)), rho_p=2.5, vel_sigma=0.0, sub=10),
-    # the packed-bed pressure-drop driver's configuration (pressure_drop_fully.py:106-116, 120-170, 200-245):
-    # 30 x 10 x 10 particle diameters at 24 cells per diameter, tau 0.68, Re 0.8 (inlet 2.0e-3 lu), frozen
-    # bed, linear contacts, one DEM sub-step, Ladd velocity inlet at x = 0, Zou-He pressure (rho = 1) at
-    # x = Nx-1, periodic y / z; the bed is seeded random sequential addition (the driver reads a packing file)
-    "pdrop": dict(desc="packed-bed pressure drop 722x242x242, Ladd velocity inlet 2.0e-3 at x=0, Zou-He pressure "
-                       "outlet rho=1 at x=Nx-1, periodic y/z, 1500 frozen spheres d=24 (RSA, 24 lu clear of the "
-                       "inlet and outlet), tau=0.68, Smagorinsky off, linear contacts, 1 DEM sub-step",
-                  shape=(722, 242, 242), n=1500, dmin=24.0, dmax=24.0, gap=0.5, walls_z=False, tau=0.68, cs=None,
-                  fluid_force=None, gravity=(0.0, 0.0, 0.0), rho_p=2.5, vel_sigma=0.0, sub=1, u_in=2.0e-3,
-                  x_clear=24.0),
-}
-W = dict(WORKLOADS["c2"], key="c2")
-NX, NY, NZ = W["shape"]
-NP = W["n"]
-SUB = W["sub"]
-TAU = W["tau"]
-CS = W["cs"]
+METRIC = "MLUPS & HBM-roofline % for D3Q19 PSC step, FP16-store vs FP32 at ≤1e-3 drag err"
+FORMS = ("f32", "f16", "bf16")
+BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}   # 19 reads + 19 writes of the storage type
+# DRAM read + write per cell of one step-kernel launch: ncu dram__bytes_read.sum
+# + dram__bytes_write.sum of a launch on the 192^3 dense suspension (844
+# spheres, the same solid fraction), divided by its cells; populations 1.08 GB
+# (FP32) / 0.54 GB (16-bit), both beyond the 126 MB L2
+TRAFFIC_PER_CELL = {"f32": 192.4, "f16": 98.5, "bf16": 98.5}
+FIXTURE = os.path.join(ROOT, "tests", "golden", "c2_fp64.npz")
 
 
 def peaks():
@@ -93,101 +69,74 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def workload(seed=2024):
-    """Seeded inputs of the selected workload (lattice units)."""
-    from tests.gpu_util import rsa_spheres_grid   # pure numpy helper
-    rng = np.random.default_rng(seed)
-    if W["key"] == "c1":
-        pos = np.array([[NX / 2 + rng.uniform(-0.5, 0.5), NY / 2 + rng.uniform(-0.5, 0.5), NZ - 18.0]])
-        rad = np.array([0.5 * W["dmin"]])
-    elif "u_in" in W:
-        xc = W["x_clear"]
-        pos, rad = rsa_spheres_grid(rng, NP, (NX - 2 * xc, NY, NZ), W["dmin"], W["dmax"], gap=W["gap"], margin=0.5)
-        pos[:, 0] += xc
-    else:
-        zlo = 1.0 if W["walls_z"] else None
-        zhi = NZ - 1.0 if W["walls_z"] else None
-        pos, rad = rsa_spheres_grid(rng, NP, (NX, NY, NZ), W["dmin"], W["dmax"], gap=W["gap"], zmin=zlo, zmax=zhi,
-                                    margin=0.5)
-    vel = rng.normal(0.0, W["vel_sigma"], (NP, 3)) if W["vel_sigma"] > 0 else np.zeros((NP, 3))
-    mass = W["rho_p"] * 4.0 / 3.0 * np.pi * rad ** 3
-    return pos, rad, vel, mass
-
-
-def cell_types():
-    ct = np.full((NX, NY, NZ), 1, np.int32)
-    if W["walls_z"]:
-        ct[:, :, 0] = ct[:, :, -1] = 8
-    if "u_in" in W:
-        ct[0] = 262144 | 8192     # VEL_INLET_LADD | LEFT
-        ct[-1] = 256 | 4096       # Pre_ZOUHE | RIGHT
-    return ct
-
-
-def open_presets(vel, rho):
-    """Inlet velocity and outlet density of the open-boundary workload (in place)."""
-    vel[0, ..., 0] = W["u_in"]
-    rho[-1] = 1.0
-
-
-def build_gpu(storage, pos, rad, vel, mass):
-    from lbdem_taichi_b200 import Vector3
-    from lbdem_taichi_b200.dem3d.demconfig import (DEMSolverConfig, DomainBounds, HertzContactConfig,
-                                                   LinearContactConfig)
-    from lbdem_taichi_b200.dem3d.demsolver import DEMSolver
-    from lbdem_taichi_b200.lbdem.psclattice3d import PSCLattice3D
-    domain = (0.0, float(NX), 0.0, float(NY), 0.0, float(NZ))
-    opened = "u_in" in W
-    contact = (LinearContactConfig(stiffness_normal=4.5e3, stiffness_tangential=2.5e3, damping_normal=0.3,
-                                   damping_tangential=0.2, pp_friction=0.15, pw_friction=0.15) if opened else
-               HertzContactConfig(pp_friction=0.3, pw_friction=0.3, pp_restitution=0.9, pw_restitution=0.9))
-    cfg = DEMSolverConfig(DomainBounds(*domain), 1.0 / SUB, Vector3(*W["gravity"]), contact)
-    cfg.set_particle_properties(elastic_modulus=1e5, poisson_ratio=0.3, max_coordinate_number=16)
-    cfg.set_wall_properties(elastic_modulus=1e5, poisson_ratio=0.3)
-    cfg.set_periodic_boundaries(not opened, True, not W["walls_z"])
-    dem = DEMSolver(cfg)
-    dem.init_particle_arrays(rad, mass, pos, vel, Vector3(0, 0, 0), Vector3(NX, NY, NZ))
-    dem.set_contact_model("linear" if opened else "hertz")
-    if opened:
-        dem.gf.freeze.from_numpy(np.ones(len(rad), np.int32))
-    lat = PSCLattice3D(NX, NY, NZ, 1.0 / TAU, 1.0, 1.0, 1.0, dem, smagorinsky="off" if CS is None else "reference",
-                       body_force=W["fluid_force"], storage=storage)
-    if CS is not None:
-        lat.SmagorinskyConstant = CS
-    if W["walls_z"] or opened:
-        lat.CT.from_numpy(cell_types())
-    if opened:
-        v, r = lat.vel.to_numpy(), lat.rho.to_numpy()
-        open_presets(v, r)
-        lat.vel.from_numpy(v)
-        lat.rho.from_numpy(r)
-    lat.initialize()
-    return lat, dem
+# ---------------------------------------------------------------------------
+# clocks during the timed regions
+# ---------------------------------------------------------------------------
+_SAMPLER = r"""
+import sys, time
+try:
+    import pynvml as N
+    N.nvmlInit()
+    key = sys.argv[1]
+    h = N.nvmlDeviceGetHandleByUUID(key) if key.startswith("GPU-") else N.nvmlDeviceGetHandleByIndex(int(key))
+    mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+except Exception as e:
+    open(sys.argv[2], "w").write("error %s\n" % e)
+    sys.exit(0)
+out = open(sys.argv[2], "w", buffering=1)
+out.write("max %d\n" % mx)
+while True:
+    t = time.time()
+    out.write("%.6f %d %d\n" % (t, N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM),
+                                N.nvmlDeviceGetCurrentClocksEventReasons(h)))
+    time.sleep(0.002)
+"""
+_REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+            0x80: "hw_power_brake_slowdown"}
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
+    """SM clock and throttle reasons read through NVML every ~2 ms by a child
+    process (it shares no interpreter lock with the launching thread), from
+    before the warm-up to the end of the bench; summary() keeps the samples
+    that fall inside the timed windows."""
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.path = None
-
-    def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
+    def __init__(self, device):
+        self.key = self._nvml_key(device)
+        fd, self.path = tempfile.mkstemp(suffix=".clk")
         os.close(fd)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.windows = []
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "20"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            self.proc = subprocess.Popen([sys.executable, "-c", _SAMPLER, self.key, self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
-        return self
 
-    def __exit__(self, *exc):
+    @staticmethod
+    def _nvml_key(device):
+        import torch
+        try:
+            return "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [v for v in vis.split(",") if v.strip()]
+            return ids[device].strip() if device < len(ids) and ids[device].strip().isdigit() else str(device)
+
+    def wait_ready(self, timeout=15.0):
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < timeout:
+            with open(self.path) as fh:
+                if len(fh.readlines()) >= 2:
+                    return
+            time.sleep(0.05)
+
+    @contextmanager
+    def window(self):
+        t0 = time.time()
+        yield
+        self.windows.append((t0, time.time()))
+
+    def stop(self):
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -196,26 +145,28 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        if self.path and os.path.exists(self.path):
-            for line in open(self.path):
-                p = [s.strip() for s in line.split(",")]
-                if len(p) < 9:
-                    continue
-                try:
-                    sm.append(float(p[1]))
-                    mx = float(p[2])
-                except ValueError:
-                    continue
-                for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
-                                   p[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(name)
-            os.remove(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        self.stop()
+        lines = open(self.path).read().splitlines() if os.path.exists(self.path) else []
+        os.remove(self.path)
+        mx, rows = None, []
+        for ln in lines:
+            p = ln.split()
+            if p and p[0] == "max":
+                mx = float(p[1])
+            elif p and p[0] == "error":
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "error": ln[6:]}
+            elif len(p) == 3:
+                rows.append((float(p[0]), float(p[1]), int(p[2])))
+        inside = [r for r in rows if any(a <= r[0] <= b for a, b in self.windows)]
+        reasons = sorted({name for _, _, m in inside for bit, name in _REASONS.items() if m & bit})
+        sm = [r[1] for r in inside]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(sm), "source": "NVML every ~2 ms, samples inside the timed windows"}
 
 
+# ---------------------------------------------------------------------------
+# multi-GPU plumbing (replicas)
+# ---------------------------------------------------------------------------
 def max_over_ranks(x, world, device="cuda"):
     """The slowest rank's value of x (a time in ms).  Every rank calls it, in
     the same order, for every reduced quantity."""
@@ -234,49 +185,36 @@ def job_mlups(world, cells, steps, ms):
     return world * cells * steps / (ms * 1e-3) / 1e6
 
 
-def run_gpu(args):
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def measure_form(c, storage, inputs, args, world, clk, barrier):
+    """Time one storage form on case `c`: the sequential loop (per-step phase
+    and step-kernel events) and the product's run(); returns (record, lat, dem)."""
     import torch
-    import torch.distributed as dist
     from lbdem_taichi_b200 import _native as Nat
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    pos, rad, vel, mass = workload()
-    lat, dem = build_gpu(args.storage, pos, rad, vel, mass)
+    sub = c["sub"]
+    cells = int(np.prod(c["shape"]))
+    lat, dem = cases.build(c, storage, *inputs)
     st = torch.cuda.current_stream()
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    # warm-up
     for _ in range(args.warmup):
-        lat.step(SUB)
+        lat.step(sub)
     torch.cuda.synchronize()
     lat.check_status()
     dem.check_status()
-
-    # ---- device-resident throughput (inputs already in HBM).  When the
-    # populations do not exceed L2 several times over, a 256 MB buffer is
-    # rewritten between steps (outside the per-step events) to flush L2.
-    cells = NX * NY * NZ
-    pop_gb = 2 * 19 * cells * (4 if args.storage == "f32" else 2) / 1e9
+    # inputs larger than L2 several times over need no flush; otherwise a
+    # 256 MB buffer is rewritten between steps (outside the per-step events)
+    pop_gb = 2 * 19 * cells * (4 if storage == "f32" else 2) / 1e9
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda") if pop_gb <= 0.5 else None
     mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     ev_step = [(mk(), mk()) for _ in range(args.steps)]
     ev_phase = [(mk(), mk(), mk()) for _ in range(args.steps)]   # before map, after step kernel, after DEM
-    lat._kernel_events = []
+    t0, t1 = mk(), mk()
     Nat.reset_launch_count()
     barrier()
     torch.cuda.synchronize()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    cpu0 = time.perf_counter()
-    with Clocks(local) as clk:
+    with clk.window():
+        cpu0 = time.perf_counter()
         t0.record(st)
         for k in range(args.steps):
             if flush is not None:
@@ -286,7 +224,7 @@ def run_gpu(args):
             lat.collide()
             lat.stream()
             ev_phase[k][1].record(st)
-            dem.run_substeps(SUB)
+            dem.run_substeps(sub)
             ev_phase[k][2].record(st)
         t1.record(st)
         cpu_launch_ms = (time.perf_counter() - cpu0) * 1e3 / args.steps
@@ -295,23 +233,20 @@ def run_gpu(args):
     launches = Nat.launch_count()
     barrier()
     # with a flush the step time is the sum of the per-step events (map to end of DEM)
-    ms = t0.elapsed_time(t1) if flush is None else sum(a.elapsed_time(c) for a, _, c in ev_phase)
+    ms = t0.elapsed_time(t1) if flush is None else sum(a.elapsed_time(b) for a, _, b in ev_phase)
     ms_seq = ms
-    # ---- the product's run(): the sequential loop above, pipelined (the blocks
-    # no particle can reach are stepped while the DEM and the next map run on a
-    # second stream).  Needs inputs larger than L2 (no flush between steps).
     pipelined = flush is None and not args.no_pipeline
     if pipelined:
-        lat.run(40, SUB)          # run()'s automatic choice is measured here, outside the timed region
+        lat.run(40, sub)          # run()'s automatic choice is measured here, outside the timed region
         pipelined = bool(lat._pipeline_choice)
         torch.cuda.synchronize()
         Nat.reset_launch_count()
         barrier()
         torch.cuda.synchronize()
-        with Clocks(local) as clk:
+        with clk.window():
             t0.record(st)
             cpu0 = time.perf_counter()
-            lat.run(args.steps, SUB)
+            lat.run(args.steps, sub)
             t1.record(st)
             cpu_launch_ms = (time.perf_counter() - cpu0) * 1e3 / args.steps
             torch.cuda.synchronize()
@@ -320,77 +255,222 @@ def run_gpu(args):
         ms = t0.elapsed_time(t1)
     ms = max_over_ranks(ms, world)
     ms_seq = max_over_ranks(ms_seq, world)
-    kern_ms = statistics.mean(a.elapsed_time(b) for a, b in ev_step)
+    kern_ms = max_over_ranks(statistics.mean(a.elapsed_time(b) for a, b in ev_step), world)
     lbm_ms = statistics.mean(a.elapsed_time(b) for a, b, _ in ev_phase)
-    dem_ms = statistics.mean(b.elapsed_time(c) for _, b, c in ev_phase)
+    dem_ms = statistics.mean(b.elapsed_time(d) for _, b, d in ev_phase)
     lat.check_status()
     dem.check_status()
-    clocks = clk.summary()
+    peak, peak_kind = peaks()
+    bpc = BYTES_PER_CELL[storage]
+    achieved = bpc * cells / (kern_ms * 1e-3) / 1e9
+    rec = {
+        "value": round(job_mlups(world, cells, args.steps, ms), 2), "ms_per_step": round(ms / args.steps, 4),
+        "pipelined": pipelined,
+        "pipeline_probe_ms": [round(v, 4) for v in lat._pipeline_probe] if lat._pipeline_probe else None,
+        "sequential": {"value": round(job_mlups(world, cells, args.steps, ms_seq), 2),
+                       "ms_per_step": round(ms_seq / args.steps, 4)},
+        "kernel_ms": round(kern_ms, 4),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "kernel": f"lbdem_psc_step_{storage}", "kernel_ms": round(kern_ms, 4),
+                     "bytes_per_cell": bpc,
+                     "traffic": round(TRAFFIC_PER_CELL[storage] * cells / 1e9, 4),
+                     "traffic_per_cell": TRAFFIC_PER_CELL[storage],
+                     "traffic_unit": "GB per launch (ncu DRAM read+write per cell of a 192^3 launch x cells)",
+                     "traffic_over_algorithmic": round(TRAFFIC_PER_CELL[storage] / bpc, 3)},
+        "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4),
+                      f"dem_{sub}_substeps": round(dem_ms, 4), "host_launch_per_step": round(cpu_launch_ms, 4)},
+        "gpu_launches": launches,
+        "l2": (f"inputs larger than L2 (populations {pop_gb:.2f} GB); no flush" if flush is None else
+               f"populations {pop_gb:.2f} GB; L2 flushed between steps (256 MB rewrite outside the step events)"),
+    }
+    return rec, lat, dem
 
-    # ---- end to end through the public API with host buffers: every step
-    # uploads the particle state from pinned host memory and reads back the
-    # per-particle fluid force/torque and the new state
-    h_in = torch.empty((2, NP, 3), dtype=torch.float64).pin_memory()
-    h_out = torch.empty((4, NP, 3), dtype=torch.float64).pin_memory()
+
+def end_to_end(c, lat, dem, args, world, clk, barrier):
+    """The same loop through the public API with host buffers: every step
+    uploads the particle state from pinned host memory, steps, and reads back
+    the per-particle fluid force/torque and the new state."""
+    import torch
+    n = c["n"]
+    st = torch.cuda.current_stream()
+    h_in = torch.empty((2, n, 3), dtype=torch.float64).pin_memory()
+    h_out = torch.empty((4, n, 3), dtype=torch.float64).pin_memory()
     h_in[0].copy_(dem._t["position"])
     h_in[1].copy_(dem._t["velocity"])
     torch.cuda.synchronize()
     e_steps = max(1, args.steps // 2)
     barrier()
-    tw0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    for _ in range(e_steps):
-        dem._t["position"].copy_(h_in[0], non_blocking=True)
-        dem._t["velocity"].copy_(h_in[1], non_blocking=True)
-        dem._touched("position")
-        lat.step(SUB)
-        h_out[0].copy_(dem._t["force_fluid"], non_blocking=True)
-        h_out[1].copy_(dem._t["moment_fluid"], non_blocking=True)
-        h_out[2].copy_(dem._t["position"], non_blocking=True)
-        h_out[3].copy_(dem._t["velocity"], non_blocking=True)
-        st.synchronize()
-        h_in[0].copy_(h_out[2])
-        h_in[1].copy_(h_out[3])
-    e1.record(st)
-    torch.cuda.synchronize()
-    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - tw0) * 1e3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with clk.window():
+        tw0 = time.perf_counter()
+        e0.record(st)
+        for _ in range(e_steps):
+            dem._t["position"].copy_(h_in[0], non_blocking=True)
+            dem._t["velocity"].copy_(h_in[1], non_blocking=True)
+            dem._touched("position")
+            lat.step(c["sub"])
+            h_out[0].copy_(dem._t["force_fluid"], non_blocking=True)
+            h_out[1].copy_(dem._t["moment_fluid"], non_blocking=True)
+            h_out[2].copy_(dem._t["position"], non_blocking=True)
+            h_out[3].copy_(dem._t["velocity"], non_blocking=True)
+            st.synchronize()
+            h_in[0].copy_(h_out[2])
+            h_in[1].copy_(h_out[3])
+        e1.record(st)
+        torch.cuda.synchronize()
+        e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - tw0) * 1e3)
     e2e_ms = max_over_ranks(e2e_ms, world)
+    cells = int(np.prod(c["shape"]))
+    return {"value": round(job_mlups(world, cells, e_steps, e2e_ms), 2), "unit": "MLUPS",
+            "h2d_bytes_per_step": 2 * n * 3 * 8, "d2h_bytes_per_step": 4 * n * 3 * 8, "steps": e_steps}
 
-    value = job_mlups(world, cells, args.steps, ms)
-    e2e_value = job_mlups(world, cells, e_steps, e2e_ms)
-    peak, peak_kind = peaks()
-    bpc = BYTES_PER_CELL[args.storage]
-    l2_note = (f"inputs larger than L2 (populations {pop_gb:.2f} GB); no flush" if flush is None else
-               f"populations {pop_gb:.2f} GB; L2 flushed between steps (256 MB rewrite outside the step events)")
-    achieved = bpc * cells / (kern_ms * 1e-3) / 1e9
+
+def record_run(c, storage, inputs, steps, drag_steps=(), state_steps=(), plane_steps=(), plane_axis=2,
+               plane_index=0):
+    """Run case `c` for `steps` coupled steps in `storage` and record what the
+    FP64 records of tests/golden/make_fullsize.py hold: per-step total drag and
+    torque, per-particle drag at `drag_steps`, particle state at `state_steps`
+    and a velocity plane at `plane_steps`."""
+    import torch
+    lat, dem = cases.build(c, storage, *inputs)
+    n = c["n"]
+    ff, mf = dem._t["force_fluid"], dem._t["moment_fluid"]
+    tot = torch.empty((steps, 2, 3), dtype=torch.float64, device="cuda")
+    per = torch.empty((len(drag_steps), n, 3), dtype=torch.float64, device="cuda")
+    st_pos = torch.empty((len(state_steps), n, 3), dtype=torch.float64, device="cuda")
+    st_vel = torch.empty_like(st_pos)
+    dset, sset = {s: k for k, s in enumerate(drag_steps)}, {s: k for k, s in enumerate(state_steps)}
+    planes = []
+    for s in range(1, steps + 1):
+        lat.collide()
+        lat.stream()
+        tot[s - 1, 0] = ff.sum(0)
+        tot[s - 1, 1] = mf.sum(0)
+        if s in dset:
+            per[dset[s]] = ff
+        if s in plane_steps:
+            sl = [slice(None)] * 3
+            sl[plane_axis] = plane_index
+            planes.append(lat.vel.to_numpy()[tuple(sl)].astype(np.float32))
+        dem.run_substeps(c["sub"])
+        if s in sset:
+            st_pos[sset[s]] = dem._t["position"]
+            st_vel[sset[s]] = dem._t["velocity"]
+    torch.cuda.synchronize()
+    lat.check_status()
+    dem.check_status()
+    out = {"drag_total": tot[:, 0].cpu().numpy(), "torque_total": tot[:, 1].cpu().numpy(),
+           "drag": per.cpu().numpy(), "pos": st_pos.cpu().numpy(), "vel": st_vel.cpu().numpy(),
+           "u_plane": np.array(planes)}
+    del lat, dem
+    torch.cuda.empty_cache()
+    return out
+
+
+def drag_errors(rec, ref):
+    """Per-step errors of a recorded run against the FP64 record:
+    total[s] = |sum_i F_i - sum_i F64_i| / |sum_i F64_i| (the metric's total
+    particle drag), particle[k] = sum_i |F_i - F64_i| / sum_i |F64_i| at the
+    recorded drag steps, plane[k] = ||u - u64|| / ||u64|| over the velocity
+    plane, position[k] = max_i |x_i - x64_i| (lattice units)."""
+    t64 = ref["drag_total"]
+    total = np.linalg.norm(rec["drag_total"] - t64, axis=1) / np.linalg.norm(t64, axis=1)
+    d64 = ref["drag"].astype(np.float64)
+    particle = (np.linalg.norm(rec["drag"] - d64, axis=2).sum(axis=1) / np.linalg.norm(d64, axis=2).sum(axis=1))
+    out = {"total": total, "particle": particle}
+    if len(ref["u_plane"]) and len(rec["u_plane"]):
+        u64 = ref["u_plane"].astype(np.float64)
+        out["plane"] = (np.sqrt(((rec["u_plane"] - u64) ** 2).sum(axis=(1, 2, 3))) /
+                        np.sqrt((u64 ** 2).sum(axis=(1, 2, 3))))
+    if len(ref["pos"]) and len(rec["pos"]):
+        out["position"] = np.abs(rec["pos"] - ref["pos"]).max(axis=(1, 2))
+    return out
+
+
+def load_record(path):
+    d = np.load(path)
+    return {k: d[k] for k in d.files}
+
+
+def drag_summary(c, storage, ref):
+    inputs = (ref["pos0"], ref["rad"], ref["vel0"], ref["mass"])
+    rec = record_run(c, storage, inputs, int(ref["steps"]), list(ref["drag_steps"]), list(ref["state_steps"]),
+                     list(ref["plane_steps"]), int(ref["plane_axis"]), int(ref["plane_index"]))
+    e = drag_errors(rec, ref)
+    tot = e["total"]
+    worst = int(np.argmax(tot))
+    return {"drag_rel_err_vs_fp64": float(tot.max()), "worst_step": worst + 1,
+            "median": float(np.median(tot)), "steps_within_1e-3": f"{int((tot <= 1e-3).sum())}/{len(tot)}",
+            "particle_drag_rel_err_max": float(e["particle"].max()),
+            "velocity_plane_rel_err": [float(v) for v in e.get("plane", [])],
+            "steps": int(ref["steps"]),
+            "reference": "FP64 oracle record of the same run (tests/golden/c2_fp64.npz)"}
+
+
+def run_gpu(c, args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    clk = Clocks(local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    inputs = cases.particles(c)
+    clk.wait_ready()
+    head, lat, dem = measure_form(c, args.storage, inputs, args, world, clk, barrier)
+    e2e = end_to_end(c, lat, dem, args, world, clk, barrier)
+    del lat, dem
+    torch.cuda.empty_cache()
+    forms = {args.storage: head}
+    if not args.no_forms:
+        for storage in FORMS:
+            if storage not in forms:
+                forms[storage], lat, dem = measure_form(c, storage, inputs, args, world, clk, barrier)
+                del lat, dem
+                torch.cuda.empty_cache()
+    full_c2 = c["key"] == "c2" and c["shape"] == cases.CASES["c2"]["shape"] and c["n"] == cases.CASES["c2"]["n"]
+    ref = load_record(FIXTURE) if (full_c2 and not args.no_drag and os.path.exists(FIXTURE)) else None
+    storage_forms = {}
+    base = forms.get("f32")
+    for storage, r in forms.items():
+        f = {"value": r["value"], "unit": "MLUPS", "ms_per_step": r["ms_per_step"], "kernel_ms": r["kernel_ms"],
+             "roofline_frac": r["roofline"]["frac"], "achieved_gbs": r["roofline"]["achieved"],
+             "traffic_per_cell": r["roofline"]["traffic_per_cell"], "pipelined": r["pipelined"]}
+        if base is not None:
+            f["kernel_speedup_vs_f32"] = round(base["kernel_ms"] / r["kernel_ms"], 3)
+            f["step_speedup_vs_f32"] = round(base["ms_per_step"] / r["ms_per_step"], 3)
+        if ref is not None:
+            f.update(drag_summary(c, storage, ref))
+        storage_forms[storage] = f
+    cells = int(np.prod(c["shape"]))
     out = {
-        "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "metric": METRIC, "value": head["value"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
-        "config": {"workload": W["desc"], "name": W["key"],
-                   "lattice": [NX, NY, NZ], "particles": NP, "dem_subcycles": SUB, "storage": args.storage,
-                   "l2": l2_note, "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "kernel": f"lbdem_psc_step_{args.storage}", "kernel_ms": round(kern_ms, 4),
-                     "bytes_per_cell": bpc,
-                     "traffic": round(TRAFFIC_PER_CELL[args.storage] * cells / 1e9, 4),
-                     "traffic_unit": "GB per launch (DRAM read+write per cell from the 128^3 ncu capture x cells)"},
-        "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 2 * NP * 3 * 8,
-                "d2h_bytes_per_step": 4 * NP * 3 * 8},
-        "gpu_launches": launches,
-        "pipelined": pipelined,
-        "pipeline_probe_ms": [round(v, 4) for v in lat._pipeline_probe] if lat._pipeline_probe else None,
-        "sequential": {"value": round(job_mlups(world, cells, args.steps, ms_seq), 2),
-                       "ms_per_step": round(ms_seq / args.steps, 4)},
-        "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4), f"dem_{SUB}_substeps": round(dem_ms, 4),
-                      "host_launch_per_step": round(cpu_launch_ms, 4)},
-        "clocks": clocks,
+        "config": {"workload": c["desc"], "name": c["key"], "lattice": list(c["shape"]), "cells": cells,
+                   "particles": c["n"], "dem_subcycles": c["sub"], "storage": args.storage, "l2": head["l2"],
+                   "parallelism": f"replicas x{world}"},
+        "roofline": head["roofline"],
+        "e2e": e2e,
+        "gpu_launches": head["gpu_launches"],
+        "pipelined": head["pipelined"],
+        "pipeline_probe_ms": head["pipeline_probe_ms"],
+        "sequential": head["sequential"],
+        "phases_ms": head["phases_ms"],
+        "storage_forms": storage_forms,
+        "clocks": clk.summary(),
     }
-    if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(pos, rad, vel, mass, budget_s=args.cpu_seconds)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(c, inputs, budget_s=args.cpu_seconds)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -398,82 +478,106 @@ def run_gpu(args):
         print(json.dumps(out), flush=True)
 
 
-def slab_depth():
-    """z-depth of the CPU sample: the oracle maps by probing every particle for
-    every cell, so the slab keeps cells x particles near 2e8 per step."""
-    return int(max(1, min(NZ, 8, 2e8 // max(1, NX * NY * NP))))
+# ---------------------------------------------------------------------------
+# CPU arm: the FP64 C restatement of the reference path (oracle/), timed on
+# the host cores.  The reference's grains2lattice probes every particle for
+# every cell, so a full-size step is sampled: the lattice part (map with the
+# reference's all-grains loop, collision, force reduction, streaming) on a
+# z-slab of the lattice that carries every particle gives the time per cell,
+# and the DEM part (10 sub-steps of all particles) the time per step; the two
+# recombine into the full lattice's step time.
+# ---------------------------------------------------------------------------
+SLAB_Z = 4
 
 
-def cpu_sample(pos, rad, vel, mass, nz_slab):
-    """Oracle (FP64 C restatement of the reference) on a z-slab of the workload
-    carrying every particle: same per-cell work (grains2lattice probes all
-    particles for every cell), NX x NY x `nz_slab` cells."""
+def cpu_sample(c, inputs, nz_slab):
     from oracle.oracle import OracleDEM, OracleGrains, OracleLattice
-    lat = OracleLattice(NX, NY, nz_slab, 1.0 / TAU, smag=CS is not None, psc=True, force=W["fluid_force"],
-                        smag_cs=CS if CS is not None else 0.1)
-    lat.ct[...] = cell_types()[:, :, :nz_slab]
-    if "u_in" in W:
-        open_presets(lat.vel, lat.rho)
-    dem = OracleDEM(pos, vel, rad, mass, dt=1.0 / SUB, gravity=W["gravity"], domain=(0, NX, 0, NY, 0, NZ),
-                    periodic=(True, True, not W["walls_z"]), E=1e5, nu=0.3, wall_E=1e5, wall_nu=0.3, pp_mu=0.3,
-                    pw_mu=0.3, pp_e=0.9, pw_e=0.9, max_coord=16)
+    nx, ny, nz = c["shape"]
+    pos, rad, vel, mass = inputs
+    lat = OracleLattice(nx, ny, nz_slab, 1.0 / c["tau"], smag=c["cs"] is not None, psc=True,
+                        force=c["fluid_force"], smag_cs=c["cs"] if c["cs"] is not None else 0.1)
+    lat.ct[...] = cases.cell_types(c)[:, :, :nz_slab]
+    if "u_in" in c:
+        cases.open_presets(c, lat.vel, lat.rho)
+    h, e = cases.HERTZ, cases.ELASTIC
+    dem = OracleDEM(pos, vel, rad, mass, dt=1.0 / c["sub"], gravity=c["gravity"], domain=(0, nx, 0, ny, 0, nz),
+                    periodic=("u_in" not in c, True, not c["walls_z"]), E=e["E"], nu=e["nu"], wall_E=e["E"],
+                    wall_nu=e["nu"], pp_mu=h["pp_friction"], pw_mu=h["pw_friction"], pp_e=h["pp_restitution"],
+                    pw_e=h["pw_restitution"], max_coord=cases.MAX_COORD)
     g = OracleGrains(dem.pos, dem.radius, dem.vel, dem.omega)
     g.force_fluid, g.moment_fluid = dem.force_fluid, dem.moment_fluid
     lat.initialize()
     return lat, dem, g
 
 
-def cpu_step(lat, dem, g):
-    lat.grains2lattice(g)
+def cpu_step(c, lat, dem, g):
+    """(lattice seconds, DEM seconds) of one sampled step."""
+    t0 = time.perf_counter()
+    lat.grains2lattice_all(g)
     lat.collide()
     lat.lattice2grains(g)
     lat.stream()
-    for _ in range(SUB):
+    t1 = time.perf_counter()
+    for _ in range(c["sub"]):
         dem.run_simulation()
+    return t1 - t0, time.perf_counter() - t1
 
 
-def cpu_baseline(pos, rad, vel, mass, budget_s=20.0):
-    nz_slab = slab_depth()
-    lat, dem, g = cpu_sample(pos, rad, vel, mass, nz_slab)
+def _full_mlups(c, nz_slab, lat_s, dem_s):
+    """MLUPS of a full-lattice step from a slab's lattice time and a DEM time."""
+    nx, ny, nz = c["shape"]
+    cells = nx * ny * nz
+    step_s = lat_s / (nx * ny * nz_slab) * cells + dem_s
+    return cells / step_s / 1e6, step_s
+
+
+def _sample_text(c, nz_slab, steps):
+    nx, ny, _ = c["shape"]
+    return (f"{steps} sampled steps: lattice part (reference all-grains map, collide, force reduction, stream) on a "
+            f"{nx}x{ny}x{nz_slab} slab carrying all {c['n']} particles, timed per cell; DEM part ({c['sub']} "
+            f"sub-steps of all particles) timed per step; recombined for the full {c['shape'][0]}x{c['shape'][1]}x"
+            f"{c['shape'][2]} lattice; FP64 C restatement, OpenMP {os.cpu_count()} threads")
+
+
+def cpu_baseline(c, inputs, budget_s=20.0):
+    nz_slab = min(SLAB_Z, c["shape"][2])
+    lat, dem, g = cpu_sample(c, inputs, nz_slab)
+    cpu_step(c, lat, dem, g)     # first touch of the oracle's arrays
     t0 = time.perf_counter()
-    steps = 0
-    while True:
-        cpu_step(lat, dem, g)
-        steps += 1
-        if time.perf_counter() - t0 > budget_s * 0.5 or steps >= 50:
-            break
-    dt = time.perf_counter() - t0
-    cells = NX * NY * nz_slab
-    return {"value": round(cells * steps / dt / 1e6, 4), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{steps} full steps (map, collide, force reduction, stream, {SUB} DEM sub-steps) on a "
-                      f"{NX}x{NY}x{nz_slab} slab of the workload carrying all {NP} particles; FP64 C "
-                      f"restatement, OpenMP {os.cpu_count()} threads"}
+    lat_s, dem_s, steps = 0.0, 0.0, 0
+    while time.perf_counter() - t0 < budget_s * 0.5 and steps < 50:
+        a, b = cpu_step(c, lat, dem, g)
+        lat_s, dem_s, steps = lat_s + a, dem_s + b, steps + 1
+    v, step_s = _full_mlups(c, nz_slab, lat_s / steps, dem_s / steps)
+    return {"value": round(v, 4), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
+            "ms_per_full_step": round(step_s * 1e3, 1), "sample": _sample_text(c, nz_slab, steps)}
 
 
-def run_reference(args):
+def run_reference(c, args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    pos, rad, vel, mass = workload()
-    nz_slab = slab_depth()
-    lat, dem, g = cpu_sample(pos, rad, vel, mass, nz_slab)
-    for _ in range(args.warmup_ref):
-        cpu_step(lat, dem, g)
-    t0 = time.perf_counter()
-    for _ in range(args.steps_ref):
-        cpu_step(lat, dem, g)
-    dt = time.perf_counter() - t0
-    cells = NX * NY * nz_slab
-    v = cells * args.steps_ref / dt / 1e6
-    sample = f"{NX}x{NY}x{nz_slab} slab of the workload with all {NP} particles per step"
+    inputs = cases.particles(c)
+    nz_slab = min(SLAB_Z, c["shape"][2])
+    lat, dem, g = cpu_sample(c, inputs, nz_slab)
+    for _ in range(args.warmup):
+        cpu_step(c, lat, dem, g)
+    lat_s = dem_s = 0.0
+    for _ in range(args.steps):
+        a, b = cpu_step(c, lat, dem, g)
+        lat_s, dem_s = lat_s + a, dem_s + b
+    steps = max(1, args.steps)
+    v, step_s = _full_mlups(c, nz_slab, lat_s / steps, dem_s / steps)
+    sample = _sample_text(c, nz_slab, args.steps)
+    nx, ny, nz = c["shape"]
     # the GPU arm's config; the reference computes in FP64 on the host cores (no GPU)
     out = {"metric": METRIC, "value": round(v, 4), "unit": "MLUPS", "impl": "reference", "n_gpus": args.gpus,
-           "device": "cpu", "steps": args.steps_ref, "warmup": args.warmup_ref,
-           "ms_per_step": round(dt * 1e3 / args.steps_ref, 2),
+           "device": "cpu", "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(step_s * 1e3, 2),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": W["desc"], "name": W["key"], "lattice": [NX, NY, NZ], "particles": NP,
-                      "dem_subcycles": SUB, "storage": "f64", "sample": f"per step: {sample}",
-                      "parallelism": f"{os.cpu_count()} host threads"},
+           "config": {"workload": c["desc"], "name": c["key"], "lattice": [nx, ny, nz], "cells": nx * ny * nz,
+                      "particles": c["n"], "dem_subcycles": c["sub"], "storage": "f64",
+                      "sample": f"per step: {sample}", "parallelism": f"{os.cpu_count()} host threads"},
            "cpu_baseline": {"value": round(v, 4), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                             "sample": sample},
            "e2e": {"value": round(v, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -490,13 +594,13 @@ def run_reference(args):
 # differences (h = 1e-4 relative) of the oracle's forward for g_x and the K-1
 # largest position components.
 # ---------------------------------------------------------------------------
-ADJ_N, ADJ_NP, ADJ_STEPS, ADJ_EVERY, ADJ_G = 128, 500, 500, 50, 2e-6
+ADJ_N, ADJ_NP, ADJ_STEPS, ADJ_EVERY, ADJ_G, ADJ_TAU = 128, 500, 500, 50, 2e-6, 0.6
 
 
 def adjoint_workload(seed=2024):
-    from tests.gpu_util import rsa_spheres
     rng = np.random.default_rng(seed)
-    pos, rad = rsa_spheres(rng, ADJ_NP, (ADJ_N, ADJ_N, ADJ_N), 10.0, 10.0, gap=0.2, zmax=ADJ_N / 2, margin=1.0)
+    pos, rad = cases.rsa_spheres(rng, ADJ_NP, (ADJ_N, ADJ_N, ADJ_N), 10.0, 10.0, gap=0.2, zmax=ADJ_N / 2,
+                                 margin=1.0)
     ct = np.full((ADJ_N,) * 3, 1, np.int32)
     ct[:, :, 0] = ct[:, :, -1] = 8
     return pos, rad, ct
@@ -509,14 +613,13 @@ def run_adjoint(args):
     from lbdem_taichi_b200.dem3d.demconfig import HertzContactConfig
     from lbdem_taichi_b200.lbdem.adjoint import FrozenBedDrag
     from lbdem_taichi_b200.lbdem.psclattice3d import PSCLattice3D
-    from tests.gpu_util import make_dem
     pos, rad, ct = adjoint_workload()
     n = len(rad)
     mass = 2.0 * 4.0 / 3.0 * np.pi * rad ** 3
-    dem = make_dem((0.0, ADJ_N, 0.0, ADJ_N, 0.0, ADJ_N), 0.1, (0, 0, 0),
-                   HertzContactConfig(pp_friction=0.3, pw_friction=0.3, pp_restitution=0.9, pw_restitution=0.9),
-                   rad, mass, pos, np.zeros((n, 3)), periodic=(True, True, False), freeze=np.ones(n, np.int32))
-    lat = PSCLattice3D(ADJ_N, ADJ_N, ADJ_N, 1.0 / TAU, 1.0, 1.0, 1.0, dem, body_force=(ADJ_G, 0.0, 0.0),
+    dem = cases.make_dem((0.0, ADJ_N, 0.0, ADJ_N, 0.0, ADJ_N), 0.1, (0, 0, 0), HertzContactConfig(**cases.HERTZ),
+                         rad, mass, pos, np.zeros((n, 3)), periodic=(True, True, False),
+                         freeze=np.ones(n, np.int32))
+    lat = PSCLattice3D(ADJ_N, ADJ_N, ADJ_N, 1.0 / ADJ_TAU, 1.0, 1.0, 1.0, dem, body_force=(ADJ_G, 0.0, 0.0),
                        solid_fraction="smooth")
     lat.CT.from_numpy(ct)
     prob = FrozenBedDrag(lat, ADJ_STEPS, direction=(1.0, 0.0, 0.0), checkpoint_every=ADJ_EVERY)
@@ -553,7 +656,7 @@ def run_adjoint(args):
         shape = (ADJ_N,) * 3
 
         def L64(Fv, P):
-            return frozen_bed_drag(shape, 1.0 / TAU, ct, rad, P, Fv, ADJ_STEPS)
+            return frozen_bed_drag(shape, 1.0 / ADJ_TAU, ct, rad, P, Fv, ADJ_STEPS)
         t0 = time.perf_counter()
         checks = []
         h = 1e-4 * ADJ_G
@@ -580,34 +683,27 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--storage", default="f32", choices=list(FORMS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pipeline", action="store_true", help="time the sequential loop (collide, stream, DEM)")
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-forms", action="store_true", help="time only --storage, not every storage form")
+    ap.add_argument("--no-drag", action="store_true", help="skip the drag error against the FP64 record")
+    ap.add_argument("--workload", default="c2", choices=sorted(cases.CASES))
     ap.add_argument("--size", type=int, default=0, help="cube edge override; only for small profiling cases")
     ap.add_argument("--particles", type=int, default=0, help="particle count override; only for profiling")
     ap.add_argument("--adjoint", action="store_true", help="drag-gradient workload instead of the step")
     ap.add_argument("--adjoint-fd", type=int, default=0, help="FP64 finite-difference checks (count)")
     args = ap.parse_args()
-    global W, NX, NY, NZ, NP, SUB, TAU, CS
-    W = dict(WORKLOADS[args.workload], key=args.workload)
-    NX, NY, NZ = W["shape"]
-    NP, SUB, TAU, CS = W["n"], W["sub"], W["tau"], W["cs"]
-    if args.size:
-        NX = NY = NZ = args.size
-    if args.particles:
-        NP = args.particles
     if args.adjoint:
         run_adjoint(args)
         return
-    args.steps_ref = max(1, min(args.steps, 3))
-    args.warmup_ref = 1
+    c = cases.case(args.workload, args.size, args.particles)
     if args.impl == "reference":
-        run_reference(args)
+        run_reference(c, args)
     else:
-        run_gpu(args)
+        run_gpu(c, args)
 
 
 if __name__ == "__main__":
