@@ -181,6 +181,7 @@ class LatticeEngine:
         self.stress_enabled = bool(stress) or smagorinsky == "reference"
         self._aux = (torch.zeros((nblk, 5, 32), dtype=tdtype, device=dev) if self.stress_enabled else None)
         self._stress = None
+        self._stress_pending = False   # compute_stress() not evaluated yet (fused into the next collide)
         self._links = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._moving = None
         self.has_moving_walls = False
@@ -191,7 +192,8 @@ class LatticeEngine:
         self._bnd_scratch = None
         self._bnd_f0 = None
         self._has_slip = False
-        self._ct_dev = torch.zeros(nc, dtype=torch.int32, device=dev)
+        # device cell types start as FLUID, as the reference fills CT (lbm_solver3d.py:136-137)
+        self._ct_dev = torch.full((nc,), int(CellType.FLUID), dtype=torch.int32, device=dev)
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
         self._sum_out = torch.zeros(4, dtype=torch.float64, device=dev)
         self._sum_part = torch.zeros(N.SUM_PARTIALS, dtype=torch.float64, device=dev)
@@ -295,6 +297,9 @@ class LatticeEngine:
         self._vel.copy_(torch.from_numpy(from_ref(host, 3).reshape(3, -1).astype(np.float32)))
 
     def _sync_inputs(self):
+        if self._stress_pending and (self.CT._dirty or self.rho._dirty or self.vel._dirty):
+            # a pending compute_stress() belongs to the state before these writes
+            self._flush_stress()
         # the Smagorinsky constant is a class attribute in the reference
         # (lbm_solver3d.py:97, read at :508); drivers may change it on the class or the instance
         self._lat.smag_cs = float(self.SmagorinskyConstant)
@@ -372,18 +377,38 @@ class LatticeEngine:
         """Stress tensor and shear magnitude of the current (post-stream) state
         (lbm_solver3d.py:347-404): sigma = -(1 - omega/2) sum c c (f - feq),
         feq and omega of the last collision.  Needs the lagged state: construct
-        the lattice with stress=True (implied by smagorinsky="reference")."""
+        the lattice with stress=True (implied by smagorinsky="reference").
+
+        The result is that of the state at this call.  It is evaluated lazily:
+        the next collide() gathers exactly this state, so it writes the stress
+        as an optional output of the fused step (no extra pass over the
+        populations -- the reference's drivers call compute_stress() after
+        every stream); reading a stress field, a plane average, changing a
+        field or restoring a state first evaluates it in a pass of its own.
+        Lattices with open boundaries (boundary-pass cells) evaluate it at once."""
         if not self.stress_enabled:
             raise RuntimeError("construct the lattice with stress=True to keep the state compute_stress needs")
         self._sync_inputs()
-        buf = self._materialize()
         if self._stress is None:
             self._stress = torch.zeros((7, self.ncells), dtype=torch.float32, device="cuda")
+        self._stress_pending = True
+        if self.has_open_boundaries or self._collided is not None:
+            self._flush_stress()
+        for name in _STRESS_FIELDS:
+            getattr(self, name).invalidate()
+
+    def _flush_stress(self):
+        """Evaluate a pending compute_stress() now, in a pass of its own."""
+        if not self._stress_pending:
+            return
+        self._stress_pending = False
+        buf = self._materialize()
         N.call("lbdem_stress", C.byref(self._lat), buf, N.ptr(self._stress), N.stream_handle())
         for name in _STRESS_FIELDS:
             getattr(self, name).invalidate()
 
     def _pull_stress(self, m):
+        self._flush_stress()
         if self._stress is None:
             return np.zeros((self.Nx, self.Ny, self.Nz))
         return to_ref(self._stress[m].cpu().numpy().reshape(self.Nz, self.Ny, self.Nx).astype(np.float64))
@@ -392,6 +417,7 @@ class LatticeEngine:
         """Mean (xy, xz, yz) stress over the FLUID cells of the plane normal to
         `axis` at index `position` (lbm_solver3d.py:406-456); zeros for an
         empty plane.  Uses the stress of the last compute_stress()."""
+        self._flush_stress()
         if self._stress is None:
             return np.zeros(3)
         st = self._stress.view(7, self.Nz, self.Ny, self.Nx)
@@ -429,6 +455,7 @@ class LatticeEngine:
             raise ValueError("restart state is for another lattice size or storage form")
         if d["smagorinsky"] != self.smagorinsky:
             raise ValueError("restart state was taken with another Smagorinsky mode")
+        self._flush_stress()
         self._sync_inputs()
         # both buffers: cells no collision writes (walls, skipped inlets) and a
         # Ladd inlet's populations must read the same from either
@@ -453,6 +480,7 @@ class LatticeEngine:
     # ------------------------------------------------------------ kernels
     def initialize(self):
         """f = feq(rho, vel) on updated cells (lbm_solver3d.py:157-171)."""
+        self._flush_stress()
         self._sync_inputs()
         N.call("lbdem_lattice_init", C.byref(self._lat), 0, N.stream_handle())
         self._cur, self._cur_kind, self._collided = 0, "f", None
@@ -471,9 +499,18 @@ class LatticeEngine:
         else:
             src, dst, gather = self._cur, 1 - self._cur, int(self._cur_kind == "fpc")
         ev = getattr(self, "_kernel_events", None)
+        fused_stress = self._stress_pending
+        if fused_stress:
+            # the step gathers the state of the pending compute_stress(): it writes the stress too
+            self._lat.stress = N.ptr(self._stress)
         if ev:
             ev[0].record()
-        N.call(self._step_fn(), C.byref(self._lat), psc, grains, src, dst, gather, N.stream_handle())
+        try:
+            N.call(self._step_fn(), C.byref(self._lat), psc, grains, src, dst, gather, N.stream_handle())
+        finally:
+            if fused_stress:
+                self._lat.stress = None
+                self._stress_pending = False
         if ev:
             ev[1].record()
         self._collided = (src, dst, gather)
