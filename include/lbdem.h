@@ -64,7 +64,7 @@
 extern "C" {
 #endif
 
-#define LBDEM_ABI_VERSION 2
+#define LBDEM_ABI_VERSION 3
 
 /* return codes */
 #define LBDEM_OK 0
@@ -110,6 +110,9 @@ extern "C" {
 #define LBDEM_CT_FRONT 65536   /* z = Nz-1 */
 #define LBDEM_CT_BACK 131072   /* z = 0 */
 
+/* link-mask bit of a FLUID cell (the value of every mask of an all-FLUID lattice) */
+#define LBDEM_LINK_FLUID (1u << 20)
+
 typedef struct lbdem_lattice {
     int32_t nx, ny, nz;
     int32_t storage;       /* LBDEM_F32 / LBDEM_F16 / LBDEM_BF16 */
@@ -146,6 +149,17 @@ typedef struct lbdem_lattice {
                                    lattice_init or a stream call; required when bnd_nb > 0 */
     int32_t bnd_slip;           /* 1: the lattice has FREE_SLIP cells (their mirrors read inlets'
                                    post-collision populations, which are then stored) */
+    float *stress;              /* optional 7 * Ncells FP32 planes (xx, yy, zz, xy, xz, yz, shear
+                                   magnitude): when not NULL, lbdem_psc_step_* also writes the stress
+                                   diagnostics of the post-stream state it gathers (its input) -- what
+                                   lbdem_stress would give for that state, fused into the step
+                                   (BasicLattice3D.compute_stress, src/lbm3d/lbm_solver3d.py:347-404).
+                                   Needs aux; not supported with boundary-pass cells (bnd_na + bnd_nb
+                                   > 0) nor by lbdem_psc_step_phase, which ignores it. */
+    uint32_t links_all;         /* nonzero: every cell's link mask equals this value (a lattice without
+                                   walls or special cells, all FLUID: the mask lbdem_build_links gives
+                                   is then LBDEM_LINK_FLUID everywhere); the step kernels then read no
+                                   per-cell masks.  0: read links[]. */
 } lbdem_lattice;
 
 typedef struct lbdem_grains {
@@ -262,7 +276,14 @@ int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G, v
  * Smagorinsky omega -> equilibrium -> PSC / BGK collision -> body force ->
  * post-collision populations into f[dst]; hydrodynamic force and torque of
  * every particle accumulated into G->force_fluid / G->moment_fluid
- * (zeroed by lbdem_psc_map).  P/G may be NULL for a particle-free lattice. */
+ * (zeroed by lbdem_psc_map).  P/G may be NULL for a particle-free lattice.
+ * With L->stress set, the stress diagnostics of the gathered state are
+ * written too.  Two kernels implement the gathered step and give identical
+ * results: one gathers with per-thread loads; the other (rows of up to 256
+ * cells) has a producer warp copy whole upwind rows into shared memory with
+ * the tensor memory accelerator, several rows ahead of the warps that collide
+ * them.  The second is the default for 16-bit storage, the first for FP32;
+ * LBDEM_STEP_KERNEL=rows or =simt in the environment selects one for all. */
 int lbdem_psc_step_f32(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
                        int32_t dst, int32_t gather, void *stream);
 int lbdem_psc_step_f16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,

@@ -17,8 +17,9 @@ ST_NAN, ST_RHO, ST_VELMAX = 1, 2, 4
 ST_CONTACT_OVERFLOW, ST_GRID_OVERFLOW, ST_GID_OVERFLOW, ST_CELL_OVERFLOW = 8, 16, 32, 64
 ST_WAIT_TIMEOUT = 128
 ST_PIPELINE_MARGIN = 256
-ABI_VERSION = 2        # LBDEM_ABI_VERSION of include/lbdem.h
+ABI_VERSION = 3        # LBDEM_ABI_VERSION of include/lbdem.h
 F32, F16, BF16 = 0, 1, 2
+LINK_FLUID = 1 << 20   # LBDEM_LINK_FLUID: the link mask of every cell of an all-FLUID lattice
 SMAG_OFF, SMAG_REFERENCE, SMAG_LOCAL = 0, 1, 2
 SUM_BLOCKS = 1184
 SUM_PARTIALS = 4 * SUM_BLOCKS
@@ -44,7 +45,7 @@ class Lattice(C.Structure):
                 ("force_on", C.c_int32), ("force", C.c_float * 3), ("scale16", C.c_float),
                 ("f", vp * 2), ("rho", vp), ("vel", vp), ("aux", vp), ("links", vp),
                 ("status", vp), ("moving", vp), ("ct", vp), ("bnd_cells", vp), ("bnd_na", C.c_uint32),
-                ("bnd_nb", C.c_uint32), ("bnd_f0", vp), ("bnd_slip", C.c_int32)]
+                ("bnd_nb", C.c_uint32), ("bnd_f0", vp), ("bnd_slip", C.c_int32), ("stress", vp), ("links_all", C.c_uint32)]
 
 
 class Grains(C.Structure):

@@ -52,7 +52,7 @@ __host__ __device__ inline uint32_t xslot(uint32_t x, uint32_t per_block) {
 
 // Per-cell link mask (built once from CellType by lbdem_build_links)
 constexpr uint32_t LINK_SKIP = 1u << 19;   // cell is not updated (OBSTACLE / VEL_LADD / FREE_SLIP [/ INLET])
-constexpr uint32_t LINK_FLUID = 1u << 20;  // FLUID: moments are recomputed
+constexpr uint32_t LINK_FLUID = LBDEM_LINK_FLUID;  // FLUID: moments are recomputed
 constexpr uint32_t LINK_MAP_SKIP = 1u << 21;  // PSC map skips the cell
 constexpr uint32_t LINK_MOVING = 1u << 22;    // some bounce-back neighbour is a moving wall (VEL_LADD)
 __host__ __device__ constexpr uint32_t LINK_BB(int q) { return 1u << q; }  // neighbour x-c_q is OBSTACLE

@@ -12,11 +12,15 @@
 // shift for c_x != 0), and all 19 populations of a cell sit at compile-time
 // offsets q*32 from one address.  The lagged Smagorinsky state (5 values per
 // cell) uses the same blocking with 5 instead of 19.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "common.cuh"
 
@@ -79,6 +83,8 @@ struct StepArgs {
     const uint32_t *bcount;         // their number (device)
     int bfrom_end;                  // the list is read from the end of blist (near blocks)
     uint32_t nblocks;               // rows * nb
+    float *stress_out;              // 7 planes of Ncells: stress of the gathered state (fused output), or NULL
+    uint32_t links_all;             // nonzero: the link mask of every cell (no per-cell masks are read)
 };
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
@@ -474,10 +480,105 @@ __device__ __forceinline__ void moving_wall_terms(const StepArgs &a, uint32_t ce
     }
 }
 
+// Stress diagnostics of the state the step gathers (compute_stress,
+// lbm_solver3d.py:347-404, evaluated on the post-stream populations h[] of
+// this cell and the lagged (drho, u, omega) of its last collision in lag[]),
+// written as an optional output of the fused step:
+// sigma = -(1 - omega/2) (sum c c (f - w) - (drho cs^2 delta + rho u u)),
+// 7 planes (xx, yy, zz, xy, xz, yz, shear magnitude), the same values as
+// k_stress computes from the materialised state.
+__device__ __forceinline__ void write_stress(const StepArgs &a, const float h[Q], const float lag[5], uint32_t cell) {
+    float sp[9];
+#pragma unroll
+    for (int p = 0; p < 9; ++p) sp[p] = h[2 * p + 1] + h[2 * p + 2];
+    const float W1 = a.W1, W2 = a.W2;
+    const float pxy = sp[3] + sp[4], pxz = sp[5] + sp[6], pyz = sp[7] + sp[8];
+    const float sxx = fmaf(W1, sp[0], W2 * (pxy + pxz));
+    const float syy = fmaf(W1, sp[1], W2 * (pxy + pyz));
+    const float szz = fmaf(W1, sp[2], W2 * (pxz + pyz));
+    const float sxy = W2 * (sp[3] - sp[4]), sxz = W2 * (sp[5] - sp[6]), syz = W2 * (sp[7] - sp[8]);
+    const float dr = lag[0], ux = lag[1], uy = lag[2], uz = lag[3], om = lag[4];
+    const float rho = 1.f + dr, ecs = dr * CS2;
+    const float k = -(1.f - 0.5f * om);
+    const float txy = k * (sxy - rho * ux * uy), txz = k * (sxz - rho * ux * uz), tyz = k * (syz - rho * uy * uz);
+    float *o = a.stress_out + cell;
+    const size_t nc = a.nc;
+    o[0] = k * (sxx - (ecs + rho * ux * ux));
+    o[nc] = k * (syy - (ecs + rho * uy * uy));
+    o[2 * nc] = k * (szz - (ecs + rho * uz * uz));
+    o[3 * nc] = txy;
+    o[4 * nc] = txz;
+    o[5 * nc] = tyz;
+    o[6 * nc] = sqrtf(0.5f * (txy * txy + txz * txz + tyz * tyz));
+}
+
+// The part of the fused step after the loads: bounce-back refetch, moving
+// walls, optional stress, collision, stores and the force reduction of one
+// cell, given its streamed populations raw[] (storage type), the lagged state
+// aux[], its owner key and link mask.  Shared by the kernel that gathers with
+// its own loads and the one that stages rows in shared memory.
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS>
+__device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z, bool inb, uint32_t cell,
+                                          uint32_t own, uint32_t aown, T raw[Q], float aux[5], uint32_t key,
+                                          uint32_t lk) {
+    const bool act = inb && !(lk & (LINK_SKIP | LINK_DEFER));
+    if (!act) key = 0u;
+    if (GATHER && (lk & 0x7FFFEu)) {
+        const T *p = static_cast<const T *>(a.src) + own;
+#pragma unroll
+        for (int q = 1; q < Q; ++q)
+            if (lk & LINK_BB(q)) raw[q] = Store<T>::ld(p + qinv(q) * 32);
+    }
+    float h[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(raw[q]);
+    if (GATHER && (lk & LINK_MOVING)) moving_wall_terms(a, cell, x, y, z, h);
+    if constexpr (STRESS) {
+        if (act) write_stress(a, h, aux, cell);
+    }
+    const bool psc = a.key != nullptr && __any_sync(0xffffffffu, key != 0u);
+    CellForce cf[1];
+    const bool acts[1] = {act};
+    const int xs[1] = {x};
+    const uint32_t keys[1] = {key};
+    const float epss[1] = {(a.eps != nullptr && key) ? a.eps[cell] : 0.f};
+    // post-collision values overwrite h[] and aux[] and are stored together
+    collide<float, SMAG, false, WRAP>(
+        a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { h[q] = v; },
+        [&](int k, float v) { aux[k] = v; },
+        [&](float r, float u3x, float u3y, float u3z) {
+            // post-stream moments of an exit's / inlet's interior neighbour, read by the boundary pass
+            if (GATHER && act && (lk & LINK_KEEP) && a.vel != nullptr) {
+                a.rho[cell] = r;
+                a.vel[cell] = u3x * (1.f / 3.f);
+                a.vel[a.nc + cell] = u3y * (1.f / 3.f);
+                a.vel[2 * a.nc + cell] = u3z * (1.f / 3.f);
+            }
+        });
+    if (act && (lk & LINK_MOVING)) a.rho[cell] = cf[0].rho;   // lagged density of the next stream
+    if (act) {
+        T *d = static_cast<T *>(a.dst) + own;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d[q * 32] = Store<T>::narrow(h[q]);
+        if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
+            T *ap = static_cast<T *>(a.aux) + aown;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+        }
+        if (a.hydro_out) {
+            a.hydro_out[cell] = cf[0].hx;
+            a.hydro_out[a.nc + cell] = cf[0].hy;
+            a.hydro_out[2 * a.nc + cell] = cf[0].hz;
+        }
+    }
+    if (psc) reduce_forces(a, cf[0]);
+}
+
 // LISTED (pipelined stepping): one-dimensional blocks whose warps take the
 // x-blocks of a compact list (blist / bcount), so every warp of a CTA has
 // work; otherwise the grid covers the lattice.  A warp is one x-block.
-template <typename T, bool GATHER, int SMAG, bool WRAP, bool LISTED = false>
+// STRESS: also write the stress diagnostics of the gathered state (a.stress_out).
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool LISTED = false, bool STRESS = false>
 __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     int x, y, z;
@@ -531,63 +632,220 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     }
     float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
     const uint32_t aown = row * a.ars + xslot((uint32_t)xc_, AB);
-    if (SMAG == LBDEM_SMAG_REFERENCE) {
+    if (SMAG == LBDEM_SMAG_REFERENCE || STRESS) {
         const T *ap = static_cast<const T *>(a.aux) + aown;
 #pragma unroll
         for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ap[k * 32]);
     }
     uint32_t key = (a.key != nullptr) ? a.key[cell] : 0u;
-    // the link mask is read for every cell: a flag that skipped this load for
-    // plain blocks cost more (a dependent load before it) than the 4 B it saved
-    const uint32_t lk = a.links[cell];
-    const bool act = inb && !(lk & (LINK_SKIP | LINK_DEFER));
-    if (!act) key = 0u;
-    if (GATHER && (lk & 0x7FFFEu)) {
-        const T *p = src + own;
+    // the link mask is read for every cell (a flag that skipped this load for
+    // plain blocks cost more -- a dependent load before it -- than the 4 B it
+    // saved), unless one value holds for the whole lattice (kernel argument)
+    const uint32_t lk = a.links_all ? a.links_all : a.links[cell];
+    step_cell<T, GATHER, SMAG, WRAP, STRESS>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
+}
+
+
+// ---------------------------------------------------------------------------
+// fused step with the gathered rows staged in shared memory by the tensor
+// memory accelerator (TMA)
+// ---------------------------------------------------------------------------
+// A lattice row (z, y) needs, for direction q, population q of the upwind row
+// (y - c_qy, z - c_qz) (periodic wrap), shifted by -c_qx along x.  In the
+// x-blocked layout population q of a whole row is one box of the 5-D view
+// [z][y][x-block][q][lane] (32 lanes x 1 direction x NB blocks), which lands
+// in shared memory as the row's x order; the x shift and its periodic wrap are
+// then an index into that copy.  Each persistent CTA walks rows r =
+// blockIdx.x + k gridDim.x, one cell per consumer thread (rows of at most 256
+// cells), with ROW_STAGES rows in flight: a producer warp issues the 19
+// population boxes, the lagged-state box (reference Smagorinsky) and the
+// owner-key and link-mask rows of a row into a free stage while the consumer
+// warps collide the rows already landed; each consumer warp releases a stage
+// as soon as it has read its cells, so warps do not wait for one another.  The
+// copies hold no registers, so many more bytes are in flight per SM than the
+// loads of resident threads could hold.  Each cell is then the same
+// arithmetic as k_psc_step (step_cell), so both kernels give identical
+// results.  Waits are bounded: a wait that gives up sets
+// LBDEM_ST_WAIT_TIMEOUT, the producer waits (bounded) for the CTA's copies in
+// flight, and the CTA returns.
+constexpr int ROW_STAGES = 4;
+constexpr int ROW_THREADS = 256;
+#ifndef ROW_MIN_BLOCKS
+#define ROW_MIN_BLOCKS 3
+#endif
+
+struct RowMaps {
+    CUtensorMap f;        // 5-D populations of the source buffer: lane, q, x-block, y, z; box 32 x 1 x NB x 1 x 1
+    CUtensorMap aux;      // 5-D lagged state: lane, k, x-block, y, z; box 32 x 5 x NB x 1 x 1
+    CUtensorMap key;      // 2-D owner keys (Nx, Ny*Nz), box BW x 1
+    CUtensorMap link;     // 2-D link masks, same
+    uint32_t slot;        // bytes per direction's row copy (128-aligned)
+    uint32_t off_aux, off_key, off_link, stage_bytes, tx_bytes;
+    int32_t kl_tma;       // key / link rows come by TMA (Nx % 4 == 0), else by plain loads
+    int32_t kl_boxes;     // boxes per key / link row
+    int32_t kl_box;       // their width
+    int32_t use_aux;      // the lagged-state box is loaded
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded: false after about 2^22 polls (seconds; a copy takes microseconds)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < (1u << 22); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1,
+                                            int c2, int c3, int c4) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, "
+        "%6, %7}], [%2];" ::"r"(dst),
+        "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+        "[%2];" ::"r"(dst),
+        "l"(map), "r"(bar), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+// issue the copies of row r into the stage at byte offset `base` (one thread)
+template <typename T>
+__device__ __forceinline__ void row_issue(const StepArgs &a, const RowMaps &m, uint32_t base, uint32_t bar, int r) {
+    const int ny = a.ny, nz = a.nz;
+    const int z = r / ny, y = r - z * ny;
+    mbar_expect_tx(bar, m.tx_bytes);
 #pragma unroll
-        for (int q = 1; q < Q; ++q)
-            if (lk & LINK_BB(q)) raw[q] = Store<T>::ld(p + qinv(q) * 32);
+    for (int q = 0; q < Q; ++q) {
+        int yq = y - cy(q), zq = z - cz(q);
+        yq = yq < 0 ? ny - 1 : (yq >= ny ? 0 : yq);
+        zq = zq < 0 ? nz - 1 : (zq >= nz ? 0 : zq);
+        tma_load_5d(base + q * m.slot, &m.f, bar, 0, q, 0, yq, zq);
     }
-    float h[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) h[q] = Store<T>::widen(raw[q]);
-    if (GATHER && (lk & LINK_MOVING)) moving_wall_terms(a, cell, x, y, z, h);
-    const bool psc = a.key != nullptr && __any_sync(0xffffffffu, key != 0u);
-    CellForce cf[1];
-    const bool acts[1] = {act};
-    const int xs[1] = {x};
-    const uint32_t keys[1] = {key};
-    const float epss[1] = {(a.eps != nullptr && key) ? a.eps[cell] : 0.f};
-    // post-collision values overwrite h[] and aux[] and are stored together
-    collide<float, SMAG, false, WRAP>(
-        a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { h[q] = v; },
-        [&](int k, float v) { aux[k] = v; },
-        [&](float r, float u3x, float u3y, float u3z) {
-            // post-stream moments of an exit's / inlet's interior neighbour, read by the boundary pass
-            if (GATHER && act && (lk & LINK_KEEP) && a.vel != nullptr) {
-                a.rho[cell] = r;
-                a.vel[cell] = u3x * (1.f / 3.f);
-                a.vel[a.nc + cell] = u3y * (1.f / 3.f);
-                a.vel[2 * a.nc + cell] = u3z * (1.f / 3.f);
+    if (m.use_aux) tma_load_5d(base + m.off_aux, &m.aux, bar, 0, 0, 0, y, z);
+    if (m.kl_tma) {
+        for (int b = 0; b < m.kl_boxes; ++b) {
+            if (a.key != nullptr) tma_load_2d(base + m.off_key + 4 * b * m.kl_box, &m.key, bar, b * m.kl_box, r);
+            if (!a.links_all) tma_load_2d(base + m.off_link + 4 * b * m.kl_box, &m.link, bar, b * m.kl_box, r);
+        }
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Warp roles: the last warp of the CTA is the producer (its lane 0 issues the
+// copies of each row into a free stage); the other 32 NB threads are the
+// consumers, one cell each.  full[s] completes when the copies of stage s have
+// landed; empty[s] when every consumer warp has released it, so consumer warps
+// run up to ROW_STAGES rows apart and no CTA-wide barrier sits in the loop.
+template <typename T, int SMAG, bool WRAP>
+__global__ void __launch_bounds__(ROW_THREADS + 32, ROW_MIN_BLOCKS) k_psc_step_rows(const StepArgs a,
+                                                                                  const __grid_constant__ RowMaps m) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[ROW_STAGES], empty[ROW_STAGES];
+    __shared__ volatile int abort_flag;
+    const int nx = a.nx, ny = a.ny;
+    const int nrows = ny * a.nz;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t ncons = blockDim.x - 32u;          // consumer threads: 32 NB
+    const bool producer = threadIdx.x >= ncons;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ROW_STAGES; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), ncons / 32u);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        abort_flag = 0;
+    }
+    __syncthreads();
+    if (producer) {
+        if (threadIdx.x == ncons) {
+            int issued = 0;
+            for (int k = 0;; ++k) {
+                const int r = blockIdx.x + k * gridDim.x;
+                if (r >= nrows || abort_flag) break;
+                const int st = k % ROW_STAGES;
+                if (k >= ROW_STAGES && !mbar_wait(smem_u32(&empty[st]), (uint32_t)(k / ROW_STAGES - 1) & 1u)) {
+                    abort_flag = 1;
+                    break;
+                }
+                row_issue<T>(a, m, sbase + st * m.stage_bytes, smem_u32(&full[st]), r);
+                issued = k + 1;
             }
-        });
-    if (act && (lk & LINK_MOVING)) a.rho[cell] = cf[0].rho;   // lagged density of the next stream
-    if (act) {
-        T *d = static_cast<T *>(a.dst) + own;
-#pragma unroll
-        for (int q = 0; q < Q; ++q) d[q * 32] = Store<T>::narrow(h[q]);
-        if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
-            T *ap = static_cast<T *>(a.aux) + aown;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+            if (abort_flag) {
+                atomicOr(a.status, (int)LBDEM_ST_WAIT_TIMEOUT);
+                // wait (bounded) for the copies this CTA still has in flight: the last row issued into each stage
+                for (int k = issued - ROW_STAGES; k < issued; ++k)
+                    if (k >= 0) mbar_wait(smem_u32(&full[k % ROW_STAGES]), (uint32_t)(k / ROW_STAGES) & 1u);
+            }
         }
-        if (a.hydro_out) {
-            a.hydro_out[cell] = cf[0].hx;
-            a.hydro_out[a.nc + cell] = cf[0].hy;
-            a.hydro_out[2 * a.nc + cell] = cf[0].hz;
-        }
+        return;
     }
-    if (psc) reduce_forces(a, cf[0]);
+    const uint32_t spe = m.slot / sizeof(T);   // elements per direction's row copy
+    for (int k = 0;; ++k) {
+        const int r = blockIdx.x + k * gridDim.x;
+        if (r >= nrows) break;
+        const int st = k % ROW_STAGES;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&full[st]), (uint32_t)(k / ROW_STAGES) & 1u));
+        if (!ok || abort_flag) {
+            if ((threadIdx.x & 31u) == 0) abort_flag = 1;
+            break;
+        }
+        const unsigned char *stage = smem + st * m.stage_bytes;
+        const T *sf = reinterpret_cast<const T *>(stage);
+        const T *sa = reinterpret_cast<const T *>(stage + m.off_aux);
+        const uint32_t *sk = reinterpret_cast<const uint32_t *>(stage + m.off_key);
+        const uint32_t *sl = reinterpret_cast<const uint32_t *>(stage + m.off_link);
+        const int z = r / ny, y = r - z * ny;
+        const int x = (int)threadIdx.x;
+        const bool inb = x < nx;
+        const int xc = inb ? x : 0;
+        const int xm = xc == 0 ? nx - 1 : xc - 1, xp = xc == nx - 1 ? 0 : xc + 1;
+        T raw[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) raw[q] = sf[q * spe + (cx(q) == 1 ? xm : (cx(q) == -1 ? xp : xc))];
+        float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
+        if (SMAG == LBDEM_SMAG_REFERENCE) {
+            const T *ap = sa + xslot((uint32_t)xc, AB);
+#pragma unroll
+            for (int kk = 0; kk < 5; ++kk) aux[kk] = aux_dec<T>(ap[kk * 32]);
+        }
+        const uint32_t cell = (uint32_t)r * (uint32_t)nx + (uint32_t)xc;
+        uint32_t key, lk;
+        if (m.kl_tma) {
+            key = a.key != nullptr ? sk[xc] : 0u;
+            lk = a.links_all ? a.links_all : sl[xc];
+        } else {
+            key = a.key != nullptr ? a.key[cell] : 0u;
+            lk = a.links_all ? a.links_all : a.links[cell];
+        }
+        // every read of this stage is done: release it to the producer
+        __syncwarp();
+        if ((threadIdx.x & 31u) == 0) mbar_arrive(smem_u32(&empty[st]));
+        const uint32_t own = (uint32_t)r * a.rs + xslot((uint32_t)xc, QB);
+        const uint32_t aown = (uint32_t)r * a.ars + xslot((uint32_t)xc, AB);
+        step_cell<T, true, SMAG, WRAP, false>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
+    }
 }
 
 // stream only: move post-collision populations to their cells and compute
@@ -1304,6 +1562,7 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
     a.aux = L->aux;
     a.keep_lag = L->aux != nullptr;
     a.links = L->links;
+    a.links_all = L->links_all;
     a.moving = L->moving;
     a.rho = L->rho;
     a.vel = L->vel;
@@ -1365,6 +1624,137 @@ static void step_geometry(const lbdem_lattice *L, dim3 &grid, dim3 &block, int n
     grid = dim3((L->nx + bx - 1) / bx, (L->ny + by - 1) / by, L->nz);
 }
 
+// ---------------------------------------------------------------------------
+// host side of the row-staged step
+// ---------------------------------------------------------------------------
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link-time
+// dependency on libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// Which form of the gathered full-lattice step runs.  By default the
+// row-staged one for 16-bit storage (measured 2 % faster than k_psc_step at
+// 256^3) and k_psc_step for FP32 (the row-staged FP32 step fits only two CTAs
+// per SM in shared memory and measured 30 % slower); LBDEM_STEP_KERNEL=rows or
+// =simt in the environment at the call selects one form for every storage.
+template <typename T>
+static bool rows_kernel_enabled() {
+    const char *e = getenv("LBDEM_STEP_KERNEL");
+    if (e && strcmp(e, "simt") == 0) return false;
+    if (e && strcmp(e, "rows") == 0) return true;
+    return sizeof(T) == 2;
+}
+
+template <typename T> constexpr CUtensorMapDataType tmap_type();
+template <> constexpr CUtensorMapDataType tmap_type<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
+template <> constexpr CUtensorMapDataType tmap_type<__half>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT16; }
+template <> constexpr CUtensorMapDataType tmap_type<__nv_bfloat16>() { return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; }
+
+static uint32_t round_up(uint32_t v, uint32_t m) { return (v + m - 1) / m * m; }
+
+constexpr int ROWS_NOT_APPLICABLE = -1;
+
+// Launch the row-staged step; ROWS_NOT_APPLICABLE for rows wider than 256
+// cells, with too little shared memory for two CTAs per SM, when the driver
+// has no tensor-map encoder, or when a copy's description is refused -- the
+// caller then launches k_psc_step.
+template <typename T, int SMAG, bool WRAP>
+static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStream_t st) {
+    auto encode = tmap_encoder();
+    // one thread per cell of a row: rows of up to ROW_THREADS cells (a loop over
+    // wider rows costs registers the step does not have)
+    if (!encode || 32u * a.nb > (uint32_t)ROW_THREADS || a.src == nullptr) return ROWS_NOT_APPLICABLE;
+    const uint32_t es = sizeof(T), nb = a.nb;
+    RowMaps m;
+    memset(&m, 0, sizeof(m));
+    m.use_aux = SMAG == LBDEM_SMAG_REFERENCE;
+    m.kl_tma = (a.nx % 4) == 0;
+    m.kl_box = (int)std::min<uint32_t>(256u, round_up((uint32_t)a.nx, 4u));
+    m.kl_boxes = (a.nx + m.kl_box - 1) / m.kl_box;
+    m.slot = round_up(32u * nb * es, 128u);
+    m.off_aux = Q * m.slot;
+    const uint32_t aux_bytes = m.use_aux ? round_up(5u * 32u * nb * es, 128u) : 0u;
+    const uint32_t klrow = m.kl_tma ? round_up(std::max<uint32_t>(m.kl_boxes * m.kl_box, 32u * nb) * 4u, 128u) : 0u;
+    m.off_key = m.off_aux + aux_bytes;
+    m.off_link = m.off_key + klrow;
+    m.stage_bytes = m.off_link + klrow;
+    m.tx_bytes = Q * 32u * nb * es + (m.use_aux ? 5u * 32u * nb * es : 0u) +
+                 (m.kl_tma ? (uint32_t)(m.kl_boxes * m.kl_box) * 4u *
+                                 ((a.key != nullptr ? 1u : 0u) + (a.links_all ? 0u : 1u))
+                           : 0u);
+    const uint32_t smem = ROW_STAGES * m.stage_bytes;
+    if (smem > 200u * 1024u) return ROWS_NOT_APPLICABLE;
+
+    const cuuint64_t ny = (cuuint64_t)a.ny, nz = (cuuint64_t)a.nz;
+    {
+        const cuuint64_t dims[5] = {32, (cuuint64_t)Q, nb, ny, nz};
+        const cuuint64_t strides[4] = {32ull * es, 32ull * Q * es, 32ull * Q * es * nb, 32ull * Q * es * nb * ny};
+        const cuuint32_t box[5] = {32, 1, nb, 1, 1};
+        const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+        if (encode(&m.f, tmap_type<T>(), 5, const_cast<void *>(a.src), dims, strides, box, one,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return ROWS_NOT_APPLICABLE;
+    }
+    if (m.use_aux) {
+        const cuuint64_t dims[5] = {32, 5, nb, ny, nz};
+        const cuuint64_t strides[4] = {32ull * es, 32ull * 5 * es, 32ull * 5 * es * nb, 32ull * 5 * es * nb * ny};
+        const cuuint32_t box[5] = {32, 5, nb, 1, 1};
+        const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+        if (!a.aux || encode(&m.aux, tmap_type<T>(), 5, a.aux, dims, strides, box, one,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return ROWS_NOT_APPLICABLE;
+    }
+    if (m.kl_tma) {
+        const cuuint64_t dims[2] = {(cuuint64_t)a.nx, ny * nz};
+        const cuuint64_t strides[1] = {(cuuint64_t)a.nx * 4ull};
+        const cuuint32_t box[2] = {(cuuint32_t)m.kl_box, 1};
+        const cuuint32_t one[2] = {1, 1};
+        if (encode(&m.link, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint32_t *>(a.links), dims, strides, box,
+                   one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return ROWS_NOT_APPLICABLE;
+        if (a.key && encode(&m.key, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint32_t *>(a.key), dims, strides,
+                            box, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return ROWS_NOT_APPLICABLE;
+    }
+    auto kern = k_psc_step_rows<T, SMAG, WRAP>;
+    static uint32_t smem_set = 0;    // per instantiation
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            cudaGetLastError();
+            return ROWS_NOT_APPLICABLE;
+        }
+        smem_set = smem;
+    }
+    const int threads = (int)(32u * nb) + 32;   // consumers + the producer warp
+    int per_sm = 0, dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 2) {
+        cudaGetLastError();
+        return ROWS_NOT_APPLICABLE;
+    }
+    const int nrows = a.ny * a.nz;
+    const int grid = std::min(nrows, nsm * per_sm);
+    kern<<<grid, threads, smem, st>>>(a, m);
+    return check_launch("psc_step_rows");
+}
+
 template <typename T>
 static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int src, int dst,
                        int gather, cudaStream_t st) {
@@ -1392,13 +1782,39 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
         a.moment_fluid = G->moment_fluid;
         a.hydro_out = P->hydro_out;
     }
+    if (L->stress) {
+        if (!L->aux) {
+            set_error("psc_step: the fused stress output needs the lagged state (aux)");
+            return LBDEM_ERR_ARG;
+        }
+        if (L->bnd_na + L->bnd_nb > 0) {
+            set_error("psc_step: the fused stress output does not cover boundary-pass cells; use lbdem_stress");
+            return LBDEM_ERR_UNSUPPORTED;
+        }
+        a.stress_out = L->stress;
+    }
     dim3 grid, block;
     step_geometry(L, grid, block, ONE_THREADS);
-#define LBDEM_STEP_CASE(G_, S_)                                        \
-    do {                                                               \
-        if (a.wrap_any) k_psc_step<T, G_, S_, true><<<grid, block, 0, st>>>(a);   \
-        else k_psc_step<T, G_, S_, false><<<grid, block, 0, st>>>(a);            \
-        launch_boundary<T, S_, G_ ? BND_GATHER : BND_LOCAL>(L, a, st); \
+#define LBDEM_STEP_CASE(G_, S_)                                                          \
+    do {                                                                                 \
+        if (G_ && !a.stress_out && rows_kernel_enabled<T>()) {                           \
+            const int rc_ = a.wrap_any ? launch_step_rows<T, S_, true>(L, a, st)          \
+                                       : launch_step_rows<T, S_, false>(L, a, st);        \
+            if (rc_ != ROWS_NOT_APPLICABLE) {                                            \
+                if (rc_ != LBDEM_OK) return rc_;                                         \
+                launch_boundary<T, S_, BND_GATHER>(L, a, st);                            \
+                return check_launch("psc_step");                                         \
+            }                                                                            \
+        }                                                                                \
+        if (a.stress_out) {                                                              \
+            if (a.wrap_any) k_psc_step<T, G_, S_, true, false, true><<<grid, block, 0, st>>>(a);  \
+            else k_psc_step<T, G_, S_, false, false, true><<<grid, block, 0, st>>>(a);           \
+        } else if (a.wrap_any) {                                                         \
+            k_psc_step<T, G_, S_, true><<<grid, block, 0, st>>>(a);                      \
+        } else {                                                                         \
+            k_psc_step<T, G_, S_, false><<<grid, block, 0, st>>>(a);                     \
+        }                                                                                \
+        launch_boundary<T, S_, G_ ? BND_GATHER : BND_LOCAL>(L, a, st);                   \
     } while (0)
     if (gather) {
         if (L->smag_mode == LBDEM_SMAG_OFF) LBDEM_STEP_CASE(true, LBDEM_SMAG_OFF);

@@ -236,6 +236,7 @@ class LatticeEngine:
         L.rho, L.vel = N.ptr(self._rho), N.ptr(self._vel)
         L.aux = N.ptr(self._aux)
         L.links = N.ptr(self._links)
+        L.links_all = N.LINK_FLUID       # cell types start as FLUID everywhere
         L.status = N.ptr(self._status)
         L.ct = N.ptr(self._ct_dev)
 
@@ -253,6 +254,8 @@ class LatticeEngine:
             raise ValueError("FREE_SLIP cells need a face bit (LEFT/RIGHT/BOTTOM/TOP/BACK/FRONT) for the mirror "
                              "direction (lbm_solver3d.py:230-236)")
         self._ct_dev.copy_(torch.from_numpy(from_ref(host.astype(np.int32)).reshape(-1)))
+        # an all-FLUID lattice has one link mask everywhere: the step reads none
+        self._lat.links_all = N.LINK_FLUID if bool((host == CellType.FLUID).all()) else 0
         self.has_open_boundaries = bool(np.bitwise_and(host, _OPEN).any())
         self._has_slip = bool(slip.any())
         # moving walls and Ladd inlets: per-cell velocity-link bits, allocated on first use

@@ -134,6 +134,77 @@ def test_moving_walls_ladd(api, read_every_step):
     lat.check_status()
 
 
+@pytest.mark.parametrize("storage,tol", [("f32", 2e-7), ("f16", 5e-5), ("bf16", 5e-4)])
+def test_stress_fused_into_the_step(api, monkeypatch, storage, tol):
+    """The shear driver's loop (shear_fullyresolved.py:226-233): compute_stress()
+    after every stream.  The next collide() gathers exactly the state the call
+    refers to and writes the stress as an optional output of the fused step;
+    no separate stress pass runs.  The fields read after that collide equal the
+    reference's stress of the previous step (stresses up to 1.2e-3 here):
+    FP32 storage within 2e-7; the 16-bit forms within the rounding of their
+    stored populations, 5e-5 (FP16) and 5e-4 (BF16)."""
+    from lbdem_taichi_b200 import _native as N
+    _, PSC, _, _ = api
+    g = load("couette_ladd")
+    nx, ny, nz = g["ct"].shape
+    dem = _golden_grains_dem(g, 0.25, 2.0)
+    lat = PSC(nx, ny, nz, float(g["omega0"]), 1.0, 1.0, 1.0, dem, stress=True, storage=storage)
+    _setup(lat, g)
+    lat.initialize()
+    fl = g["ct"] == 1
+    calls = []
+    orig = N.call
+    monkeypatch.setattr(N, "call", lambda name, *a: (calls.append(name), orig(name, *a))[1])
+    names = ("stress_xx", "stress_yy", "stress_zz", "stress_xy", "stress_xz", "stress_yz", "shear_stress_mag")
+    checked = 0
+    for s in range(int(g["nsteps"])):
+        lat.collide()
+        if s > 0:
+            for k in names:
+                assert np.abs(getattr(lat, k).to_numpy() - g[f"{k}_{s - 1}"])[fl].max() < tol, (k, s)
+            for key, (axis, pos) in (("plane_top", (2, nz - 2)), ("plane_y", (1, 3)), ("plane_x", (0, 4))):
+                got = lat.compute_plane_average_stress(axis, pos)
+                assert np.abs(got - g[f"{key}_{s - 1}"]).max() < tol, key
+            checked += 1
+        lat.stream()
+        lat.compute_stress()
+    assert checked >= 2
+    assert "lbdem_stress" not in calls
+    # a read with a compute_stress() pending evaluates it in a pass of its own: the last step's stress
+    for k in names:
+        assert np.abs(getattr(lat, k).to_numpy() - g[f"{k}_{s}"])[fl].max() < tol, k
+    assert calls.count("lbdem_stress") == 1
+    lat.check_status()
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_stress_fused_equals_separate_pass(api, storage):
+    """The stress the fused step writes equals the separate pass's
+    (lbdem_stress) on the same stored state, for every storage form: the same
+    FP32 arithmetic in another order (within 1e-6 of the largest value)."""
+    _, PSC, _, _ = api
+    g = load("couette_ladd")
+    nx, ny, nz = g["ct"].shape
+    dem = _golden_grains_dem(g, 0.25, 2.0)
+    lat = PSC(nx, ny, nz, float(g["omega0"]), 1.0, 1.0, 1.0, dem, stress=True, storage=storage)
+    _setup(lat, g)
+    lat.initialize()
+    fl = g["ct"] == 1
+    names = ("stress_xx", "stress_yy", "stress_zz", "stress_xy", "stress_xz", "stress_yz", "shear_stress_mag")
+    for s in range(int(g["nsteps"])):
+        lat.collide()
+        lat.stream()
+        lat.compute_stress()
+        sep = [getattr(lat, k).to_numpy() for k in names]       # read with the call pending: separate pass
+        lat.compute_stress()                                      # pending again: fused into the next collide
+        lat.collide()
+        fused = [getattr(lat, k).to_numpy() for k in names]
+        for k, a, b in zip(names, sep, fused):
+            assert np.abs(a - b)[fl].max() <= 1e-6 * max(np.abs(a[fl]).max(), 1e-30), (k, s)
+        lat.stream()
+    lat.check_status()
+
+
 def test_hybrid_psc_smagorinsky(api):
     _, PSC, _, _ = api
     g = load("hybrid")
