@@ -679,13 +679,27 @@ struct RowMaps {
     CUtensorMap aux;      // 5-D lagged state: lane, k, x-block, y, z; box 32 x 5 x NB x 1 x 1
     CUtensorMap key;      // 2-D owner keys (Nx, Ny*Nz), box BW x 1
     CUtensorMap link;     // 2-D link masks, same
-    uint32_t slot;        // bytes per direction's row copy (128-aligned)
-    uint32_t off_aux, off_key, off_link, stage_bytes, tx_bytes;
+    uint32_t tx_bytes;    // bytes the copies of one row deliver
     int32_t kl_tma;       // key / link rows come by TMA (Nx % 4 == 0), else by plain loads
-    int32_t kl_boxes;     // boxes per key / link row
-    int32_t kl_box;       // their width
+    int32_t kl_box;       // width of the key / link boxes (Nx rounded up to 4)
     int32_t use_aux;      // the lagged-state box is loaded
 };
+
+// Stage layout in shared memory, fixed at compile time so that every
+// direction's copy sits at an immediate offset (rows of at most 256 cells =
+// 8 x-blocks): 19 direction slots, the lagged state, the key and link rows.
+template <typename T> struct RowLayout {
+    static constexpr uint32_t slot = 32u * 8u * sizeof(T);
+    static constexpr uint32_t off_aux = Q * slot;
+    static constexpr uint32_t off_key = off_aux + 5u * 32u * 8u * sizeof(T);
+    static constexpr uint32_t off_link = off_key + 256u * 4u;
+    static constexpr uint32_t stage = off_link + 256u * 4u;
+    static_assert(slot % 128u == 0 && off_key % 128u == 0 && stage % 128u == 0, "128-byte aligned copies");
+};
+
+#ifndef ROW_L2_PROMOTION
+#define ROW_L2_PROMOTION CU_TENSOR_MAP_L2_PROMOTION_NONE
+#endif
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -730,6 +744,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
 // issue the copies of row r into the stage at byte offset `base` (one thread)
 template <typename T>
 __device__ __forceinline__ void row_issue(const StepArgs &a, const RowMaps &m, uint32_t base, uint32_t bar, int r) {
+    using RL = RowLayout<T>;
     const int ny = a.ny, nz = a.nz;
     const int z = r / ny, y = r - z * ny;
     mbar_expect_tx(bar, m.tx_bytes);
@@ -738,14 +753,12 @@ __device__ __forceinline__ void row_issue(const StepArgs &a, const RowMaps &m, u
         int yq = y - cy(q), zq = z - cz(q);
         yq = yq < 0 ? ny - 1 : (yq >= ny ? 0 : yq);
         zq = zq < 0 ? nz - 1 : (zq >= nz ? 0 : zq);
-        tma_load_5d(base + q * m.slot, &m.f, bar, 0, q, 0, yq, zq);
+        tma_load_5d(base + q * RL::slot, &m.f, bar, 0, q, 0, yq, zq);
     }
-    if (m.use_aux) tma_load_5d(base + m.off_aux, &m.aux, bar, 0, 0, 0, y, z);
+    if (m.use_aux) tma_load_5d(base + RL::off_aux, &m.aux, bar, 0, 0, 0, y, z);
     if (m.kl_tma) {
-        for (int b = 0; b < m.kl_boxes; ++b) {
-            if (a.key != nullptr) tma_load_2d(base + m.off_key + 4 * b * m.kl_box, &m.key, bar, b * m.kl_box, r);
-            if (!a.links_all) tma_load_2d(base + m.off_link + 4 * b * m.kl_box, &m.link, bar, b * m.kl_box, r);
-        }
+        if (a.key != nullptr) tma_load_2d(base + RL::off_key, &m.key, bar, 0, r);
+        if (!a.links_all) tma_load_2d(base + RL::off_link, &m.link, bar, 0, r);
     }
 }
 
@@ -789,7 +802,7 @@ __global__ void __launch_bounds__(ROW_THREADS + 32, ROW_MIN_BLOCKS) k_psc_step_r
                     abort_flag = 1;
                     break;
                 }
-                row_issue<T>(a, m, sbase + st * m.stage_bytes, smem_u32(&full[st]), r);
+                row_issue<T>(a, m, sbase + st * RowLayout<T>::stage, smem_u32(&full[st]), r);
                 issued = k + 1;
             }
             if (abort_flag) {
@@ -801,7 +814,8 @@ __global__ void __launch_bounds__(ROW_THREADS + 32, ROW_MIN_BLOCKS) k_psc_step_r
         }
         return;
     }
-    const uint32_t spe = m.slot / sizeof(T);   // elements per direction's row copy
+    using RL = RowLayout<T>;
+    constexpr uint32_t spe = RL::slot / sizeof(T);   // elements per direction's row copy
     for (int k = 0;; ++k) {
         const int r = blockIdx.x + k * gridDim.x;
         if (r >= nrows) break;
@@ -811,11 +825,11 @@ __global__ void __launch_bounds__(ROW_THREADS + 32, ROW_MIN_BLOCKS) k_psc_step_r
             if ((threadIdx.x & 31u) == 0) abort_flag = 1;
             break;
         }
-        const unsigned char *stage = smem + st * m.stage_bytes;
+        const unsigned char *stage = smem + st * RL::stage;
         const T *sf = reinterpret_cast<const T *>(stage);
-        const T *sa = reinterpret_cast<const T *>(stage + m.off_aux);
-        const uint32_t *sk = reinterpret_cast<const uint32_t *>(stage + m.off_key);
-        const uint32_t *sl = reinterpret_cast<const uint32_t *>(stage + m.off_link);
+        const T *sa = reinterpret_cast<const T *>(stage + RL::off_aux);
+        const uint32_t *sk = reinterpret_cast<const uint32_t *>(stage + RL::off_key);
+        const uint32_t *sl = reinterpret_cast<const uint32_t *>(stage + RL::off_link);
         const int z = r / ny, y = r - z * ny;
         const int x = (int)threadIdx.x;
         const bool inb = x < nx;
@@ -1681,22 +1695,10 @@ static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStrea
     memset(&m, 0, sizeof(m));
     m.use_aux = SMAG == LBDEM_SMAG_REFERENCE;
     m.kl_tma = (a.nx % 4) == 0;
-    m.kl_box = (int)std::min<uint32_t>(256u, round_up((uint32_t)a.nx, 4u));
-    m.kl_boxes = (a.nx + m.kl_box - 1) / m.kl_box;
-    m.slot = round_up(32u * nb * es, 128u);
-    m.off_aux = Q * m.slot;
-    const uint32_t aux_bytes = m.use_aux ? round_up(5u * 32u * nb * es, 128u) : 0u;
-    const uint32_t klrow = m.kl_tma ? round_up(std::max<uint32_t>(m.kl_boxes * m.kl_box, 32u * nb) * 4u, 128u) : 0u;
-    m.off_key = m.off_aux + aux_bytes;
-    m.off_link = m.off_key + klrow;
-    m.stage_bytes = m.off_link + klrow;
+    m.kl_box = (int)round_up((uint32_t)a.nx, 4u);
     m.tx_bytes = Q * 32u * nb * es + (m.use_aux ? 5u * 32u * nb * es : 0u) +
-                 (m.kl_tma ? (uint32_t)(m.kl_boxes * m.kl_box) * 4u *
-                                 ((a.key != nullptr ? 1u : 0u) + (a.links_all ? 0u : 1u))
-                           : 0u);
-    const uint32_t smem = ROW_STAGES * m.stage_bytes;
-    if (smem > 200u * 1024u) return ROWS_NOT_APPLICABLE;
-
+                 (m.kl_tma ? (uint32_t)m.kl_box * 4u * ((a.key != nullptr ? 1u : 0u) + (a.links_all ? 0u : 1u)) : 0u);
+    const uint32_t smem = ROW_STAGES * RowLayout<T>::stage;
     const cuuint64_t ny = (cuuint64_t)a.ny, nz = (cuuint64_t)a.nz;
     {
         const cuuint64_t dims[5] = {32, (cuuint64_t)Q, nb, ny, nz};
@@ -1704,7 +1706,7 @@ static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStrea
         const cuuint32_t box[5] = {32, 1, nb, 1, 1};
         const cuuint32_t one[5] = {1, 1, 1, 1, 1};
         if (encode(&m.f, tmap_type<T>(), 5, const_cast<void *>(a.src), dims, strides, box, one,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, ROW_L2_PROMOTION,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return ROWS_NOT_APPLICABLE;
     }
@@ -1714,8 +1716,8 @@ static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStrea
         const cuuint32_t box[5] = {32, 5, nb, 1, 1};
         const cuuint32_t one[5] = {1, 1, 1, 1, 1};
         if (!a.aux || encode(&m.aux, tmap_type<T>(), 5, a.aux, dims, strides, box, one,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, ROW_L2_PROMOTION,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return ROWS_NOT_APPLICABLE;
     }
     if (m.kl_tma) {
