@@ -210,7 +210,10 @@ __device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float
 // OVR: collide with the density and velocity in ovr[4] = (rho, ux, uy, uz)
 // instead of the moments of h -- the boundary pass, where a wet-node rule set
 // them (the reference always collides with its rho / vel fields).
-template <class V, int SMAG, bool OVR = false, bool WRAP = false, class Out, class AuxOut, class Macro>
+// PACK_PSC: the PSC pair updates also run two pairs per f32x2 instruction
+// (same rounding per lane; needs the registers of the row-staged kernel).
+template <class V, int SMAG, bool OVR = false, bool WRAP = false, bool PACK_PSC = false, class Out, class AuxOut,
+          class Macro>
 __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const bool act[], const int xs[], int y,
                                         int z, const V aux[5], bool psc, const uint32_t key[], const float eps[],
                                         CellForce cf[], Out &&out, AuxOut &&aux_out, Macro &&macro,
@@ -397,17 +400,43 @@ __device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const b
     const V Vz = vfma(kb, u3z, vfma(ks, s3z, rg3z));
     // q = 0: h0' = (c1 + B) h0 + Bf A0 + B (As0 - A0), A0 = S drho - k2 U
     out(0, vfma(c1 + Bw, h[0], vfma(eA, nU, vfma(eS, nUs, e0))));
+    if constexpr (PACK_PSC && L::N == 1) {
+        // pairs (0,1) (2,3) (4,5) (6,7) packed, pair 8 scalar
+        const float2 eA_ = f2(eA, eA), nU_ = f2(nU, nU), eS_ = f2(eS, eS), nUs_ = f2(nUs, nUs), e0_ = f2(e0, e0);
+        const float2 ca_ = f2(ca, ca), cb_ = f2(cb, cb);
 #pragma unroll
-    for (int p = 0; p < 9; ++p) {
-        const int q = 2 * p + 1;
-        const V v = cdot(q, u3x, u3y, u3z);
-        const V vs = cdot(q, s3x, s3y, s3z);
-        const V O = cdot(q, Vx, Vy, Vz);
+        for (int p = 0; p < 8; p += 2) {
+            const int q = 2 * p + 1, r = q + 2;
+            const float2 v = f2(cdot(q, u3x, u3y, u3z), cdot(r, u3x, u3y, u3z));
+            const float2 vs = f2(cdot(q, s3x, s3y, s3z), cdot(r, s3x, s3y, s3z));
+            const float2 O = f2(cdot(q, Vx, Vy, Vz), cdot(r, Vx, Vy, Vz));
+            const float2 E = fma2(eA_, fma2(v, v, nU_), fma2(eS_, fma2(vs, vs, nUs_), e0_));
+            const float2 SE = fma2(ca_, f2(sp[p], sp[p + 1]), E);
+            const float2 AO = fma2(cb_, f2(am[p], am[p + 1]), O);
+            const float2 hp = add2(SE, AO), hm = sub2(SE, AO);
+            out(q, hp.x); out(q + 1, hm.x); out(r, hp.y); out(r + 1, hm.y);
+        }
+        const V v = cdot(17, u3x, u3y, u3z);
+        const V vs = cdot(17, s3x, s3y, s3z);
+        const V O = cdot(17, Vx, Vy, Vz);
         const V E = vfma(eA, vfma(v, v, nU), vfma(eS, vfma(vs, vs, nUs), e0));
-        const V SE = vfma(ca, sp[p], E);
-        const V AO = vfma(cb, am[p], O);
-        out(q, SE + AO);
-        out(q + 1, SE - AO);
+        const V SE = vfma(ca, sp[8], E);
+        const V AO = vfma(cb, am[8], O);
+        out(17, SE + AO);
+        out(18, SE - AO);
+    } else {
+#pragma unroll
+        for (int p = 0; p < 9; ++p) {
+            const int q = 2 * p + 1;
+            const V v = cdot(q, u3x, u3y, u3z);
+            const V vs = cdot(q, s3x, s3y, s3z);
+            const V O = cdot(q, Vx, Vy, Vz);
+            const V E = vfma(eA, vfma(v, v, nU), vfma(eS, vfma(vs, vs, nUs), e0));
+            const V SE = vfma(ca, sp[p], E);
+            const V AO = vfma(cb, am[p], O);
+            out(q, SE + AO);
+            out(q + 1, SE - AO);
+        }
     }
 }
 
@@ -517,7 +546,7 @@ __device__ __forceinline__ void write_stress(const StepArgs &a, const float h[Q]
 // cell, given its streamed populations raw[] (storage type), the lagged state
 // aux[], its owner key and link mask.  Shared by the kernel that gathers with
 // its own loads and the one that stages rows in shared memory.
-template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS>
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS, bool PACK_PSC = false>
 __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z, bool inb, uint32_t cell,
                                           uint32_t own, uint32_t aown, T raw[Q], float aux[5], uint32_t key,
                                           uint32_t lk) {
@@ -543,7 +572,7 @@ __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z
     const uint32_t keys[1] = {key};
     const float epss[1] = {(a.eps != nullptr && key) ? a.eps[cell] : 0.f};
     // post-collision values overwrite h[] and aux[] and are stored together
-    collide<float, SMAG, false, WRAP>(
+    collide<float, SMAG, false, WRAP, PACK_PSC>(
         a, h, acts, xs, y, z, aux, psc, keys, epss, cf, [&](int q, float v) { h[q] = v; },
         [&](int k, float v) { aux[k] = v; },
         [&](float r, float u3x, float u3y, float u3z) {
@@ -858,7 +887,7 @@ __global__ void __launch_bounds__(ROW_THREADS + 32, ROW_MIN_BLOCKS) k_psc_step_r
         if ((threadIdx.x & 31u) == 0) mbar_arrive(smem_u32(&empty[st]));
         const uint32_t own = (uint32_t)r * a.rs + xslot((uint32_t)xc, QB);
         const uint32_t aown = (uint32_t)r * a.ars + xslot((uint32_t)xc, AB);
-        step_cell<T, true, SMAG, WRAP, false>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
+        step_cell<T, true, SMAG, WRAP, false, true>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
     }
 }
 

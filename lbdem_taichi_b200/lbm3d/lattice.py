@@ -182,6 +182,7 @@ class LatticeEngine:
         self._aux = (torch.zeros((nblk, 5, 32), dtype=tdtype, device=dev) if self.stress_enabled else None)
         self._stress = None
         self._stress_pending = False   # compute_stress() not evaluated yet (fused into the next collide)
+        self._links_all = N.LINK_FLUID   # cell types start as FLUID everywhere: one link mask
         self._links = torch.zeros(nc, dtype=torch.int32, device=dev)
         self._moving = None
         self.has_moving_walls = False
@@ -236,7 +237,7 @@ class LatticeEngine:
         L.rho, L.vel = N.ptr(self._rho), N.ptr(self._vel)
         L.aux = N.ptr(self._aux)
         L.links = N.ptr(self._links)
-        L.links_all = N.LINK_FLUID       # cell types start as FLUID everywhere
+        L.links_all = self._links_all    # one mask for every cell (all FLUID), else 0
         L.status = N.ptr(self._status)
         L.ct = N.ptr(self._ct_dev)
 
@@ -255,7 +256,8 @@ class LatticeEngine:
                              "direction (lbm_solver3d.py:230-236)")
         self._ct_dev.copy_(torch.from_numpy(from_ref(host.astype(np.int32)).reshape(-1)))
         # an all-FLUID lattice has one link mask everywhere: the step reads none
-        self._lat.links_all = N.LINK_FLUID if bool((host == CellType.FLUID).all()) else 0
+        self._links_all = N.LINK_FLUID if bool((host == CellType.FLUID).all()) else 0
+        self._lat.links_all = self._links_all
         self.has_open_boundaries = bool(np.bitwise_and(host, _OPEN).any())
         self._has_slip = bool(slip.any())
         # moving walls and Ladd inlets: per-cell velocity-link bits, allocated on first use
