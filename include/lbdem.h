@@ -278,12 +278,16 @@ int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G, v
  * every particle accumulated into G->force_fluid / G->moment_fluid
  * (zeroed by lbdem_psc_map).  P/G may be NULL for a particle-free lattice.
  * With L->stress set, the stress diagnostics of the gathered state are
- * written too.  Two kernels implement the gathered step and give identical
- * results: one gathers with per-thread loads; the other (rows of up to 256
- * cells) has a producer warp copy whole upwind rows into shared memory with
- * the tensor memory accelerator, several rows ahead of the warps that collide
- * them.  The second is the default for 16-bit storage, the first for FP32;
- * LBDEM_STEP_KERNEL=rows or =simt in the environment selects one for all. */
+ * written too.  Three kernels implement the gathered step and give identical
+ * populations: one gathers with per-thread loads; the others (rows of up to
+ * 256 cells) have a producer warp copy whole upwind rows into shared memory
+ * with the tensor memory accelerator, several rows ahead of the warps that
+ * collide them, one cell per thread or -- 16-bit storage, even Nx, an even
+ * number of x-blocks -- two x-adjacent cells per thread in f32x2 arithmetic
+ * (its force sums group the cells differently: the same forces to FP32
+ * rounding).  Defaults: two cells per thread where it applies, else one, for
+ * 16-bit storage; per-thread gathers for FP32.  LBDEM_STEP_KERNEL=simt, =rows
+ * or =rows2 in the environment selects one form for every storage. */
 int lbdem_psc_step_f32(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
                        int32_t dst, int32_t gather, void *stream);
 int lbdem_psc_step_f16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,

@@ -133,6 +133,23 @@ template <> struct Lanes<float> {
     __device__ __forceinline__ static float rcp(float v) { return rcp_fast(v); }
     __device__ __forceinline__ static float sqrt(float v) { return sqrt_fast(v); }
 };
+// Two cells per thread: V = float2, every operation one f32x2 instruction
+// rounded per lane exactly as its scalar form (a - b as fma(b, -1, a)).
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return sub2(a, b); }
+__device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+template <> struct Lanes<float2> {
+    static constexpr int N = 2;
+    __device__ __forceinline__ static float2 splat(float s) { return make_float2(s, s); }
+    __device__ __forceinline__ static float get(float2 v, int i) { return i ? v.y : v.x; }
+    __device__ __forceinline__ static void set(float2 &v, int i, float s) {
+        if (i) v.y = s;
+        else v.x = s;
+    }
+    __device__ __forceinline__ static float2 rcp(float2 v) { return make_float2(rcp_fast(v.x), rcp_fast(v.y)); }
+    __device__ __forceinline__ static float2 sqrt(float2 v) { return make_float2(sqrt_fast(v.x), sqrt_fast(v.y)); }
+};
 // c_q . (x, y, z) for odd q (whose first non-zero component is +1), with the
 // zero components dropped at compile time (q is a constant after unrolling;
 // 0 * v is not foldable under IEEE rules).
@@ -212,9 +229,9 @@ __device__ __forceinline__ float psc_cell(const StepArgs &a, uint32_t key, float
 // them (the reference always collides with its rho / vel fields).
 // PACK_PSC: the PSC pair updates also run two pairs per f32x2 instruction
 // (same rounding per lane; needs the registers of the row-staged kernel).
-template <class V, int SMAG, bool OVR = false, bool WRAP = false, bool PACK_PSC = false, class Out, class AuxOut,
-          class Macro>
-__device__ __forceinline__ void collide(const StepArgs &a, const V h[Q], const bool act[], const int xs[], int y,
+template <class V, int SMAG, bool OVR = false, bool WRAP = false, bool PACK_PSC = false, class HA, class Out,
+          class AuxOut, class Macro>
+__device__ __forceinline__ void collide(const StepArgs &a, const HA &h, const bool act[], const int xs[], int y,
                                         int z, const V aux[5], bool psc, const uint32_t key[], const float eps[],
                                         CellForce cf[], Out &&out, AuxOut &&aux_out, Macro &&macro,
                                         const float *ovr = nullptr) {
@@ -546,10 +563,12 @@ __device__ __forceinline__ void write_stress(const StepArgs &a, const float h[Q]
 // cell, given its streamed populations raw[] (storage type), the lagged state
 // aux[], its owner key and link mask.  Shared by the kernel that gathers with
 // its own loads and the one that stages rows in shared memory.
+// psc_given: the collision form when the caller has decided it (0 BGK, 1
+// PSC); -1: PSC when any cell of the warp is owned (a warp is one x-block).
 template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS, bool PACK_PSC = false>
 __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z, bool inb, uint32_t cell,
                                           uint32_t own, uint32_t aown, T raw[Q], float aux[5], uint32_t key,
-                                          uint32_t lk) {
+                                          uint32_t lk, int psc_given = -1) {
     const bool act = inb && !(lk & (LINK_SKIP | LINK_DEFER));
     if (!act) key = 0u;
     if (GATHER && (lk & 0x7FFFEu)) {
@@ -565,7 +584,8 @@ __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z
     if constexpr (STRESS) {
         if (act) write_stress(a, h, aux, cell);
     }
-    const bool psc = a.key != nullptr && __any_sync(0xffffffffu, key != 0u);
+    const unsigned owners = __ballot_sync(0xffffffffu, key != 0u);
+    const bool psc = a.key != nullptr && (psc_given >= 0 ? psc_given != 0 : owners != 0u);
     CellForce cf[1];
     const bool acts[1] = {act};
     const int xs[1] = {x};
@@ -600,7 +620,7 @@ __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z
             a.hydro_out[2 * a.nc + cell] = cf[0].hz;
         }
     }
-    if (psc) reduce_forces(a, cf[0]);
+    if (a.key != nullptr && owners != 0u) reduce_forces(a, cf[0]);
 }
 
 // LISTED (pipelined stepping): one-dimensional blocks whose warps take the
@@ -888,6 +908,232 @@ __global__ void __launch_bounds__(ROW_THREADS + 32, ROW_MIN_BLOCKS) k_psc_step_r
         const uint32_t own = (uint32_t)r * a.rs + xslot((uint32_t)xc, QB);
         const uint32_t aown = (uint32_t)r * a.ars + xslot((uint32_t)xc, AB);
         step_cell<T, true, SMAG, WRAP, false, true>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
+    }
+}
+
+// Two x-adjacent cells per consumer thread (16-bit storage, even Nx): the
+// staged rows are read as 32-bit pairs (x, x+1) -- for c_x = +-1 the shifted
+// pair is assembled from two aligned words with a byte permute -- and the
+// collision runs on float2 values (f32x2 instructions, each lane rounded as
+// the one-cell form, so the results are identical), with every population
+// widened on demand from the packed pair instead of held as two floats.
+// Stores are pairs too.  Warps whose 64 cells include wall, moving-wall,
+// open-boundary or skipped cells, or that use the smooth solid fraction, run
+// the one-cell step for each of their two cells instead.
+template <typename T> struct Pair16;
+template <> struct Pair16<__half> {
+    __device__ __forceinline__ static float2 widen(uint32_t w) {
+        return __half22float2(*reinterpret_cast<const __half2 *>(&w));
+    }
+    __device__ __forceinline__ static uint32_t narrow(float2 v) {
+        const __half2 h = __floats2half2_rn(v.x, v.y);
+        return *reinterpret_cast<const uint32_t *>(&h);
+    }
+};
+template <> struct Pair16<__nv_bfloat16> {
+    __device__ __forceinline__ static float2 widen(uint32_t w) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&w));
+    }
+    __device__ __forceinline__ static uint32_t narrow(float2 v) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+        return *reinterpret_cast<const uint32_t *>(&h);
+    }
+};
+template <typename T> struct PairRow {
+    const uint32_t *w;
+    __device__ __forceinline__ float2 operator[](int q) const { return Pair16<T>::widen(w[q]); }
+};
+
+#ifndef ROW2_MIN_BLOCKS
+#define ROW2_MIN_BLOCKS 3
+#endif
+constexpr uint32_t LINK_NOT_PLAIN = 0x7FFFEu | LINK_SKIP | LINK_DEFER | LINK_MOVING | LINK_KEEP;
+
+template <typename T, int SMAG, bool WRAP>
+__global__ void __launch_bounds__(ROW_THREADS / 2 + 32, ROW2_MIN_BLOCKS) k_psc_step_rows2(
+    const StepArgs a, const __grid_constant__ RowMaps m) {
+    using RL = RowLayout<T>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[ROW_STAGES], empty[ROW_STAGES];
+    __shared__ volatile int abort_flag;
+    const int nx = a.nx, ny = a.ny;
+    const int nrows = ny * a.nz;
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t ncons = blockDim.x - 32u;          // consumer threads: 16 NB, NB even (whole warps)
+    const bool producer = threadIdx.x >= ncons;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ROW_STAGES; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), ncons / 32u);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        abort_flag = 0;
+    }
+    __syncthreads();
+    if (producer) {
+        if (threadIdx.x == ncons) {
+            int issued = 0;
+            for (int k = 0;; ++k) {
+                const int r = blockIdx.x + k * gridDim.x;
+                if (r >= nrows || abort_flag) break;
+                const int st = k % ROW_STAGES;
+                if (k >= ROW_STAGES && !mbar_wait(smem_u32(&empty[st]), (uint32_t)(k / ROW_STAGES - 1) & 1u)) {
+                    abort_flag = 1;
+                    break;
+                }
+                row_issue<T>(a, m, sbase + st * RL::stage, smem_u32(&full[st]), r);
+                issued = k + 1;
+            }
+            if (abort_flag) {
+                atomicOr(a.status, (int)LBDEM_ST_WAIT_TIMEOUT);
+                for (int k = issued - ROW_STAGES; k < issued; ++k)
+                    if (k >= 0) mbar_wait(smem_u32(&full[k % ROW_STAGES]), (uint32_t)(k / ROW_STAGES) & 1u);
+            }
+        }
+        return;
+    }
+    constexpr uint32_t spe = RL::slot / sizeof(T);   // elements per direction's row copy
+    for (int k = 0;; ++k) {
+        const int r = blockIdx.x + k * gridDim.x;
+        if (r >= nrows) break;
+        const int st = k % ROW_STAGES;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&full[st]), (uint32_t)(k / ROW_STAGES) & 1u));
+        if (!ok || abort_flag) {
+            if ((threadIdx.x & 31u) == 0) abort_flag = 1;
+            break;
+        }
+        const unsigned char *stage = smem + st * RL::stage;
+        const T *sf = reinterpret_cast<const T *>(stage);
+        const T *sa = reinterpret_cast<const T *>(stage + RL::off_aux);
+        const uint32_t *sk = reinterpret_cast<const uint32_t *>(stage + RL::off_key);
+        const uint32_t *sl = reinterpret_cast<const uint32_t *>(stage + RL::off_link);
+        const int z = r / ny, y = r - z * ny;
+        const int x0 = 2 * (int)threadIdx.x;
+        const bool inb = x0 < nx;                     // Nx even: both cells or neither
+        const int xc = inb ? x0 : 0;
+        const uint32_t cell = (uint32_t)r * (uint32_t)nx + (uint32_t)xc;
+        uint32_t key0, key1, lk0, lk1;
+        if (m.kl_tma) {
+            key0 = a.key != nullptr ? sk[xc] : 0u;
+            key1 = a.key != nullptr ? sk[xc + 1] : 0u;
+            lk0 = a.links_all ? a.links_all : sl[xc];
+            lk1 = a.links_all ? a.links_all : sl[xc + 1];
+        } else {
+            key0 = a.key != nullptr ? a.key[cell] : 0u;
+            key1 = a.key != nullptr ? a.key[cell + 1] : 0u;
+            lk0 = a.links_all ? a.links_all : a.links[cell];
+            lk1 = a.links_all ? a.links_all : a.links[cell + 1];
+        }
+        const bool plain = !__any_sync(0xffffffffu, ((lk0 | lk1) & LINK_NOT_PLAIN) != 0u) && a.eps == nullptr;
+        if (plain) {
+            const int xm2 = xc == 0 ? nx - 2 : xc - 2, xp2 = xc + 2 == nx ? 0 : xc + 2;
+            const uint32_t *sw = reinterpret_cast<const uint32_t *>(sf);
+            uint32_t raw[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const uint32_t *row = sw + q * (spe / 2);
+                if (cx(q) == 0) {
+                    raw[q] = row[xc >> 1];
+                } else if (cx(q) == 1) {       // (x - 1, x): high half of word x-2, low half of word x
+                    raw[q] = __byte_perm(row[xm2 >> 1], row[xc >> 1], 0x5432);
+                } else {                       // (x + 1, x + 2): high half of word x, low half of word x+2
+                    raw[q] = __byte_perm(row[xc >> 1], row[xp2 >> 1], 0x5432);
+                }
+            }
+            float2 aux[5] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                             make_float2(0.f, 0.f), make_float2(a.omega0, a.omega0)};
+            if (SMAG == LBDEM_SMAG_REFERENCE) {
+                const uint32_t *ap = reinterpret_cast<const uint32_t *>(sa + xslot((uint32_t)xc, AB));
+#pragma unroll
+                for (int kk = 0; kk < 5; ++kk) aux[kk] = Pair16<T>::widen(ap[kk * 16]);
+            }
+            __syncwarp();
+            if ((threadIdx.x & 31u) == 0) mbar_arrive(smem_u32(&empty[st]));
+            const bool act = inb;
+            const uint32_t own = (uint32_t)r * a.rs + xslot((uint32_t)xc, QB);
+            const uint32_t aown = (uint32_t)r * a.ars + xslot((uint32_t)xc, AB);
+            const uint32_t k0 = act ? key0 : 0u, k1 = act ? key1 : 0u;
+            // the PSC form is chosen per x-block (16 lanes) as the one-cell kernel chooses it per warp: the
+            // PSC update with B = 0 rounds differently from the BGK one
+            const unsigned owners = __ballot_sync(0xffffffffu, (k0 | k1) != 0u);
+            const bool psc_warp = a.key != nullptr && owners != 0u;
+            const bool psc = psc_warp && (owners & ((threadIdx.x & 16u) ? 0xFFFF0000u : 0x0000FFFFu)) != 0u;
+            CellForce cf[2];
+            const bool acts[2] = {act, act};
+            const int xs[2] = {x0, x0 + 1};
+            const uint32_t keys[2] = {k0, k1};
+            const float epss[2] = {0.f, 0.f};
+            uint32_t *d = reinterpret_cast<uint32_t *>(static_cast<T *>(a.dst) + own);
+            const PairRow<T> hrow{raw};
+            collide<float2, SMAG, false, WRAP>(
+                a, hrow, acts, xs, y, z, aux, psc, keys, epss, cf,
+                [&](int q, float2 v) {
+                    if (act) d[q * 16] = Pair16<T>::narrow(v);
+                },
+                [&](int kk, float2 v) { aux[kk] = v; }, [&](float2, float2, float2, float2) {});
+            if (act) {
+                if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
+                    uint32_t *ap = reinterpret_cast<uint32_t *>(static_cast<T *>(a.aux) + aown);
+#pragma unroll
+                    for (int kk = 0; kk < 5; ++kk) ap[kk * 16] = Pair16<T>::narrow(aux[kk]);
+                }
+                if (a.hydro_out) {
+                    a.hydro_out[cell] = cf[0].hx;
+                    a.hydro_out[a.nc + cell] = cf[0].hy;
+                    a.hydro_out[2 * a.nc + cell] = cf[0].hz;
+                    a.hydro_out[cell + 1] = cf[1].hx;
+                    a.hydro_out[a.nc + cell + 1] = cf[1].hy;
+                    a.hydro_out[2 * a.nc + cell + 1] = cf[1].hz;
+                }
+            }
+            if (psc_warp) {
+                // one reduction of the pair's summed force where both cells have the same owner (or one
+                // has none) in every lane; otherwise one per cell
+                const bool split = __any_sync(0xffffffffu, cf[0].gid >= 0 && cf[1].gid >= 0 && cf[0].gid != cf[1].gid);
+                if (!split) {
+                    CellForce c2 = cf[0];
+                    c2.gid = cf[0].gid >= 0 ? cf[0].gid : cf[1].gid;
+                    c2.hx += cf[1].hx; c2.hy += cf[1].hy; c2.hz += cf[1].hz;
+                    c2.tx += cf[1].tx; c2.ty += cf[1].ty; c2.tz += cf[1].tz;
+                    reduce_forces(a, c2);
+                } else {
+                    reduce_forces(a, cf[0]);
+                    reduce_forces(a, cf[1]);
+                }
+            }
+        } else {
+            // one cell at a time with the one-cell step; the stage is released after both reads.  The
+            // collision form is the one-cell kernel's: PSC when any cell of the x-block (this warp's lanes
+            // 0-15 or 16-31, both cells of each) is owned and updated
+            const uint32_t ab = LINK_SKIP | LINK_DEFER;
+            const bool owned = (inb && !(lk0 & ab) && key0) || (inb && !(lk1 & ab) && key1);
+            const unsigned owners = __ballot_sync(0xffffffffu, owned);
+            const int psc_block = (owners & ((threadIdx.x & 16u) ? 0xFFFF0000u : 0x0000FFFFu)) != 0u;
+#pragma unroll 1
+            for (int c = 0; c < 2; ++c) {
+                const int x = x0 + c;
+                const int xx = inb ? x : 0;
+                const int xm = xx == 0 ? nx - 1 : xx - 1, xp = xx == nx - 1 ? 0 : xx + 1;
+                T raw[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) raw[q] = sf[q * spe + (cx(q) == 1 ? xm : (cx(q) == -1 ? xp : xx))];
+                float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
+                if (SMAG == LBDEM_SMAG_REFERENCE) {
+                    const T *ap = sa + xslot((uint32_t)xx, AB);
+#pragma unroll
+                    for (int kk = 0; kk < 5; ++kk) aux[kk] = aux_dec<T>(ap[kk * 32]);
+                }
+                if (c == 1) {
+                    __syncwarp();
+                    if ((threadIdx.x & 31u) == 0) mbar_arrive(smem_u32(&empty[st]));
+                }
+                const uint32_t cl = (uint32_t)r * (uint32_t)nx + (uint32_t)xx;
+                const uint32_t own = (uint32_t)r * a.rs + xslot((uint32_t)xx, QB);
+                const uint32_t aown = (uint32_t)r * a.ars + xslot((uint32_t)xx, AB);
+                step_cell<T, true, SMAG, WRAP, false>(a, x, y, z, inb, cl, own, aown, raw, aux, c ? key1 : key0,
+                                                      c ? lk1 : lk0, psc_block);
+            }
+        }
     }
 }
 
@@ -1687,17 +1933,21 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     return fn;
 }
 
-// Which form of the gathered full-lattice step runs.  By default the
-// row-staged one for 16-bit storage (measured 2 % faster than k_psc_step at
-// 256^3) and k_psc_step for FP32 (the row-staged FP32 step fits only two CTAs
-// per SM in shared memory and measured 30 % slower); LBDEM_STEP_KERNEL=rows or
-// =simt in the environment at the call selects one form for every storage.
+// Which form of the gathered full-lattice step runs: 0 per-thread gathers
+// (k_psc_step), 1 row-staged one cell per thread, 2 row-staged two cells per
+// thread.  By default the row-staged forms for 16-bit storage (two cells per
+// thread where Nx is even) and k_psc_step for FP32 (the row-staged FP32 step
+// fits only two CTAs per SM in shared memory and measured 30 % slower);
+// LBDEM_STEP_KERNEL=simt, =rows or =rows2 in the environment at the call
+// selects one form for every storage (=rows2 falls back to =rows where it
+// does not apply).
 template <typename T>
-static bool rows_kernel_enabled() {
+static int step_kernel_form() {
     const char *e = getenv("LBDEM_STEP_KERNEL");
-    if (e && strcmp(e, "simt") == 0) return false;
-    if (e && strcmp(e, "rows") == 0) return true;
-    return sizeof(T) == 2;
+    if (e && strcmp(e, "simt") == 0) return 0;
+    if (e && strcmp(e, "rows") == 0) return 1;
+    if (e && strcmp(e, "rows2") == 0) return 2;
+    return sizeof(T) == 2 ? 2 : 0;
 }
 
 template <typename T> constexpr CUtensorMapDataType tmap_type();
@@ -1707,18 +1957,32 @@ template <> constexpr CUtensorMapDataType tmap_type<__nv_bfloat16>() { return CU
 
 static uint32_t round_up(uint32_t v, uint32_t m) { return (v + m - 1) / m * m; }
 
+// the row-staged kernel of a form: two cells per thread exists for 16-bit storage only
+template <typename T, int SMAG, bool WRAP, bool PAIRS> struct RowKernel {
+    static auto fn() { return k_psc_step_rows<T, SMAG, WRAP>; }
+};
+template <int SMAG, bool WRAP> struct RowKernel<__half, SMAG, WRAP, true> {
+    static auto fn() { return k_psc_step_rows2<__half, SMAG, WRAP>; }
+};
+template <int SMAG, bool WRAP> struct RowKernel<__nv_bfloat16, SMAG, WRAP, true> {
+    static auto fn() { return k_psc_step_rows2<__nv_bfloat16, SMAG, WRAP>; }
+};
+
 constexpr int ROWS_NOT_APPLICABLE = -1;
 
 // Launch the row-staged step; ROWS_NOT_APPLICABLE for rows wider than 256
 // cells, with too little shared memory for two CTAs per SM, when the driver
 // has no tensor-map encoder, or when a copy's description is refused -- the
 // caller then launches k_psc_step.
-template <typename T, int SMAG, bool WRAP>
+template <typename T, int SMAG, bool WRAP, bool PAIRS>
 static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStream_t st) {
     auto encode = tmap_encoder();
-    // one thread per cell of a row: rows of up to ROW_THREADS cells (a loop over
-    // wider rows costs registers the step does not have)
+    // one thread per cell (PAIRS: per two cells) of a row: rows of up to
+    // ROW_THREADS cells (a loop over wider rows costs registers the step does not have)
     if (!encode || 32u * a.nb > (uint32_t)ROW_THREADS || a.src == nullptr) return ROWS_NOT_APPLICABLE;
+    // two cells per thread: 16-bit storage, even Nx, and an even number of x-blocks so that the 16 NB
+    // consumer threads are whole warps (the producer warp then starts on a warp boundary)
+    if (PAIRS && (sizeof(T) != 2 || (a.nx & 1) || (a.nb & 1u))) return ROWS_NOT_APPLICABLE;
     const uint32_t es = sizeof(T), nb = a.nb;
     RowMaps m;
     memset(&m, 0, sizeof(m));
@@ -1763,7 +2027,7 @@ static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStrea
                             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return ROWS_NOT_APPLICABLE;
     }
-    auto kern = k_psc_step_rows<T, SMAG, WRAP>;
+    auto kern = RowKernel<T, SMAG, WRAP, PAIRS>::fn();
     static uint32_t smem_set = 0;    // per instantiation
     if (smem > smem_set) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
@@ -1772,7 +2036,7 @@ static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStrea
         }
         smem_set = smem;
     }
-    const int threads = (int)(32u * nb) + 32;   // consumers + the producer warp
+    const int threads = (int)((PAIRS ? 16u : 32u) * nb) + 32;   // consumers + the producer warp
     int per_sm = 0, dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1828,9 +2092,15 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
     step_geometry(L, grid, block, ONE_THREADS);
 #define LBDEM_STEP_CASE(G_, S_)                                                          \
     do {                                                                                 \
-        if (G_ && !a.stress_out && rows_kernel_enabled<T>()) {                           \
-            const int rc_ = a.wrap_any ? launch_step_rows<T, S_, true>(L, a, st)          \
-                                       : launch_step_rows<T, S_, false>(L, a, st);        \
+        const int form_ = step_kernel_form<T>();                                         \
+        if (G_ && !a.stress_out && form_ > 0) {                                          \
+            int rc_ = ROWS_NOT_APPLICABLE;                                               \
+            if (form_ == 2)                                                              \
+                rc_ = a.wrap_any ? launch_step_rows<T, S_, true, true>(L, a, st)          \
+                                 : launch_step_rows<T, S_, false, true>(L, a, st);        \
+            if (rc_ == ROWS_NOT_APPLICABLE)                                              \
+                rc_ = a.wrap_any ? launch_step_rows<T, S_, true, false>(L, a, st)         \
+                                 : launch_step_rows<T, S_, false, false>(L, a, st);       \
             if (rc_ != ROWS_NOT_APPLICABLE) {                                            \
                 if (rc_ != LBDEM_OK) return rc_;                                         \
                 launch_boundary<T, S_, BND_GATHER>(L, a, st);                            \

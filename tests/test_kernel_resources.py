@@ -5,6 +5,11 @@ writes (no GPU needed).  The measured speeds depend on them:
   form and map form): at most 64 registers (4 blocks of 256 threads per SM)
   and no spills; with the fused stress output at most 64 registers and a
   few spilled words (16 bytes at most);
+- the row-staged steps: one cell per thread at most 72 registers (three CTAs
+  of 288 threads per SM) with at most two spilled words; two cells per thread
+  (16-bit storage) at most 128 registers (three CTAs of 160 threads), no
+  spills in the reference Smagorinsky form the benchmarks run and at most
+  24 bytes in the others;
 - the PSC map scatter without periodic images: at most 48 registers (five
   256-thread blocks per SM) and no spills;
 - the DEM kernels (contacts, integration, the cooperative and the one-block
@@ -62,6 +67,17 @@ def test_fused_step_with_stress(res):
     assert len(got) == 3 * 3 * 2
     bad = {k: v for k, v in got.items() if v[0] > 64 or v[1] > 16}
     assert not bad, bad
+
+
+def test_row_staged_steps(res):
+    one = _match(res, r"k_psc_step_rowsI")
+    assert len(one) == 3 * 3 * 2
+    assert all(r <= 72 and s <= 8 for r, s in one.values()), one
+    two = _match(res, r"k_psc_step_rows2I")
+    assert len(two) == 2 * 3 * 2
+    assert all(r <= 128 and s <= 24 for r, s in two.values()), two
+    ref = {k: v for k, v in two.items() if "Li1E" in k}
+    assert ref and all(s == 0 for _, s in ref.values()), ref
 
 
 def test_map_scatter(res):
