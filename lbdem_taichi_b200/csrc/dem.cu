@@ -665,10 +665,10 @@ __global__ void __launch_bounds__(128) k_dem_block(const __grid_constant__ DemAr
 // All sub-steps of one call in ONE cooperative launch (the default): every
 // block of the grid is resident (cudaLaunchCooperativeKernel), the contact
 // lanes and the particles are grid-strided, and the two phases of each
-// sub-step are separated by a grid barrier.  The barrier is a counter plus a
-// generation word in caller-owned memory (reset before each launch); its wait
-// is bounded: after ~0.25 s without progress it sets LBDEM_ST_WAIT_TIMEOUT and
-// continues, so a fault can never hang the GPU.
+// sub-step are separated by a grid barrier.  The barrier is an arrival counter
+// in caller-owned memory (zeroed before each launch); its wait is bounded:
+// after ~0.25 s without progress it sets LBDEM_ST_WAIT_TIMEOUT and continues,
+// so a fault can never hang the GPU.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
     unsigned v;
@@ -679,26 +679,25 @@ __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Arrivals count up monotonically in sync[0] (zeroed before each launch): the
+// k-th barrier is passed when the count reaches k * gridDim.x.  One fence and
+// one atomic per block and barrier (the fence publishes the block's writes of
+// the phase, ordered before thread 0 by the block barrier), then polling with
+// acquire loads; no reset, so no second fence.
 __device__ __forceinline__ void grid_barrier(uint32_t *sync, unsigned &gen, int32_t *status) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();   // this block's writes of the phase, visible GPU-wide
-        const unsigned target = gen + 1;
-        if (atomicAdd(sync, 1u) == gridDim.x - 1) {
-            sync[0] = 0u;   // nobody arrives again before the generation moves
-            __threadfence();
-            st_release_gpu(sync + 1, target);
-        } else {
-            unsigned it = 0;
-            while (ld_acquire_gpu(sync + 1) != target) {
-                if (++it > (1u << 22)) {
-                    atomicOr(status, (int)LBDEM_ST_WAIT_TIMEOUT);
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
+        const unsigned target = (gen + 1) * gridDim.x;
         __threadfence();
+        atomicAdd(sync, 1u);
+        unsigned it = 0;
+        while (ld_acquire_gpu(sync) < target) {
+            if (++it > (1u << 22)) {
+                atomicOr(status, (int)LBDEM_ST_WAIT_TIMEOUT);
+                break;
+            }
+            __nanosleep(32);
+        }
     }
     gen += 1;
     __syncthreads();
@@ -850,7 +849,8 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
             // grid-stride loop serialises the phases' memory-latency chains and
             // two launches per sub-step (all lanes in flight) are faster
             const int nb = max(nb_con, nb_int);
-            if (nb <= per_sm * nsm) {
+            // the arrival counter reaches 2 nsub nb within the launch: keep it far from wrapping
+            if (nb <= per_sm * nsm && 2ll * nsub * nb < (1ll << 30)) {
                 if (cudaMemsetAsync(D->sync, 0, 2 * sizeof(uint32_t), st) != cudaSuccess)
                     return check_launch("dem_substeps (barrier reset)");
                 A.parity = D->parity;
