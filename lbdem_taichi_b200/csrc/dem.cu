@@ -500,7 +500,8 @@ __device__ __forceinline__ void wrap_position(const lbdem_dem &d, double *p) {
     }
 }
 
-__device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, int i);
+__device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, int i, int role);
+__device__ __forceinline__ void integrate_unit(const lbdem_dem &d, int ncell, int parity, int u);
 
 __global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemArgs A) {
     const lbdem_dem &d = A.d;
@@ -508,111 +509,131 @@ __global__ void __launch_bounds__(128) k_integrate(const __grid_constant__ DemAr
     // clear the counts consumed by this sub-step (the other half receives the new binning)
     int32_t *used = d.cell_count + (size_t)A.parity * A.ncell;
     for (int c = tid; c < A.ncell; c += gridDim.x * blockDim.x) used[c] = 0;
-    if (tid < d.n) integrate_particle(d, A.ncell, A.parity, tid);
+    if (tid < 3 * d.n) integrate_unit(d, A.ncell, A.parity, tid);
 }
 
-__device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, int i) {
+__device__ void integrate_particle(const lbdem_dem &d, int ncell, int parity, int i, int role) {
     const double dt = d.dt;
-    // every input of the particle is fetched before any store, so the loads
-    // overlap (one memory round trip instead of a chain)
-    double af[3], am[3], ffl[3], mfl[3], p[3], v[3], acc[3], w[3], wd[3], q[4], I[9];
-    for (int t = 0; t < 3; ++t) {
-        af[t] = d.acc_force[3 * i + t];
-        am[t] = d.acc_moment[3 * i + t];
-        ffl[t] = d.force_fluid[3 * i + t];
-        mfl[t] = d.moment_fluid[3 * i + t];
-        p[t] = d.pos[3 * i + t];
-        v[t] = d.vel[3 * i + t];
-        acc[t] = d.acc[3 * i + t];
-        w[t] = d.omega[3 * i + t];
-        wd[t] = d.omega_dot[3 * i + t];
-    }
-    for (int t = 0; t < 4; ++t) q[t] = d.quat[4 * i + t];
-    for (int t = 0; t < 9; ++t) I[t] = d.inertia[9 * i + t];
-    const double mass = d.mass[i];
     const int frozen = d.freeze[i], fixed = d.fixvel[i];
-    const size_t base = (size_t)i * d.maxc;
-    const int nfirst = d.cfn[i], nadd = d.cf_add[i];
-    int act[SLOTS_IN_REGS];
-#pragma unroll
-    for (int o = 0; o < SLOTS_IN_REGS; ++o) act[o] = o < d.maxc ? d.cf_active[base + o] : 0;
-
-    // clear_state (demsolver.py:422-429) + contacts, then apply_body_force (:437-448)
-    double force[3], moment[3];
-    for (int t = 0; t < 3; ++t) {
-        double f = af[t], m = am[t];
-        f += mass * d.g[t];
-        m += 0.0;
-        f += ffl[t];
-        m += mfl[t];
-        force[t] = f;
-        moment[t] = m;
-    }
-    // update (demsolver.py:514-636)
-    if (!frozen) {
-        if (fixed) {
-            for (int t = 0; t < 3; ++t) p[t] += v[t] * dt;
-            wrap_position(d, p);
-            rotate_update(dt, q, w, wd, moment, I);
-        } else {
-            double a[3];
-            for (int t = 0; t < 3; ++t) a[t] = force[t] / mass;
-            for (int t = 0; t < 3; ++t) v[t] += 0.5 * (acc[t] + a[t]) * dt;
-            for (int t = 0; t < 3; ++t) p[t] += v[t] * dt + 0.5 * a[t] * (dt * dt);
-            wrap_position(d, p);
-            for (int t = 0; t < 3; ++t) acc[t] = a[t];
-            rotate_update(dt, q, w, wd, moment, I);
+    if (role == 0) {
+        // clear_state (demsolver.py:422-429) + contacts, then apply_body_force (:437-448): the force;
+        // update (demsolver.py:514-589): translation; then the binning for the next sub-step.  Every
+        // input is fetched before any store, so the loads overlap.
+        double af[3], ffl[3], p[3], v[3], acc[3];
+        for (int t = 0; t < 3; ++t) {
+            af[t] = d.acc_force[3 * i + t];
+            ffl[t] = d.force_fluid[3 * i + t];
+            p[t] = d.pos[3 * i + t];
+            v[t] = d.vel[3 * i + t];
+            acc[t] = d.acc[3 * i + t];
         }
-    }
-    for (int t = 0; t < 3; ++t) {
-        d.acc_force[3 * i + t] = 0.0;
-        d.acc_moment[3 * i + t] = 0.0;
-        d.force[3 * i + t] = force[t];
-        d.moment[3 * i + t] = moment[t];
-        d.pos[3 * i + t] = p[t];
-        d.vel[3 * i + t] = v[t];
-        d.acc[3 * i + t] = acc[t];
-        d.omega[3 * i + t] = w[t];
-        d.omega_dot[3 * i + t] = wd[t];
-    }
-    for (int t = 0; t < 4; ++t) d.quat[4 * i + t] = q[t];
-    // late_clear_state / remove_inactive_contact (demsolver.py:371-386, 431-436):
-    // slots are only moved when an inactive one precedes an active one
-    const int cnt = min(nfirst + nadd, d.maxc);
-    int w_ = 0;
-    auto keep = [&](int o) {
-        if (w_ != o) {
-            const size_t dd = base + w_, ss = base + o;
-            d.cf_j[dd] = d.cf_j[ss];
-            d.cf_active[dd] = 1;
-            for (int t = 0; t < 3; ++t) {
-                d.cf_shear[3 * dd + t] = d.cf_shear[3 * ss + t];
-                d.cf_pos[3 * dd + t] = d.cf_pos[3 * ss + t];
-                d.cf_force[3 * dd + t] = d.cf_force[3 * ss + t];
+        const double mass = d.mass[i];
+        double force[3];
+        for (int t = 0; t < 3; ++t) {
+            double f = af[t];
+            f += mass * d.g[t];
+            f += ffl[t];
+            force[t] = f;
+        }
+        if (!frozen) {
+            if (fixed) {
+                for (int t = 0; t < 3; ++t) p[t] += v[t] * dt;
+                wrap_position(d, p);
+            } else {
+                double a[3];
+                for (int t = 0; t < 3; ++t) a[t] = force[t] / mass;
+                for (int t = 0; t < 3; ++t) v[t] += 0.5 * (acc[t] + a[t]) * dt;
+                for (int t = 0; t < 3; ++t) p[t] += v[t] * dt + 0.5 * a[t] * (dt * dt);
+                wrap_position(d, p);
+                for (int t = 0; t < 3; ++t) acc[t] = a[t];
             }
         }
-        ++w_;
-    };
+        for (int t = 0; t < 3; ++t) {
+            d.acc_force[3 * i + t] = 0.0;
+            d.force[3 * i + t] = force[t];
+            d.pos[3 * i + t] = p[t];
+            d.vel[3 * i + t] = v[t];
+            d.acc[3 * i + t] = acc[t];
+        }
+        // bin the new position for the next sub-step
+        int ijk[3];
+        ref_cell(d, p, ijk);
+        const int c = cell_index(d, ijk[0], ijk[1], ijk[2]);
+        if (c < 0) {
+            atomicOr(d.status, (int)LBDEM_ST_GRID_OVERFLOW);
+            return;
+        }
+        int32_t *count = d.cell_count + (size_t)(parity ^ 1) * ncell;
+        const int rank = atomicAdd(count + c, 1);
+        if (rank < d.cell_cap) d.cell_list[(size_t)c * d.cell_cap + rank] = i;
+        else atomicOr(d.status, (int)LBDEM_ST_CELL_OVERFLOW);
+    } else if (role == 1) {
+        // the moment and the Euler rotation update (demsolver.py:590-636)
+        double am[3], mfl[3], w[3], wd[3], q[4], I[9];
+        for (int t = 0; t < 3; ++t) {
+            am[t] = d.acc_moment[3 * i + t];
+            mfl[t] = d.moment_fluid[3 * i + t];
+            w[t] = d.omega[3 * i + t];
+            wd[t] = d.omega_dot[3 * i + t];
+        }
+        for (int t = 0; t < 4; ++t) q[t] = d.quat[4 * i + t];
+        for (int t = 0; t < 9; ++t) I[t] = d.inertia[9 * i + t];
+        double moment[3];
+        for (int t = 0; t < 3; ++t) {
+            double m = am[t];
+            m += 0.0;
+            m += mfl[t];
+            moment[t] = m;
+        }
+        if (!frozen) rotate_update(dt, q, w, wd, moment, I);
+        for (int t = 0; t < 3; ++t) {
+            d.acc_moment[3 * i + t] = 0.0;
+            d.moment[3 * i + t] = moment[t];
+            d.omega[3 * i + t] = w[t];
+            d.omega_dot[3 * i + t] = wd[t];
+        }
+        for (int t = 0; t < 4; ++t) d.quat[4 * i + t] = q[t];
+    } else {
+        // late_clear_state / remove_inactive_contact (demsolver.py:371-386, 431-436):
+        // slots are only moved when an inactive one precedes an active one
+        const size_t base = (size_t)i * d.maxc;
+        const int nfirst = d.cfn[i], nadd = d.cf_add[i];
+        int act[SLOTS_IN_REGS];
 #pragma unroll
-    for (int o = 0; o < SLOTS_IN_REGS; ++o)
-        if (o < cnt && act[o]) keep(o);
-    for (int o = SLOTS_IN_REGS; o < cnt; ++o)
-        if (d.cf_active[base + o]) keep(o);
-    for (int o = w_; o < cnt; ++o) d.cf_active[base + o] = 0;
-    d.cfn[i] = w_;
-    d.cf_add[i] = 0;
-    // bin the new position for the next sub-step
-    int ijk[3];
-    ref_cell(d, p, ijk);
-    const int c = cell_index(d, ijk[0], ijk[1], ijk[2]);
-    if (c < 0) {
-        atomicOr(d.status, (int)LBDEM_ST_GRID_OVERFLOW);
-        return;
+        for (int o = 0; o < SLOTS_IN_REGS; ++o) act[o] = o < d.maxc ? d.cf_active[base + o] : 0;
+        const int cnt = min(nfirst + nadd, d.maxc);
+        int w_ = 0;
+        auto keep = [&](int o) {
+            if (w_ != o) {
+                const size_t dd = base + w_, ss = base + o;
+                d.cf_j[dd] = d.cf_j[ss];
+                d.cf_active[dd] = 1;
+                for (int t = 0; t < 3; ++t) {
+                    d.cf_shear[3 * dd + t] = d.cf_shear[3 * ss + t];
+                    d.cf_pos[3 * dd + t] = d.cf_pos[3 * ss + t];
+                    d.cf_force[3 * dd + t] = d.cf_force[3 * ss + t];
+                }
+            }
+            ++w_;
+        };
+#pragma unroll
+        for (int o = 0; o < SLOTS_IN_REGS; ++o)
+            if (o < cnt && act[o]) keep(o);
+        for (int o = SLOTS_IN_REGS; o < cnt; ++o)
+            if (d.cf_active[base + o]) keep(o);
+        for (int o = w_; o < cnt; ++o) d.cf_active[base + o] = 0;
+        d.cfn[i] = w_;
+        d.cf_add[i] = 0;
     }
-    int32_t *count = d.cell_count + (size_t)(parity ^ 1) * ncell;
-    const int rank = atomicAdd(count + c, 1);
-    if (rank < d.cell_cap) d.cell_list[(size_t)c * d.cell_cap + rank] = i;
-    else atomicOr(d.status, (int)LBDEM_ST_CELL_OVERFLOW);
+}
+
+// Integration of unit u of 3 n: role u / n (0 translation and binning, 1
+// rotation, 2 contact-slot compaction) of particle u % n.  The three parts
+// read and write disjoint state, so they run as three independent chains in
+// different warps.
+__device__ __forceinline__ void integrate_unit(const lbdem_dem &d, int ncell, int parity, int u) {
+    const int role = u / d.n;
+    integrate_particle(d, ncell, parity, u - role * d.n, role);
 }
 
 // All sub-steps of one call in ONE launch: a single thread-block cluster (up
@@ -635,7 +656,7 @@ __global__ void __launch_bounds__(512) k_dem_cluster(const __grid_constant__ Dem
         cl.sync();
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
-        for (int i = me; i < d.n; i += nthr) integrate_particle(d, A.ncell, parity, i);
+        for (int u = me; u < 3 * d.n; u += nthr) integrate_unit(d, A.ncell, parity, u);
         cl.sync();
     }
 }
@@ -656,7 +677,7 @@ __global__ void __launch_bounds__(128) k_dem_block(const __grid_constant__ DemAr
         __syncthreads();
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
-        for (int i = me; i < d.n; i += nthr) integrate_particle(d, A.ncell, parity, i);
+        for (int u = me; u < 3 * d.n; u += nthr) integrate_unit(d, A.ncell, parity, u);
         __syncthreads();
     }
 }
@@ -717,7 +738,7 @@ __global__ void __launch_bounds__(128) k_dem_coop(const __grid_constant__ DemArg
         grid_barrier(d.sync, gen, d.status);
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
-        for (int i = me; i < d.n; i += nthr) integrate_particle(d, A.ncell, parity, i);
+        for (int u = me; u < 3 * d.n; u += nthr) integrate_unit(d, A.ncell, parity, u);
         grid_barrier(d.sync, gen, d.status);
     }
 }
@@ -782,7 +803,7 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     DemArgs A;
     A.d = *D;
     A.ncell = D->gdim[0] * D->gdim[1] * D->gdim[2];
-    const int nb_int = max((D->n + 127) / 128, min(148, (A.ncell + 127) / 128));
+    const int nb_int = max((3 * D->n + 127) / 128, min(148, (A.ncell + 127) / 128));   // 3 units per particle
     const int nb_con = (int)((8ll * D->n + 127) / 128);
     // "cluster": all sub-steps in one launch of a single thread-block cluster
     // (opt-in: it confines the contact phase to <= 16 SMs and measured slower
