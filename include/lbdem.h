@@ -318,11 +318,17 @@ int lbdem_psc_step_bf16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_
  * Phase 1 and phase 2 together equal lbdem_psc_step_* when no particle moved
  * farther than the margin between the lists and the map (checked by
  * lbdem_psc_map when P->disp_limit > 0).  Periodic images (P->wrap) are not
- * supported here (LBDEM_ERR_UNSUPPORTED). */
+ * supported here (LBDEM_ERR_UNSUPPORTED).  entries: the caller's estimate of
+ * the phase's list length (e.g. the length an earlier step's lists had, read
+ * back asynchronously), or 0.  With 0 the launch covers every x-block and the
+ * CTAs past the device-side length exit at once; with an estimate it covers
+ * that many entries and a second, grid-striding launch of one CTA per SM
+ * processes any beyond them, so every listed block is stepped either way. */
 int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, double margin,
                           uint8_t *mask, uint32_t *blocks, uint32_t *counts, void *stream);
 int lbdem_psc_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
-                         int32_t dst, int32_t phase, const uint32_t *blocks, const uint32_t *counts, void *stream);
+                         int32_t dst, int32_t phase, const uint32_t *blocks, const uint32_t *counts,
+                         uint32_t entries, void *stream);
 
 /* Stream the post-collision populations of f[src] into f[dst] and write
  * rho/vel of FLUID cells (the reference's stream(), no collision). */

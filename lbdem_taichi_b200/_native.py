@@ -103,7 +103,7 @@ EXPORTS = {
     "lbdem_psc_force_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
     "lbdem_boundary_cells": ([vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_uint32, vp, vp, vp], C.c_int),
     "lbdem_psc_near_blocks": ([vp, vp, vp, C.c_double, vp, vp, vp, vp], C.c_int),
-    "lbdem_psc_step_phase": ([vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
+    "lbdem_psc_step_phase": ([vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_uint32, vp], C.c_int),
 }
 
 _lib = None
@@ -158,6 +158,8 @@ def _boundary_phases(arg):
 def call(name: str, *args):
     rc = getattr(load(), name)(*args)
     _launches[0] += load().lbdem_dem_launches_last() if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
+    if name == "lbdem_psc_step_phase" and args[8]:
+        _launches[0] += 1     # a launch sized from an estimate is followed by the one that takes the rest
     if name in _BOUNDARY_CALLS or (name == "lbdem_psc_step_phase" and args[5] == 2):
         _launches[0] += _boundary_phases(args[0])
     if rc != LBDEM_OK:

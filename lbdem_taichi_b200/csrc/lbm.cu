@@ -85,6 +85,7 @@ struct StepArgs {
     uint32_t nblocks;               // rows * nb
     float *stress_out;              // 7 planes of Ncells: stress of the gathered state (fused output), or NULL
     uint32_t links_all;             // nonzero: the link mask of every cell (no per-cell masks are read)
+    uint32_t lbase;                 // listed launches: index of the first list entry of this launch
 };
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
@@ -623,27 +624,11 @@ __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z
     if (a.key != nullptr && owners != 0u) reduce_forces(a, cf[0]);
 }
 
-// LISTED (pipelined stepping): one-dimensional blocks whose warps take the
-// x-blocks of a compact list (blist / bcount), so every warp of a CTA has
-// work; otherwise the grid covers the lattice.  A warp is one x-block.
-// STRESS: also write the stress diagnostics of the gathered state (a.stress_out).
-template <typename T, bool GATHER, int SMAG, bool WRAP, bool LISTED = false, bool STRESS = false>
-__global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
+// The fused step of the cell (x, y, z) of this thread: gathers, lagged state,
+// key and link mask, then step_cell.
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS>
+__device__ __forceinline__ void step_at(const StepArgs &a, int x, int y, int z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    int x, y, z;
-    if constexpr (LISTED) {
-        const uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-        if (w >= *a.bcount) return;   // warp-uniform
-        // entry: z | y | x-block (bits 20-31 | 8-19 | 0-7)
-        const uint32_t e = a.blist[a.bfrom_end ? a.nblocks - *a.bcount + w : w];
-        x = (int)((e & 0xFFu) * 32u + (threadIdx.x & 31u));
-        y = (int)((e >> 8) & 0xFFFu);
-        z = (int)(e >> 20);
-    } else {
-        x = blockIdx.x * blockDim.x + threadIdx.x;
-        y = blockIdx.y * blockDim.y + threadIdx.y;
-        z = blockIdx.z;
-    }
     const bool inb = (x < nx) && (y < ny);
     const int xc_ = inb ? x : 0, yc_ = inb ? y : 0;
     const uint32_t row = (uint32_t)(z * ny + yc_);
@@ -694,6 +679,42 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
     step_cell<T, GATHER, SMAG, WRAP, STRESS>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
 }
 
+// LISTED (pipelined stepping): one-dimensional blocks whose warps take the
+// x-blocks of a compact list (blist / bcount), so every warp of a CTA has
+// work; otherwise the grid covers the lattice.  A warp is one x-block.
+// STRESS: also write the stress diagnostics of the gathered state (a.stress_out).
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool LISTED = false, bool STRESS = false>
+__global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
+    int x, y, z;
+    if constexpr (LISTED) {
+        const uint32_t w = a.lbase + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (w >= *a.bcount) return;   // warp-uniform
+        // entry: z | y | x-block (bits 20-31 | 8-19 | 0-7)
+        const uint32_t e = a.blist[a.bfrom_end ? a.nblocks - *a.bcount + w : w];
+        x = (int)((e & 0xFFu) * 32u + (threadIdx.x & 31u));
+        y = (int)((e >> 8) & 0xFFFu);
+        z = (int)(e >> 20);
+    } else {
+        x = blockIdx.x * blockDim.x + threadIdx.x;
+        y = blockIdx.y * blockDim.y + threadIdx.y;
+        z = blockIdx.z;
+    }
+    step_at<T, GATHER, SMAG, WRAP, STRESS>(a, x, y, z);
+}
+
+// The list entries beyond those a listed launch of k_psc_step covered (from
+// a.lbase), a warp per entry, striding by the grid's warps: a launch sized
+// from an earlier step's list length leaves none or a few for this one.
+template <typename T, int SMAG>
+__global__ void __launch_bounds__(ONE_THREADS) k_psc_step_listed_rest(const StepArgs a) {
+    const uint32_t n = *a.bcount;
+    const uint32_t stride = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t w = a.lbase + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n; w += stride) {
+        const uint32_t e = a.blist[a.bfrom_end ? a.nblocks - n + w : w];
+        step_at<T, true, SMAG, false, false>(a, (int)((e & 0xFFu) * 32u + (threadIdx.x & 31u)),
+                                             (int)((e >> 8) & 0xFFFu), (int)(e >> 20));
+    }
+}
 
 // ---------------------------------------------------------------------------
 // fused step with the gathered rows staged in shared memory by the tensor
@@ -2134,7 +2155,8 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
 // force), phase 2 = near blocks with the map, then the boundary pass.
 template <typename T>
 static int launch_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int src, int dst,
-                             int phase, const uint32_t *blocks, const uint32_t *counts, cudaStream_t st) {
+                             int phase, const uint32_t *blocks, const uint32_t *counts, uint32_t entries,
+                             cudaStream_t st) {
     if (phase != 1 && phase != 2) {
         set_error("psc_step_phase: phase must be 1 or 2");
         return LBDEM_ERR_ARG;
@@ -2175,11 +2197,28 @@ static int launch_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const l
         a.moment_fluid = G->moment_fluid;
         a.hydro_out = P->hydro_out;
     }
-    // the list length is on the device: cover every block; CTAs past it leave at once
-    const dim3 block(ONE_THREADS, 1, 1), grid((a.nblocks + ONE_THREADS / 32 - 1) / (ONE_THREADS / 32), 1, 1);
+    // The list length is on the device.  Without an estimate (entries = 0) the
+    // launch covers every block and CTAs past the length leave at once; with
+    // one, it covers `entries` list entries and a grid-striding launch of one
+    // CTA per SM takes any beyond them.
+    const uint32_t wpb = ONE_THREADS / 32;
+    const bool sized = entries > 0 && entries < a.nblocks;
+    const uint32_t cover = sized ? entries : a.nblocks;
+    const dim3 block(ONE_THREADS, 1, 1), grid((cover + wpb - 1) / wpb, 1, 1);
+    int nsm = 0;
+    if (sized) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    }
 #define LBDEM_PHASE_CASE(S_)                                                              \
     do {                                                                                  \
         k_psc_step<T, true, S_, false, true><<<grid, block, 0, st>>>(a);                  \
+        if (sized) {                                                                      \
+            StepArgs r = a;                                                               \
+            r.lbase = grid.x * wpb;                                                       \
+            k_psc_step_listed_rest<T, S_><<<nsm, ONE_THREADS, 0, st>>>(r);                \
+        }                                                                                 \
         if (phase == 2) launch_boundary<T, S_, BND_GATHER>(L, a, st);                     \
     } while (0)
     if (L->smag_mode == LBDEM_SMAG_OFF) LBDEM_PHASE_CASE(LBDEM_SMAG_OFF);
@@ -2410,13 +2449,15 @@ int lbdem_psc_step_bf16(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_
 }
 
 int lbdem_psc_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_grains *G, int32_t src,
-                         int32_t dst, int32_t phase, const uint32_t *blocks, const uint32_t *counts, void *stream) {
+                         int32_t dst, int32_t phase, const uint32_t *blocks, const uint32_t *counts, uint32_t entries,
+                         void *stream) {
     if (!L) return LBDEM_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     switch (L->storage) {
-        case LBDEM_F32: return launch_step_phase<float>(L, P, G, src, dst, phase, blocks, counts, st);
-        case LBDEM_F16: return launch_step_phase<__half>(L, P, G, src, dst, phase, blocks, counts, st);
-        case LBDEM_BF16: return launch_step_phase<__nv_bfloat16>(L, P, G, src, dst, phase, blocks, counts, st);
+        case LBDEM_F32: return launch_step_phase<float>(L, P, G, src, dst, phase, blocks, counts, entries, st);
+        case LBDEM_F16: return launch_step_phase<__half>(L, P, G, src, dst, phase, blocks, counts, entries, st);
+        case LBDEM_BF16:
+            return launch_step_phase<__nv_bfloat16>(L, P, G, src, dst, phase, blocks, counts, entries, st);
     }
     set_error("unknown storage form %d", L->storage);
     return LBDEM_ERR_ARG;

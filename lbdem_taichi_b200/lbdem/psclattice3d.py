@@ -83,6 +83,7 @@ class PSCLattice3D(LatticeEngine):
         # pipelined run(): near-block mask, side stream for the DEM and the next map
         self.pipeline_margin = 0.25
         self._pipeline_choice = None      # run(pipeline="auto"): measured on the first long run
+        self._hcounts = None              # pipelined run: list lengths read back (pinned host memory)
         self._pipeline_probe = None       # (sequential, pipelined) ms per step of that measurement
         self._near = None
         self._side = None
@@ -246,10 +247,37 @@ class PSCLattice3D(LatticeEngine):
         d.sync = None                      # no grid-wide DEM launch: its blocks share the GPU with the step
         self._psc.disp_limit = float(self.pipeline_margin)
 
+        nblk = self._near.numel()
+        if self._hcounts is None:
+            # list lengths read back asynchronously: each phase launch is sized from the latest one
+            # that has arrived (a launch beside it takes any entries beyond), not from all blocks
+            self._hcounts = torch.zeros((4, 2), dtype=torch.int32).pin_memory()
+            self._hcount_ev = [None] * 4
+        slot = [0]
+
         def near_blocks(buf, stream):
             # blocks a particle can reach before the DEM moves it (current positions)
             N.call("lbdem_psc_near_blocks", lat, psc, grains, float(self.pipeline_margin), N.ptr(self._near),
                    N.ptr(self._blocks[buf]), N.ptr(self._bcounts[buf]), stream.cuda_stream)
+            i = slot[0] % 4
+            with torch.cuda.stream(stream):
+                self._hcounts[i].copy_(self._bcounts[buf][:2], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+            self._hcount_ev[i] = (slot[0], ev)
+            slot[0] += 1
+
+        def estimate():
+            # (far, near) list lengths of the newest read-back that has completed, with 3 % + 64 headroom
+            best = None
+            for rec in self._hcount_ev:
+                if rec is not None and (best is None or rec[0] > best[0]) and rec[1].query():
+                    best = rec
+            if best is None:
+                return 0, 0
+            far, near = (int(v) for v in self._hcounts[best[0] % 4])
+            pad = lambda c: c + c // 32 + 64 if c + c // 32 + 64 < nblk else 0  # noqa: E731
+            return pad(far), pad(near)
 
         try:
             self.collide()                 # step 0: map and full fused step
@@ -280,11 +308,12 @@ class PSCLattice3D(LatticeEngine):
                 lists = nxt if k < n - 2 else None
                 src = self._cur
                 blk = (N.ptr(self._blocks[buf]), N.ptr(self._bcounts[buf]))
-                N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 1, *blk, S.cuda_stream)
+                far_n, near_n = estimate()
+                N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 1, *blk, far_n, S.cuda_stream)
                 S.wait_event(mapped)
                 if self._hydro is not None:
                     self._hydro.zero_()
-                N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 2, *blk, S.cuda_stream)
+                N.call("lbdem_psc_step_phase", lat, psc, grains, src, 1 - src, 2, *blk, near_n, S.cuda_stream)
                 self._cur, self._cur_kind, self._collided = 1 - src, "fpc", None
         finally:
             d.sync = sync
