@@ -50,13 +50,15 @@ sys.path.insert(0, ROOT)
 from lbdem_taichi_b200 import cases  # noqa: E402
 
 METRIC = "MLUPS & HBM-roofline % for D3Q19 PSC step, FP16-store vs FP32 at ≤1e-3 drag err"
-FORMS = ("f32", "f16", "bf16")
-BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}   # 19 reads + 19 writes of the storage type
+# storage forms: population storage, and "f32-lag16" = FP32 populations with
+# the lagged Smagorinsky state in FP16 (cases.split_form)
+FORMS = ("f32", "f16", "bf16", "f32-lag16")
+BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76, "f32-lag16": 152}   # 19 reads + 19 writes of the storage type
 # DRAM read + write per cell of one step-kernel launch: ncu dram__bytes_read.sum
 # + dram__bytes_write.sum of a launch on the 192^3 dense suspension (844
 # spheres, the same solid fraction), divided by its cells; populations 1.08 GB
 # (FP32) / 0.54 GB (16-bit), both beyond the 126 MB L2
-TRAFFIC_PER_CELL = {"f32": 192.4, "f16": 98.5, "bf16": 98.5}
+TRAFFIC_PER_CELL = {"f32": 188.4, "f16": 98.9, "bf16": 98.0, "f32-lag16": 169.0}
 FIXTURE = os.path.join(ROOT, "tests", "golden", "c2_fp64.npz")
 
 
@@ -204,7 +206,7 @@ def measure_form(c, storage, inputs, args, world, clk, barrier):
     dem.check_status()
     # inputs larger than L2 several times over need no flush; otherwise a
     # 256 MB buffer is rewritten between steps (outside the per-step events)
-    pop_gb = 2 * 19 * cells * (4 if storage == "f32" else 2) / 1e9
+    pop_gb = 2 * 19 * cells * (4 if cases.split_form(storage)[0] == "f32" else 2) / 1e9
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda") if pop_gb <= 0.5 else None
     mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     ev_step = [(mk(), mk()) for _ in range(args.steps)]
@@ -272,12 +274,14 @@ def measure_form(c, storage, inputs, args, world, clk, barrier):
         "kernel_ms": round(kern_ms, 4),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "kernel": f"lbdem_psc_step_{storage}", "kernel_ms": round(kern_ms, 4),
+                     "kernel": f"lbdem_psc_step_{cases.split_form(storage)[0]}", "kernel_ms": round(kern_ms, 4),
                      "bytes_per_cell": bpc,
-                     "traffic": round(TRAFFIC_PER_CELL[storage] * cells / 1e9, 4),
-                     "traffic_per_cell": TRAFFIC_PER_CELL[storage],
+                     "traffic": round(TRAFFIC_PER_CELL[storage] * cells / 1e9, 4) if storage in TRAFFIC_PER_CELL
+                     else None,
+                     "traffic_per_cell": TRAFFIC_PER_CELL.get(storage),
                      "traffic_unit": "GB per launch (ncu DRAM read+write per cell of a 192^3 launch x cells)",
-                     "traffic_over_algorithmic": round(TRAFFIC_PER_CELL[storage] / bpc, 3)},
+                     "traffic_over_algorithmic": (round(TRAFFIC_PER_CELL[storage] / bpc, 3)
+                                                  if storage in TRAFFIC_PER_CELL else None)},
         "phases_ms": {"map+step": round(lbm_ms, 4), "step_kernel": round(kern_ms, 4),
                       f"dem_{sub}_substeps": round(dem_ms, 4), "host_launch_per_step": round(cpu_launch_ms, 4)},
         "gpu_launches": launches,

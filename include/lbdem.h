@@ -64,7 +64,7 @@
 extern "C" {
 #endif
 
-#define LBDEM_ABI_VERSION 3
+#define LBDEM_ABI_VERSION 4
 
 /* return codes */
 #define LBDEM_OK 0
@@ -126,7 +126,7 @@ typedef struct lbdem_lattice {
     float *rho;            /* Ncells, FP32 (moments; also the initial state) */
     float *vel;            /* 3*Ncells, FP32 SoA (ux | uy | uz) */
     void *aux;             /* lagged state (drho, u, omega) of the last collision, 5*32*NB*Ny*Nz of the
-                              storage type (blocked): required by LBDEM_SMAG_REFERENCE and by
+                              storage type, or FP16 with aux_half (blocked): required by LBDEM_SMAG_REFERENCE and by
                               lbdem_stress, NULL otherwise (then the step neither reads nor writes it) */
     const uint32_t *links; /* per-cell link mask from lbdem_build_links */
     int32_t *status;       /* device status word */
@@ -160,6 +160,11 @@ typedef struct lbdem_lattice {
                                    walls or special cells, all FLUID: the mask lbdem_build_links gives
                                    is then LBDEM_LINK_FLUID everywhere); the step kernels then read no
                                    per-cell masks.  0: read links[]. */
+    int32_t aux_half;           /* 1: aux holds FP16 elements under FP32 storage -- the lagged state at
+                                   half the bytes (20 B per cell less traffic for the step with
+                                   LBDEM_SMAG_REFERENCE), rounded to FP16 between steps; no counterpart
+                                   in the reference, whose lagged state is FP32.  0: aux has the storage
+                                   type.  Must be 0 for the 16-bit storage forms. */
 } lbdem_lattice;
 
 typedef struct lbdem_grains {
@@ -270,6 +275,18 @@ int lbdem_boundary_cells(const uint32_t *links, int32_t nx, int32_t ny, int32_t 
 int lbdem_lattice_init(const lbdem_lattice *L, int32_t buf, void *stream);
 
 int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G, void *stream);
+
+/* Clear, ahead of the next lbdem_psc_map, the owner keys that the previous
+ * exact map claimed (the cells within each particle's previous mapping reach,
+ * from P->prev), and set P->have_prev = 0 so that the next map claims on clear
+ * keys without a clearing pass of its own (and does not reuse the previous
+ * map).  It reads only P->prev and writes only the keys, so it may run on
+ * another stream beside the DEM sub-steps once the last reader of the keys
+ * (the step, lbdem_psc_decode) is done; the next map must be ordered after
+ * it.  No counterpart in the reference, which rebuilds its fields every step.
+ * Not with P->disp_limit > 0 (pipelined stepping checks displacements in the
+ * map's own clearing pass): LBDEM_ERR_UNSUPPORTED. */
+int lbdem_psc_map_clear(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G, void *stream);
 
 /* One fused pass: [stream of the pending post-collision populations in
  * f[src] (gather=1) | read populations in place (gather=0)] -> moments ->

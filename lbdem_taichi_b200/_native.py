@@ -17,7 +17,7 @@ ST_NAN, ST_RHO, ST_VELMAX = 1, 2, 4
 ST_CONTACT_OVERFLOW, ST_GRID_OVERFLOW, ST_GID_OVERFLOW, ST_CELL_OVERFLOW = 8, 16, 32, 64
 ST_WAIT_TIMEOUT = 128
 ST_PIPELINE_MARGIN = 256
-ABI_VERSION = 3        # LBDEM_ABI_VERSION of include/lbdem.h
+ABI_VERSION = 4        # LBDEM_ABI_VERSION of include/lbdem.h
 F32, F16, BF16 = 0, 1, 2
 LINK_FLUID = 1 << 20   # LBDEM_LINK_FLUID: the link mask of every cell of an all-FLUID lattice
 SMAG_OFF, SMAG_REFERENCE, SMAG_LOCAL = 0, 1, 2
@@ -45,7 +45,8 @@ class Lattice(C.Structure):
                 ("force_on", C.c_int32), ("force", C.c_float * 3), ("scale16", C.c_float),
                 ("f", vp * 2), ("rho", vp), ("vel", vp), ("aux", vp), ("links", vp),
                 ("status", vp), ("moving", vp), ("ct", vp), ("bnd_cells", vp), ("bnd_na", C.c_uint32),
-                ("bnd_nb", C.c_uint32), ("bnd_f0", vp), ("bnd_slip", C.c_int32), ("stress", vp), ("links_all", C.c_uint32)]
+                ("bnd_nb", C.c_uint32), ("bnd_f0", vp), ("bnd_slip", C.c_int32), ("stress", vp), ("links_all", C.c_uint32),
+                ("aux_half", C.c_int32)]
 
 
 class Grains(C.Structure):
@@ -104,6 +105,7 @@ EXPORTS = {
     "lbdem_boundary_cells": ([vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_uint32, vp, vp, vp], C.c_int),
     "lbdem_psc_near_blocks": ([vp, vp, vp, C.c_double, vp, vp, vp, vp], C.c_int),
     "lbdem_psc_step_phase": ([vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_uint32, vp], C.c_int),
+    "lbdem_psc_map_clear": ([vp, vp, vp, vp], C.c_int),
 }
 
 _lib = None
@@ -114,7 +116,8 @@ KERNELS_PER_CALL = {"lbdem_build_links": 1, "lbdem_lattice_init": 1, "lbdem_psc_
                     "lbdem_stream_moments": 1, "lbdem_psc_decode": 1, "lbdem_dem_bin": 1,
                     "lbdem_global_sums_f64": 2, "lbdem_global_sums_f64_noalloc": 2,
                     "lbdem_psc_map_smooth": 3, "lbdem_stress": 1, "lbdem_psc_step_adjoint_f32": 1, "lbdem_psc_force_adjoint": 1,
-                    "lbdem_boundary_cells": 3, "lbdem_psc_near_blocks": 4, "lbdem_psc_step_phase": 1}
+                    "lbdem_boundary_cells": 3, "lbdem_psc_near_blocks": 4, "lbdem_psc_step_phase": 1,
+                    "lbdem_psc_map_clear": 1}
 # calls followed by the boundary pass: one more kernel per non-empty phase
 _BOUNDARY_CALLS = ("lbdem_psc_step_f32", "lbdem_psc_step_f16", "lbdem_psc_step_bf16", "lbdem_stream_moments")
 _launches = [0]

@@ -204,8 +204,18 @@ def make_dem(domain, dt, gravity, contact, radius, mass, pos, vel, omega=None, p
     return dem
 
 
+def split_form(form: str):
+    """(storage, lagged_storage) of a storage-form name: "f32", "f16", "bf16",
+    or "f32-lag16" (FP32 populations, FP16 lagged Smagorinsky state)."""
+    if form == "f32-lag16":
+        return "f32", "f16"
+    return form, None
+
+
 def build(c: dict, storage: str, pos, rad, vel, mass):
-    """(PSCLattice3D, DEMSolver) of case `c`, initialised, in `storage`."""
+    """(PSCLattice3D, DEMSolver) of case `c`, initialised, in storage form
+    `storage` (``split_form``)."""
+    storage, lagged = split_form(storage)
     from .dem3d.demconfig import HertzContactConfig, LinearContactConfig
     from .lbdem.psclattice3d import PSCLattice3D
     nx, ny, nz = c["shape"]
@@ -218,7 +228,7 @@ def build(c: dict, storage: str, pos, rad, vel, mass):
                    freeze=np.ones(len(rad), np.int32) if opened else None)
     lat = PSCLattice3D(nx, ny, nz, 1.0 / c["tau"], 1.0, 1.0, 1.0, dem,
                        smagorinsky="off" if c["cs"] is None else "reference", body_force=c["fluid_force"],
-                       storage=storage)
+                       storage=storage, lagged_storage=lagged)
     if c["cs"] is not None:
         lat.SmagorinskyConstant = c["cs"]
     if c["walls_z"] or opened:

@@ -86,7 +86,34 @@ struct StepArgs {
     float *stress_out;              // 7 planes of Ncells: stress of the gathered state (fused output), or NULL
     uint32_t links_all;             // nonzero: the link mask of every cell (no per-cell masks are read)
     uint32_t lbase;                 // listed launches: index of the first list entry of this launch
+    int aux16;                      // FP32 storage with the lagged state in FP16 (aux is __half)
 };
+
+// Lagged-state element idx of aux (the blocked offsets do not depend on the
+// element width): the storage type, or FP16 under FP32 storage with aux16.
+// LAGM: the width as a template argument (LAG_STORE: the storage type,
+// LAG_HALF: FP16; the fused step's own instantiations) or read from a.aux16
+// (LAG_RUNTIME: every other kernel).
+constexpr int LAG_STORE = 0, LAG_HALF = 1, LAG_RUNTIME = 2;
+// Element `base + off` (off a compile-time constant at the call sites, so it
+// folds into the address).
+template <typename T, int LAGM = LAG_RUNTIME>
+__device__ __forceinline__ float lag_ld(const StepArgs &a, uint32_t base, uint32_t off) {
+    if constexpr (sizeof(T) == 4 && LAGM != LAG_STORE) {
+        if (LAGM == LAG_HALF || a.aux16) return __half2float((static_cast<const __half *>(a.aux) + base)[off]);
+    }
+    return aux_dec<T>((static_cast<const T *>(a.aux) + base)[off]);
+}
+template <typename T, int LAGM = LAG_RUNTIME>
+__device__ __forceinline__ void lag_st(const StepArgs &a, uint32_t base, uint32_t off, float v) {
+    if constexpr (sizeof(T) == 4 && LAGM != LAG_STORE) {
+        if (LAGM == LAG_HALF || a.aux16) {
+            (static_cast<__half *>(a.aux) + base)[off] = __float2half_rn(v);
+            return;
+        }
+    }
+    (static_cast<T *>(a.aux) + base)[off] = aux_enc<T>(v);
+}
 
 // Pull streaming (lbm_solver3d.py:207-236 for FLUID and OBSTACLE neighbours;
 // periodic wrap as compute_neigh_index :308-342) is inlined in the kernels.
@@ -566,7 +593,7 @@ __device__ __forceinline__ void write_stress(const StepArgs &a, const float h[Q]
 // its own loads and the one that stages rows in shared memory.
 // psc_given: the collision form when the caller has decided it (0 BGK, 1
 // PSC); -1: PSC when any cell of the warp is owned (a warp is one x-block).
-template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS, bool PACK_PSC = false>
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS, bool PACK_PSC = false, int LAGM = LAG_RUNTIME>
 __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z, bool inb, uint32_t cell,
                                           uint32_t own, uint32_t aown, T raw[Q], float aux[5], uint32_t key,
                                           uint32_t lk, int psc_given = -1) {
@@ -611,9 +638,8 @@ __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z
 #pragma unroll
         for (int q = 0; q < Q; ++q) d[q * 32] = Store<T>::narrow(h[q]);
         if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
-            T *ap = static_cast<T *>(a.aux) + aown;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+            for (int k = 0; k < 5; ++k) lag_st<T, LAGM>(a, aown, k * 32, aux[k]);
         }
         if (a.hydro_out) {
             a.hydro_out[cell] = cf[0].hx;
@@ -626,7 +652,7 @@ __device__ __forceinline__ void step_cell(const StepArgs &a, int x, int y, int z
 
 // The fused step of the cell (x, y, z) of this thread: gathers, lagged state,
 // key and link mask, then step_cell.
-template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS>
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool STRESS, int LAGM = LAG_RUNTIME>
 __device__ __forceinline__ void step_at(const StepArgs &a, int x, int y, int z) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const bool inb = (x < nx) && (y < ny);
@@ -667,23 +693,24 @@ __device__ __forceinline__ void step_at(const StepArgs &a, int x, int y, int z) 
     float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
     const uint32_t aown = row * a.ars + xslot((uint32_t)xc_, AB);
     if (SMAG == LBDEM_SMAG_REFERENCE || STRESS) {
-        const T *ap = static_cast<const T *>(a.aux) + aown;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ap[k * 32]);
+        for (int k = 0; k < 5; ++k) aux[k] = lag_ld<T, LAGM>(a, aown, k * 32);
     }
     uint32_t key = (a.key != nullptr) ? a.key[cell] : 0u;
     // the link mask is read for every cell (a flag that skipped this load for
     // plain blocks cost more -- a dependent load before it -- than the 4 B it
     // saved), unless one value holds for the whole lattice (kernel argument)
     const uint32_t lk = a.links_all ? a.links_all : a.links[cell];
-    step_cell<T, GATHER, SMAG, WRAP, STRESS>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
+    step_cell<T, GATHER, SMAG, WRAP, STRESS, false, LAGM>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
 }
 
 // LISTED (pipelined stepping): one-dimensional blocks whose warps take the
 // x-blocks of a compact list (blist / bcount), so every warp of a CTA has
 // work; otherwise the grid covers the lattice.  A warp is one x-block.
 // STRESS: also write the stress diagnostics of the gathered state (a.stress_out).
-template <typename T, bool GATHER, int SMAG, bool WRAP, bool LISTED = false, bool STRESS = false>
+// LAGM: the lagged state's width (LAG_STORE / LAG_HALF fixed, or LAG_RUNTIME).
+template <typename T, bool GATHER, int SMAG, bool WRAP, bool LISTED = false, bool STRESS = false,
+          int LAGM = LAG_RUNTIME>
 __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const StepArgs a) {
     int x, y, z;
     if constexpr (LISTED) {
@@ -699,19 +726,19 @@ __global__ void __launch_bounds__(ONE_THREADS, ONE_MIN_BLOCKS) k_psc_step(const 
         y = blockIdx.y * blockDim.y + threadIdx.y;
         z = blockIdx.z;
     }
-    step_at<T, GATHER, SMAG, WRAP, STRESS>(a, x, y, z);
+    step_at<T, GATHER, SMAG, WRAP, STRESS, LAGM>(a, x, y, z);
 }
 
 // The list entries beyond those a listed launch of k_psc_step covered (from
 // a.lbase), a warp per entry, striding by the grid's warps: a launch sized
 // from an earlier step's list length leaves none or a few for this one.
-template <typename T, int SMAG>
+template <typename T, int SMAG, int LAGM>
 __global__ void __launch_bounds__(ONE_THREADS) k_psc_step_listed_rest(const StepArgs a) {
     const uint32_t n = *a.bcount;
     const uint32_t stride = gridDim.x * (blockDim.x >> 5);
     for (uint32_t w = a.lbase + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n; w += stride) {
         const uint32_t e = a.blist[a.bfrom_end ? a.nblocks - n + w : w];
-        step_at<T, true, SMAG, false, false>(a, (int)((e & 0xFFu) * 32u + (threadIdx.x & 31u)),
+        step_at<T, true, SMAG, false, false, LAGM>(a, (int)((e & 0xFFu) * 32u + (threadIdx.x & 31u)),
                                              (int)((e >> 8) & 0xFFFu), (int)(e >> 20));
     }
 }
@@ -928,7 +955,7 @@ __global__ void __launch_bounds__(ROW_THREADS + 32, ROW_MIN_BLOCKS) k_psc_step_r
         if ((threadIdx.x & 31u) == 0) mbar_arrive(smem_u32(&empty[st]));
         const uint32_t own = (uint32_t)r * a.rs + xslot((uint32_t)xc, QB);
         const uint32_t aown = (uint32_t)r * a.ars + xslot((uint32_t)xc, AB);
-        step_cell<T, true, SMAG, WRAP, false, true>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
+        step_cell<T, true, SMAG, WRAP, false, true, LAG_STORE>(a, x, y, z, inb, cell, own, aown, raw, aux, key, lk);
     }
 }
 
@@ -1151,7 +1178,7 @@ __global__ void __launch_bounds__(ROW_THREADS / 2 + 32, ROW2_MIN_BLOCKS) k_psc_s
                 const uint32_t cl = (uint32_t)r * (uint32_t)nx + (uint32_t)xx;
                 const uint32_t own = (uint32_t)r * a.rs + xslot((uint32_t)xx, QB);
                 const uint32_t aown = (uint32_t)r * a.ars + xslot((uint32_t)xx, AB);
-                step_cell<T, true, SMAG, WRAP, false>(a, x, y, z, inb, cl, own, aown, raw, aux, c ? key1 : key0,
+                step_cell<T, true, SMAG, WRAP, false, false, LAG_STORE>(a, x, y, z, inb, cl, own, aown, raw, aux, c ? key1 : key0,
                                                       c ? lk1 : lk0, psc_block);
             }
         }
@@ -1388,9 +1415,8 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
     float u[3] = {a.vel[cell], a.vel[nc + cell], a.vel[2 * nc + cell]};
     float aux[5] = {0.f, 0.f, 0.f, 0.f, a.omega0};
     if (a.aux != nullptr) {
-        const T *ap = static_cast<const T *>(a.aux) + aown;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) aux[k] = aux_dec<T>(ap[k * 32]);
+        for (int k = 0; k < 5; ++k) aux[k] = lag_ld<T>(a, aown, k * 32);
     }
     // interior neighbour of a face cell (no periodic wrap, lbm_solver3d.py:522-527, 647-658)
     int ax = 0, s = 0;
@@ -1490,9 +1516,8 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
 #pragma unroll
             for (int q = 0; q < Q; ++q) dst[own + q * 32] = Store<T>::narrow(h[q]);
             if (rule == WET_EXIT && a.aux != nullptr) {
-                T *ap = static_cast<T *>(a.aux) + aown;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+                for (int k = 0; k < 4; ++k) lag_st<T>(a, aown, k * 32, aux[k]);
             }
         }
         return;
@@ -1517,9 +1542,8 @@ __global__ void __launch_bounds__(128) k_boundary(const StepArgs a, const uint32
     }
     if (act) {
         if (SMAG == LBDEM_SMAG_REFERENCE || a.keep_lag) {
-            T *ap = static_cast<T *>(a.aux) + aown;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) ap[k * 32] = aux_enc<T>(aux[k]);
+            for (int k = 0; k < 5; ++k) lag_st<T>(a, aown, k * 32, aux[k]);
         }
         if (a.hydro_out) {
             a.hydro_out[cell] = cf[0].hx;
@@ -1564,12 +1588,12 @@ __global__ void k_init(const StepArgs a, const float *rho_in, const float *vel_i
         }
     }
     if (smag_ref) {
-        T *ax = static_cast<T *>(a.aux) + (row * a.ars + xslot((uint32_t)x, AB));
-        ax[0] = aux_enc<T>(drho);
-        ax[32] = aux_enc<T>(ux);
-        ax[64] = aux_enc<T>(uy);
-        ax[96] = aux_enc<T>(uz);
-        ax[128] = aux_enc<T>(a.omega0);
+        const uint32_t ax = row * a.ars + xslot((uint32_t)x, AB);
+        lag_st<T>(a, ax, 0, drho);
+        lag_st<T>(a, ax, 32, ux);
+        lag_st<T>(a, ax, 64, uy);
+        lag_st<T>(a, ax, 96, uz);
+        lag_st<T>(a, ax, 128, a.omega0);
     }
 }
 
@@ -1652,8 +1676,7 @@ __global__ void k_decode(const StepArgs a, int smag_ref, int32_t *id, float *vol
     const int gid = (int)key_gid(key);
     const float eps = a.eps ? a.eps[c] : ((key & KEY_FULL) ? 1.f : (float)key_count(key) * (1.f / 125.f));
     const uint32_t row = (uint32_t)(c / (size_t)a.nx), xx = (uint32_t)(c % (size_t)a.nx);
-    const float om = smag_ref ? aux_dec<T>(static_cast<const T *>(a.aux)[row * a.ars + xslot(xx, AB) + 4 * 32])
-                              : a.omega0;
+    const float om = smag_ref ? lag_ld<T>(a, row * a.ars + xslot(xx, AB), 4 * 32) : a.omega0;
     const float taum = 1.f / om - 0.5f;
     id[c] = gid;
     volfrac[c] = eps;
@@ -1739,9 +1762,9 @@ __global__ void __launch_bounds__(256) k_stress(const StepArgs a, float *out) {
         if (cx(q) * cz(q)) sxz += (float)(cx(q) * cz(q)) * d;
         if (cy(q) * cz(q)) syz += (float)(cy(q) * cz(q)) * d;
     }
-    const T *ap = static_cast<const T *>(a.aux) + (row * a.ars + xslot((uint32_t)x, AB));
-    const float dr = aux_dec<T>(ap[0]), ux = aux_dec<T>(ap[32]), uy = aux_dec<T>(ap[64]), uz = aux_dec<T>(ap[96]);
-    const float om = aux_dec<T>(ap[128]);
+    const uint32_t ap = row * a.ars + xslot((uint32_t)x, AB);
+    const float dr = lag_ld<T>(a, ap, 0), ux = lag_ld<T>(a, ap, 32), uy = lag_ld<T>(a, ap, 64), uz = lag_ld<T>(a, ap, 96);
+    const float om = lag_ld<T>(a, ap, 128);
     const float rho = 1.f + dr, ecs = dr * CS2;
     const float k = -(1.f - 0.5f * om);
     const size_t nc = a.nc;
@@ -1871,6 +1894,15 @@ static int fill_args(const lbdem_lattice *L, StepArgs &a) {
     }
     a.aux = L->aux;
     a.keep_lag = L->aux != nullptr;
+    if (L->aux_half != 0 && L->aux_half != 1) {
+        set_error("aux_half must be 0 or 1");
+        return LBDEM_ERR_ARG;
+    }
+    if (L->aux_half && L->storage != LBDEM_F32) {
+        set_error("aux_half applies to FP32 storage (the 16-bit forms keep the lagged state in their own type)");
+        return LBDEM_ERR_ARG;
+    }
+    a.aux16 = L->aux_half;
     a.links = L->links;
     a.links_all = L->links_all;
     a.moving = L->moving;
@@ -2004,6 +2036,8 @@ static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStrea
     // two cells per thread: 16-bit storage, even Nx, and an even number of x-blocks so that the 16 NB
     // consumer threads are whole warps (the producer warp then starts on a warp boundary)
     if (PAIRS && (sizeof(T) != 2 || (a.nx & 1) || (a.nb & 1u))) return ROWS_NOT_APPLICABLE;
+    // the staged lagged-state rows and the stores have the storage type
+    if (a.aux16) return ROWS_NOT_APPLICABLE;
     const uint32_t es = sizeof(T), nb = a.nb;
     RowMaps m;
     memset(&m, 0, sizeof(m));
@@ -2111,6 +2145,8 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
     }
     dim3 grid, block;
     step_geometry(L, grid, block, ONE_THREADS);
+    // FP16 lagged state exists under FP32 storage only (fill_args checks)
+    constexpr int LAG_H = sizeof(T) == 4 ? LAG_HALF : LAG_STORE;
 #define LBDEM_STEP_CASE(G_, S_)                                                          \
     do {                                                                                 \
         const int form_ = step_kernel_form<T>();                                         \
@@ -2131,10 +2167,13 @@ static int launch_step(const lbdem_lattice *L, const lbdem_psc *P, const lbdem_g
         if (a.stress_out) {                                                              \
             if (a.wrap_any) k_psc_step<T, G_, S_, true, false, true><<<grid, block, 0, st>>>(a);  \
             else k_psc_step<T, G_, S_, false, false, true><<<grid, block, 0, st>>>(a);           \
+        } else if (a.aux16) {                                                            \
+            if (a.wrap_any) k_psc_step<T, G_, S_, true, false, false, LAG_H><<<grid, block, 0, st>>>(a);  \
+            else k_psc_step<T, G_, S_, false, false, false, LAG_H><<<grid, block, 0, st>>>(a);           \
         } else if (a.wrap_any) {                                                         \
-            k_psc_step<T, G_, S_, true><<<grid, block, 0, st>>>(a);                      \
+            k_psc_step<T, G_, S_, true, false, false, LAG_STORE><<<grid, block, 0, st>>>(a); \
         } else {                                                                         \
-            k_psc_step<T, G_, S_, false><<<grid, block, 0, st>>>(a);                     \
+            k_psc_step<T, G_, S_, false, false, false, LAG_STORE><<<grid, block, 0, st>>>(a); \
         }                                                                                \
         launch_boundary<T, S_, G_ ? BND_GATHER : BND_LOCAL>(L, a, st);                   \
     } while (0)
@@ -2211,19 +2250,26 @@ static int launch_step_phase(const lbdem_lattice *L, const lbdem_psc *P, const l
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     }
-#define LBDEM_PHASE_CASE(S_)                                                              \
+    constexpr int LAG_H = sizeof(T) == 4 ? LAG_HALF : LAG_STORE;
+#define LBDEM_PHASE_CASE(S_, M_)                                                          \
     do {                                                                                  \
-        k_psc_step<T, true, S_, false, true><<<grid, block, 0, st>>>(a);                  \
+        k_psc_step<T, true, S_, false, true, false, M_><<<grid, block, 0, st>>>(a);       \
         if (sized) {                                                                      \
             StepArgs r = a;                                                               \
             r.lbase = grid.x * wpb;                                                       \
-            k_psc_step_listed_rest<T, S_><<<nsm, ONE_THREADS, 0, st>>>(r);                \
+            k_psc_step_listed_rest<T, S_, M_><<<nsm, ONE_THREADS, 0, st>>>(r);            \
         }                                                                                 \
         if (phase == 2) launch_boundary<T, S_, BND_GATHER>(L, a, st);                     \
     } while (0)
-    if (L->smag_mode == LBDEM_SMAG_OFF) LBDEM_PHASE_CASE(LBDEM_SMAG_OFF);
-    else if (L->smag_mode == LBDEM_SMAG_REFERENCE) LBDEM_PHASE_CASE(LBDEM_SMAG_REFERENCE);
-    else LBDEM_PHASE_CASE(LBDEM_SMAG_LOCAL);
+#define LBDEM_PHASE_LAG(S_)                                                               \
+    do {                                                                                  \
+        if (a.aux16) LBDEM_PHASE_CASE(S_, LAG_H);                                         \
+        else LBDEM_PHASE_CASE(S_, LAG_STORE);                                             \
+    } while (0)
+    if (L->smag_mode == LBDEM_SMAG_OFF) LBDEM_PHASE_LAG(LBDEM_SMAG_OFF);
+    else if (L->smag_mode == LBDEM_SMAG_REFERENCE) LBDEM_PHASE_LAG(LBDEM_SMAG_REFERENCE);
+    else LBDEM_PHASE_LAG(LBDEM_SMAG_LOCAL);
+#undef LBDEM_PHASE_LAG
 #undef LBDEM_PHASE_CASE
     return check_launch("psc_step_phase");
 }

@@ -18,6 +18,7 @@ namespace lbdem {
 
 struct MapArgs {
     int n, nx, ny, nz;
+    int keys_only;           // the clearing pass zeroes the previous map's keys only (no table, no force reset)
     double dx, dt, xmin, ymin, zmin;
     const double *pos, *radius, *vel, *omega;
     const uint32_t *links;
@@ -36,6 +37,9 @@ struct MapArgs {
 };
 
 constexpr double HALF_DIAG = 0.8660254037844386;  // 0.5 * sqrt(3.0), psclattice3d.py:111
+// Largest distance of a 5^3 sub-point (offsets -0.4 .. 0.4 per axis,
+// psclattice3d.py:121-128) from its cell centre, 0.4 sqrt(3), rounded up.
+constexpr double SUB_REACH = 0.6928204;
 
 __device__ __forceinline__ void particle_lattice(const MapArgs &a, int g, double &xc, double &yc, double &zc,
                                                  double &r) {
@@ -121,7 +125,7 @@ __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
             }
         }
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !a.keys_only) {
         for (int t = 0; t < 3; ++t) a.ff[3 * g + t] = a.mf[3 * g + t] = 0.0;
         double xc, yc, zc, r;
         particle_lattice(a, g, xc, yc, zc, r);
@@ -154,7 +158,10 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
 //  1. each thread classifies one cell -- outside / fully covered / partial
 //     (psclattice3d.py:108-113).  FP32 with a safety margin decides the clear
 //     cases; the exact FP64 comparisons run only for cells near a threshold.
-//     Full covers are claimed at once; partial cells go to a shared list.
+//     Full covers are claimed at once, and so are partial cells whose 125
+//     sub-points all lie inside the sphere; partial cells with sub-points on
+//     both sides of the surface go to a shared list (those with none inside
+//     are dropped).
 //  2. one thread per partial cell counts its 5^3 sub-points
 //     (psclattice3d.py:121-131) from the squared per-axis offsets; the few
 //     cells with a sub-point near the surface are recounted one warp per
@@ -202,6 +209,12 @@ __global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs
         const float in2 = t_in > 0.0 ? (float)(t_in * t_in) : -1.f, marg_i = (float)(1e-4 * (1.0 + t_in * t_in));
         const double rr = r > 0.0 ? r * r : 0.0;
         const float band = (float)(1e-4 * (1.0 + rr));
+        // sub-points lie within SUB_REACH of their cell centre: a partial cell
+        // whose centre is within r - SUB_REACH counts all 125, one beyond
+        // r + SUB_REACH none (FP32 with the same kind of margin)
+        const double t_all = r - SUB_REACH, t_none = r + SUB_REACH;
+        const float all2 = t_all > 0.0 ? (float)(t_all * t_all) : -1.f, marg_a = (float)(1e-4 * (1.0 + t_all * t_all));
+        const float none2 = (float)(t_none * t_none), marg_n = (float)(1e-4 * (1.0 + t_none * t_none));
         const float lo = (float)rr - band, hi = (float)rr + band;
         const unsigned tot = (unsigned)ex * (unsigned)ey * (unsigned)ez;
         // this block's range of the box's cells
@@ -242,7 +255,9 @@ __global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs
                 }
                 if (full) {
                     atomicMax(a.key + c, KEY_FULL | gbits);
-                } else if (r > 0.0) {
+                } else if (r > 0.0 && d2 < all2 - marg_a) {
+                    atomicMax(a.key + c, (125u << 24) | gbits);   // every sub-point inside
+                } else if (r > 0.0 && !(d2 > none2 + marg_n)) {
                     const int slot = atomicAdd(&s_n, 1);
                     s_off[slot] = make_float4(fx, fy, fz, __uint_as_float(c));
                 }
@@ -448,6 +463,7 @@ extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const 
     if (cudaMemsetAsync(scratch, 0, nc * sizeof(uint64_t), st) != cudaSuccess) return check_launch("psc_map_smooth");
     if (G->n > 0) {
         MapArgs a;
+    a.keys_only = 0;
         a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
         a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;
         a.pos = G->pos; a.radius = G->radius; a.vel = G->vel; a.omega = G->omega;
@@ -489,6 +505,7 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
         return LBDEM_ERR_ARG;
     }
     MapArgs a;
+    a.keys_only = 0;
     a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
     a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;
     a.pos = G->pos; a.radius = G->radius; a.vel = G->vel; a.omega = G->omega;
@@ -529,6 +546,35 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     }
     P->have_prev = 1;
     return check_launch("psc_map");
+}
+
+extern "C" int lbdem_psc_map_clear(const lbdem_lattice *L, lbdem_psc *P, const lbdem_grains *G, void *stream) {
+    if (!L || !P || !G || !P->key || !P->prev) {
+        set_error("psc_map_clear: bad arguments");
+        return LBDEM_ERR_ARG;
+    }
+    if (P->disp_limit > 0.0) {
+        set_error("psc_map_clear: pipelined stepping (disp_limit > 0) checks displacements in the map's own clear");
+        return LBDEM_ERR_UNSUPPORTED;
+    }
+    if (G->n <= 0 || !P->have_prev) return LBDEM_OK;
+    MapArgs a;
+    memset(&a, 0, sizeof(a));
+    a.keys_only = 1;
+    a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
+    a.key = P->key;
+    a.prev = P->prev;
+    a.have_prev = 1;
+    a.status = L->status;
+    for (int t = 0; t < 3; ++t) {
+        a.wrap[t] = P->wrap[t] != 0;
+        a.period[t] = P->period[t];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (a.wrap[0] || a.wrap[1] || a.wrap[2]) k_map_clear<true><<<G->n, 128, 0, st>>>(a);
+    else k_map_clear<false><<<G->n, 128, 0, st>>>(a);
+    P->have_prev = 0;
+    return check_launch("psc_map_clear");
 }
 
 // Ordered block lists (ascending ids, so each phase walks memory in order):
@@ -632,6 +678,7 @@ extern "C" int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P,
     cudaStream_t st = (cudaStream_t)stream;
     if (cudaMemsetAsync(near, 0, nblocks, st) != cudaSuccess) return check_launch("near_blocks");
     MapArgs a;
+    a.keys_only = 0;
     memset(&a, 0, sizeof(a));
     a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
     a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;

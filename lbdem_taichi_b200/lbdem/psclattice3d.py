@@ -14,6 +14,10 @@ reference PSC lattice exactly):
                the PSC blend, HybridLattice3D.collide order), or "local"
   body_force   lattice-unit body force added as in ForcedLattice3D (default none)
   storage      "f32" | "f16" | "bf16" population storage (FP32 arithmetic)
+  lagged_storage   "f16" with storage="f32": the lagged Smagorinsky state
+               (drho, u, omega of the previous collision) in FP16 -- 20 B
+               per cell less traffic per step, the lagged values rounded to
+               FP16 between steps (the reference keeps them in FP32)
   keep_hydroforce  also store the per-cell hydrodynamic force field
   stress       keep the lagged state that compute_stress() needs (the reference's
                stress diagnostics, lbm_solver3d.py:347-456)
@@ -38,9 +42,9 @@ from ..lbm3d.lbmutils import CellType  # noqa: F401  (in the module namespace, a
 class PSCLattice3D(LatticeEngine):
     def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, demslover: DEMSolver, *, smagorinsky="off",
                  body_force=None, storage="f32", keep_hydroforce=False, skip_inlet=False,
-                 solid_fraction="exact", stress=False):
+                 solid_fraction="exact", stress=False, lagged_storage=None):
         super().__init__(Nx, Ny, Nz, omega, dx, dt, rho, smagorinsky=smagorinsky, body_force=body_force,
-                         storage=storage, skip_inlet=skip_inlet, stress=stress)
+                         storage=storage, skip_inlet=skip_inlet, stress=stress, lagged_storage=lagged_storage)
         if solid_fraction not in ("exact", "smooth"):
             raise ValueError('solid_fraction must be "exact" or "smooth"')
         self.dem = demslover
@@ -87,6 +91,7 @@ class PSCLattice3D(LatticeEngine):
         self._pipeline_probe = None       # (sequential, pipelined) ms per step of that measurement
         self._near = None
         self._side = None
+        self._clear_stream = None
         if solid_fraction == "smooth":
             self._eps = torch.zeros(nc, dtype=torch.float32, device=dev)
             self._map_scratch = torch.zeros(nc, dtype=torch.int64, device=dev)
@@ -214,26 +219,62 @@ class PSCLattice3D(LatticeEngine):
                     e1.record()
                     e1.synchronize()
                     return e0.elapsed_time(e1)
-                # untimed first: the first launches of the pipelined kernels load their code
+                # untimed first: the first launches of either form's kernels load their code
                 self._run_pipelined(2, sub_cycles)
-                t_seq = timed(lambda: [self.step(sub_cycles) for _ in range(12)]) / 12
+                self._run_sequential(2, sub_cycles)
+                t_seq = timed(lambda: self._run_sequential(12, sub_cycles)) / 12
                 t_pipe = timed(lambda: self._run_pipelined(12, sub_cycles)) / 12
                 self._pipeline_choice = t_pipe < t_seq
                 self._pipeline_probe = (t_seq, t_pipe)
-                n -= 26
+                n -= 28
                 pipeline = self._pipeline_choice
             else:
                 pipeline = bool(self._pipeline_choice)
         if not pipeline or not eligible or n < 2:
-            for _ in range(n):
-                self.step(sub_cycles)
+            self._run_sequential(n, sub_cycles)
             return
         self._run_pipelined(n, sub_cycles)
 
-    def _run_pipelined(self, n: int, sub_cycles: int):
+    def _run_sequential(self, n: int, sub_cycles: int):
+        """step() n times.  Where particles move (so the map cannot be reused),
+        the owner keys of each step's map but the last are cleared on a second
+        stream beside the DEM sub-steps (lbdem_psc_map_clear) instead of by the
+        next map: the step kernel is their last reader, and the next map then
+        claims on clear keys."""
+        early = (n > 1 and self.dem.n > 0 and self.solid_fraction == "exact"
+                 and bool((self.dem._t["freeze"] == 0).any()))
+        if not early:
+            for _ in range(n):
+                self.step(sub_cycles)
+            return
         S = torch.cuda.current_stream()
+        if self._clear_stream is None:
+            self._clear_stream = torch.cuda.Stream()   # default priority: the DEM's blocks are not held back
+        D = self._clear_stream
+        lat, psc, grains = C.byref(self._lat), C.byref(self._psc), C.byref(self._grains)
+        for k in range(n):
+            self.collide()
+            self.stream()
+            stepped = torch.cuda.Event()
+            stepped.record(S)
+            self.dem.run_substeps(sub_cycles)
+            if k < n - 1:
+                with torch.cuda.stream(D):
+                    D.wait_event(stepped)
+                    N.call("lbdem_psc_map_clear", lat, psc, grains, D.cuda_stream)
+                    cleared = torch.cuda.Event()
+                    cleared.record(D)
+                S.wait_event(cleared)
+
+    def _side_stream(self):
         if self._side is None:
             self._side = torch.cuda.Stream(priority=-1)
+        return self._side
+
+    def _run_pipelined(self, n: int, sub_cycles: int):
+        S = torch.cuda.current_stream()
+        if self._near is None:
+            self._side_stream()
             nblk = self.Ny * self.Nz * self._nb
             self._near = torch.zeros(nblk, dtype=torch.uint8, device="cuda")
             # two block lists: the side stream builds the next step's while this step's is in use

@@ -151,10 +151,12 @@ class LatticeEngine:
     SmagorinskyConstant = 0.1
 
     def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, smagorinsky="off", body_force=None,
-                 storage="f32", skip_inlet=True, stress=False):
+                 storage="f32", skip_inlet=True, stress=False, lagged_storage=None):
         N.require_cuda()
         if storage not in _STORAGE:
             raise ValueError(f"storage must be one of {sorted(_STORAGE)}")
+        if lagged_storage not in (None, storage) and (storage, lagged_storage) != ("f32", "f16"):
+            raise ValueError('lagged_storage: "f16" under storage="f32" (or the storage form itself)')
         if smagorinsky not in _SMAG:
             raise ValueError(f"smagorinsky must be one of {sorted(_SMAG)}")
         self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
@@ -179,7 +181,11 @@ class LatticeEngine:
         # lagged state (drho, u, omega) of the last collision: needed by the
         # reference Smagorinsky form and by the stress diagnostics
         self.stress_enabled = bool(stress) or smagorinsky == "reference"
-        self._aux = (torch.zeros((nblk, 5, 32), dtype=tdtype, device=dev) if self.stress_enabled else None)
+        # (FP32 storage may keep it in FP16: lagged_storage="f16", 20 B per cell less step traffic)
+        self._aux_half = lagged_storage == "f16" and storage == "f32"
+        self.lagged_storage = "f16" if self._aux_half else storage
+        self._aux = (torch.zeros((nblk, 5, 32), dtype=torch.float16 if self._aux_half else tdtype, device=dev)
+                     if self.stress_enabled else None)
         self._stress = None
         self._stress_pending = False   # compute_stress() not evaluated yet (fused into the next collide)
         self._links_all = N.LINK_FLUID   # cell types start as FLUID everywhere: one link mask
@@ -236,6 +242,7 @@ class LatticeEngine:
         L.f[0], L.f[1] = N.ptr(self._f[0]), N.ptr(self._f[1])
         L.rho, L.vel = N.ptr(self._rho), N.ptr(self._vel)
         L.aux = N.ptr(self._aux)
+        L.aux_half = int(self._aux_half)
         L.links = N.ptr(self._links)
         L.links_all = self._links_all    # one mask for every cell (all FLUID), else 0
         L.status = N.ptr(self._status)
@@ -449,6 +456,7 @@ class LatticeEngine:
         self._sync_inputs()
         buf = self._materialize()
         d = {"shape": (self.Nx, self.Ny, self.Nz), "storage": self.storage, "smagorinsky": self.smagorinsky,
+             "lagged_storage": self.lagged_storage,
              "omega0": self.omega0, "f": self._f[buf].detach().cpu().clone(),
              "rho": self._rho.detach().cpu().clone(), "vel": self._vel.detach().cpu().clone()}
         if self._aux is not None:
@@ -555,9 +563,10 @@ class BasicLattice3D(LatticeEngine):
     """BGK + Smagorinsky lattice (BasicLattice3D.collide, lbm_solver3d.py:176-192:
     computeOmega with the previous step's feq and omega, then BGK)."""
 
-    def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, storage="f32", smagorinsky="reference", stress=False):
+    def __init__(self, Nx, Ny, Nz, omega, dx, dt, rho, *, storage="f32", smagorinsky="reference", stress=False,
+                 lagged_storage=None):
         super().__init__(Nx, Ny, Nz, omega, dx, dt, rho, smagorinsky=smagorinsky, storage=storage,
-                         skip_inlet=True, stress=stress)
+                         skip_inlet=True, stress=stress, lagged_storage=lagged_storage)
 
 
 class ForcedLattice3D(LatticeEngine):

@@ -29,7 +29,7 @@ def test_every_declared_function_is_exported():
     assert not missing, missing
     # every declared function has a ctypes signature in the bindings, and vice versa
     assert set(names) == set(N.EXPORTS), set(names) ^ set(N.EXPORTS)
-    assert lib.lbdem_abi_version() == N.ABI_VERSION == 3
+    assert lib.lbdem_abi_version() == N.ABI_VERSION == 4
 
 
 def test_host_side_argument_checks():

@@ -106,3 +106,22 @@ def test_particle_beyond_the_margin_is_flagged():
     lat.run(3, 10, pipeline=True)
     assert int(lat._status.item()) & N.ST_PIPELINE_MARGIN
     lat.clear_status()
+
+
+@pytest.mark.parametrize("storage,ftol", [("f32", 1e-6), ("f16", 1e-5 * 4096)])
+def test_sequential_run_with_early_key_clear(storage, ftol):
+    """run(pipeline=False) clears each map's keys beside the DEM
+    (lbdem_psc_map_clear) rather than in the next map: the same as step() n
+    times, and the last map's keys stay for the fields read after it."""
+    a = _suspension(storage)
+    b = _suspension(storage)
+    a[0].run(12, 10, pipeline=False)
+    for _ in range(12):
+        b[0].step(10)
+    _compare(a, b, ftol)
+    assert a[0]._psc.have_prev == 1
+    np.testing.assert_array_equal(a[0].volfrac.to_numpy(), b[0].volfrac.to_numpy())
+    assert a[0].volfrac.to_numpy().max() == 1.0
+    for lat, dem in (a, b):
+        lat.check_status()
+        dem.check_status()

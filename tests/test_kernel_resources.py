@@ -54,16 +54,17 @@ def _match(res, pattern):
 
 
 def test_fused_step(res):
-    # k_psc_step<T, GATHER=1, SMAG, WRAP, LISTED=0, STRESS=0>
-    got = _match(res, r"k_psc_stepI(f|6__half|13__nv_bfloat16)Lb1ELi[012]ELb[01]ELb0ELb0E")
-    assert len(got) == 3 * 3 * 2
+    # k_psc_step<T, GATHER=1, SMAG, WRAP, LISTED=0, STRESS=0, LAGM>: the lagged state in the storage
+    # type (LAGM 0) for every form, and in FP16 (LAGM 1) under FP32 storage
+    got = _match(res, r"k_psc_stepI(f|6__half|13__nv_bfloat16)Lb1ELi[012]ELb[01]ELb0ELb0ELi[01]E")
+    assert len(got) == 3 * 3 * 2 + 3 * 2
     bad = {k: v for k, v in got.items() if v[0] > 64 or v[1] > 0}
     assert not bad, bad
 
 
 def test_fused_step_with_stress(res):
-    # k_psc_step<T, GATHER=1, SMAG, WRAP, LISTED=0, STRESS=1>
-    got = _match(res, r"k_psc_stepI(f|6__half|13__nv_bfloat16)Lb1ELi[012]ELb[01]ELb0ELb1E")
+    # k_psc_step<T, GATHER=1, SMAG, WRAP, LISTED=0, STRESS=1, LAGM=2 (width read at run time)>
+    got = _match(res, r"k_psc_stepI(f|6__half|13__nv_bfloat16)Lb1ELi[012]ELb[01]ELb0ELb1ELi2E")
     assert len(got) == 3 * 3 * 2
     bad = {k: v for k, v in got.items() if v[0] > 64 or v[1] > 16}
     assert not bad, bad
