@@ -158,9 +158,22 @@ def _boundary_phases(arg):
     return int(L.bnd_na > 0) + int(L.bnd_nb > 0) if isinstance(L, Lattice) else 0
 
 
+def _map_launches(arg):
+    # lbdem_psc_map skips its clearing pass when there is nothing to clear or check
+    P = getattr(arg, "_obj", None)
+    if P is None or P.have_prev or P.disp_limit > 0.0:
+        return 2
+    return 1
+
+
 def call(name: str, *args):
+    pre = _map_launches(args[1]) if name == "lbdem_psc_map" else None
     rc = getattr(load(), name)(*args)
-    _launches[0] += load().lbdem_dem_launches_last() if name == "lbdem_dem_substeps" else KERNELS_PER_CALL.get(name, 0)
+    if pre is not None:
+        _launches[0] += pre
+    else:
+        _launches[0] += (load().lbdem_dem_launches_last() if name == "lbdem_dem_substeps"
+                         else KERNELS_PER_CALL.get(name, 0))
     if name == "lbdem_psc_step_phase" and args[8]:
         _launches[0] += 1     # a launch sized from an estimate is followed by the one that takes the rest
     if name in _BOUNDARY_CALLS or (name == "lbdem_psc_step_phase" and args[5] == 2):

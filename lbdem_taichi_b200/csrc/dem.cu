@@ -215,11 +215,11 @@ struct PState {
 };
 
 // resolve(i, j) (demsolver.py:638-740); forces on i accumulated in Fi/Mi,
-// forces on j added atomically.  hj/ha: i's first contact slots (partner,
-// active) as they were when the sub-step started (only i's lanes touch i's
-// slots, each for its own partner).
-__device__ __forceinline__ void resolve_pair(const lbdem_dem &d, int i, const PState &P, int n_i, const int *hj,
-                                             const int *ha, int j, double *Fi_acc, double *Mi_acc) {
+// forces on j added atomically.  hk: i's first contact slots (the partner of
+// an active slot, -1 for an inactive one) as they were when the sub-step
+// started (only i's lanes touch i's slots, each for its own partner).
+__device__ __forceinline__ void resolve_pair(const lbdem_dem &d, int i, const PState &P, int n_i, const int *hk,
+                                             int j, double *Fi_acc, double *Mi_acc) {
     const size_t base = (size_t)i * d.maxc;
     // partner state: all loads issued together
     double pj[3], vj[3], wj[3];
@@ -233,7 +233,7 @@ __device__ __forceinline__ void resolve_pair(const lbdem_dem &d, int i, const PS
     const int nreg = min(n_i, min(d.maxc, SLOTS_IN_REGS));
 #pragma unroll
     for (int o = SLOTS_IN_REGS - 1; o >= 0; --o)   // lowest matching slot wins, as a forward search
-        if (o < nreg && hj[o] == j && ha[o]) off = o;
+        if (o < nreg && hk[o] == j) off = o;
     if (off < 0)
         for (int o = SLOTS_IN_REGS; o < n_i && o < d.maxc; ++o)
             if (d.cf_j[base + o] == j && d.cf_active[base + o]) {
@@ -368,12 +368,12 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
         P.mass = d.mass[i];
         const int n_i = d.cfn[i];   // slots in use when the sub-step started
         const size_t base = (size_t)i * d.maxc;
-        int hj[SLOTS_IN_REGS], ha[SLOTS_IN_REGS];
+        int hk[SLOTS_IN_REGS];
 #pragma unroll
         for (int o = 0; o < SLOTS_IN_REGS; ++o) {
             const bool in = o < d.maxc;
-            hj[o] = in ? d.cf_j[base + o] : -1;
-            ha[o] = in ? d.cf_active[base + o] : 0;
+            const int pj = in ? d.cf_j[base + o] : -1, act_o = in ? d.cf_active[base + o] : 0;
+            hk[o] = act_o ? pj : -1;
         }
         const bool wall_lane = k < 6 && !d.wall_periodic[k];
         const int wact = wall_lane ? d.wcf_active[(size_t)i * 6 + k] : 0;
@@ -394,7 +394,7 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
                 const int32_t *lst = d.cell_list + (size_t)c * d.cell_cap;
                 for (int t = 0; t < n; ++t) {
                     const int j = lst[t];
-                    if (j > i) resolve_pair(d, i, P, n_i, hj, ha, j, Fi, Mi);
+                    if (j > i) resolve_pair(d, i, P, n_i, hk, j, Fi, Mi);
                 }
             }
         };
@@ -700,17 +700,20 @@ __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+__device__ __forceinline__ void red_release_gpu(unsigned *p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Arrivals count up monotonically in sync[0] (zeroed before each launch): the
-// k-th barrier is passed when the count reaches k * gridDim.x.  One fence and
-// one atomic per block and barrier (the fence publishes the block's writes of
-// the phase, ordered before thread 0 by the block barrier), then polling with
-// acquire loads; no reset, so no second fence.
+// k-th barrier is passed when the count reaches k * gridDim.x.  One release
+// reduction per block and barrier (after the block barrier, which orders the
+// block's writes of the phase before thread 0, so the release publishes them
+// all), then polling with acquire loads; no reset.
 __device__ __forceinline__ void grid_barrier(uint32_t *sync, unsigned &gen, int32_t *status) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned target = (gen + 1) * gridDim.x;
-        __threadfence();
-        atomicAdd(sync, 1u);
+        red_release_gpu(sync, 1u);
         unsigned it = 0;
         while (ld_acquire_gpu(sync) < target) {
             if (++it > (1u << 22)) {

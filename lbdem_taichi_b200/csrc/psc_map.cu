@@ -19,6 +19,7 @@ namespace lbdem {
 struct MapArgs {
     int n, nx, ny, nz;
     int keys_only;           // the clearing pass zeroes the previous map's keys only (no table, no force reset)
+    int table_in_scatter;    // no clearing pass runs: the scatter writes the table and resets the forces
     double dx, dt, xmin, ymin, zmin;
     const double *pos, *radius, *vel, *omega;
     const uint32_t *links;
@@ -59,6 +60,24 @@ __device__ __forceinline__ int image_shifts(const MapArgs &a, int axis, double c
     if (c - reach < 0.0) { sh[1] = a.period[axis]; return 2; }
     if (c + reach > (double)(n - 1)) { sh[1] = -a.period[axis]; return 2; }
     return 1;
+}
+
+// Particle g's row of the FP32 table the step reads, and its force
+// accumulators reset (one thread).
+__device__ __forceinline__ void particle_table(const MapArgs &a, int g) {
+    for (int t = 0; t < 3; ++t) a.ff[3 * g + t] = a.mf[3 * g + t] = 0.0;
+    double xc, yc, zc, r;
+    particle_lattice(a, g, xc, yc, zc, r);
+    const double fx = floor(xc), fy = floor(yc), fz = floor(zc);
+    // cell-centre offsets are formed as (x - floor) - frac in FP32 (exact
+    // integer part), keeping the lever arm accurate to ~1e-7 lattice units
+    a.table[4 * g + 0] = make_float4((float)fx, (float)fy, (float)fz, 0.f);
+    a.table[4 * g + 1] = make_float4((float)(xc - fx), (float)(yc - fy), (float)(zc - fz), 0.f);
+    const double s = a.dt / a.dx;
+    a.table[4 * g + 2] = make_float4((float)(a.vel[3 * g] * s), (float)(a.vel[3 * g + 1] * s),
+                                     (float)(a.vel[3 * g + 2] * s), 0.f);
+    a.table[4 * g + 3] = make_float4((float)(a.omega[3 * g] * a.dt), (float)(a.omega[3 * g + 1] * a.dt),
+                                     (float)(a.omega[3 * g + 2] * a.dt), 0.f);
 }
 
 // Clear the cells claimed by the previous map (conservative shell), zero the
@@ -125,21 +144,7 @@ __global__ void __launch_bounds__(128) k_map_clear(const MapArgs a) {
             }
         }
     }
-    if (threadIdx.x == 0 && !a.keys_only) {
-        for (int t = 0; t < 3; ++t) a.ff[3 * g + t] = a.mf[3 * g + t] = 0.0;
-        double xc, yc, zc, r;
-        particle_lattice(a, g, xc, yc, zc, r);
-        const double fx = floor(xc), fy = floor(yc), fz = floor(zc);
-        // cell-centre offsets are formed as (x - floor) - frac in FP32 (exact
-        // integer part), keeping the lever arm accurate to ~1e-7 lattice units
-        a.table[4 * g + 0] = make_float4((float)fx, (float)fy, (float)fz, 0.f);
-        a.table[4 * g + 1] = make_float4((float)(xc - fx), (float)(yc - fy), (float)(zc - fz), 0.f);
-        const double s = a.dt / a.dx;
-        a.table[4 * g + 2] = make_float4((float)(a.vel[3 * g] * s), (float)(a.vel[3 * g + 1] * s),
-                                         (float)(a.vel[3 * g + 2] * s), 0.f);
-        a.table[4 * g + 3] = make_float4((float)(a.omega[3 * g] * a.dt), (float)(a.omega[3 * g + 1] * a.dt),
-                                         (float)(a.omega[3 * g + 2] * a.dt), 0.f);
-    }
+    if (threadIdx.x == 0 && !a.keys_only) particle_table(a, g);
 }
 
 // Exact FP64 sub-cell test, in the reference's operation order
@@ -179,16 +184,16 @@ __global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs
     __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32; w = global cell index
     __shared__ int s_amb[MAP_CHUNK];      // partial cells needing the exact recount (index into s_off)
     __shared__ int s_n, s_na;
-    if (a.moved != nullptr && *a.moved == 0u) return;   // reuse: nothing moved, keys unchanged
     const int g = blockIdx.x;
+    if (a.moved != nullptr && *a.moved == 0u) return;   // reuse: nothing moved, keys unchanged (clear pass ran)
     double xc0, yc0, zc0, r;
     particle_lattice(a, g, xc0, yc0, zc0, r);
     if (threadIdx.x == 0 && blockIdx.y == 0) {
         a.prev[4 * g] = xc0; a.prev[4 * g + 1] = yc0; a.prev[4 * g + 2] = zc0; a.prev[4 * g + 3] = r;
     }
     const double t_out = r + HALF_DIAG, t_in = r - HALF_DIAG;
-    if (!(t_out > 0.0)) return;
-    // the sphere, and in wrap mode its periodic images (block-uniform loop)
+    // the sphere, and in wrap mode its periodic images (block-uniform loop;
+    // none for a radius that reaches no cell centre)
     double shx[2], shy[2], shz[2];
     shx[0] = shy[0] = shz[0] = 0.0;
     int nix = 1, niy = 1, niz = 1;
@@ -197,7 +202,8 @@ __global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs
         niy = image_shifts(a, 1, yc0, t_out, a.ny, shy);
         niz = image_shifts(a, 2, zc0, t_out, a.nz, shz);
     }
-    for (int im = 0; im < nix * niy * niz; ++im) {
+    const int nimg = t_out > 0.0 ? nix * niy * niz : 0;
+    for (int im = 0; im < nimg; ++im) {
         const double xc = xc0 + shx[im % nix], yc = yc0 + shy[(im / nix) % niy], zc = zc0 + shz[im / (nix * niy)];
         const int x0 = max(0, (int)floor(xc - t_out)), x1 = min(a.nx - 1, (int)ceil(xc + t_out));
         const int y0 = max(0, (int)floor(yc - t_out)), y1 = min(a.ny - 1, (int)ceil(yc + t_out));
@@ -331,6 +337,9 @@ __global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs
             __syncthreads();
         }
     }
+    // without a clearing pass the table row and the force reset are written
+    // here, last, where the registers of the claims are free again
+    if (a.table_in_scatter && threadIdx.x == 0 && blockIdx.y == 0) particle_table(a, g);
 }
 
 
@@ -464,6 +473,7 @@ extern "C" int lbdem_psc_map_smooth(const lbdem_lattice *L, lbdem_psc *P, const 
     if (G->n > 0) {
         MapArgs a;
     a.keys_only = 0;
+    a.table_in_scatter = 0;
         a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
         a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;
         a.pos = G->pos; a.radius = G->radius; a.vel = G->vel; a.omega = G->omega;
@@ -506,6 +516,7 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     }
     MapArgs a;
     a.keys_only = 0;
+    a.table_in_scatter = 0;
     a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
     a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;
     a.pos = G->pos; a.radius = G->radius; a.vel = G->vel; a.omega = G->omega;
@@ -537,11 +548,15 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     }
     // fewer particles than about four blocks per SM: split each box over several blocks
     const dim3 sgrid((unsigned)G->n, (unsigned)(G->n >= MAP_SPLIT_BELOW ? 1 : min(16, (MAP_SPLIT_BELOW + G->n - 1) / G->n)));
+    // with nothing to clear or check (keys cleared ahead by lbdem_psc_map_clear,
+    // or the first map) the scatter writes the table itself: one launch
+    const bool clear_pass = a.have_prev || a.moved != nullptr || a.disp_limit > 0.0;
+    a.table_in_scatter = !clear_pass;
     if (a.wrap[0] || a.wrap[1] || a.wrap[2]) {
-        k_map_clear<true><<<G->n, 128, 0, st>>>(a);
+        if (clear_pass) k_map_clear<true><<<G->n, 128, 0, st>>>(a);
         k_map_scatter<true><<<sgrid, 256, 0, st>>>(a);
     } else {
-        k_map_clear<false><<<G->n, 128, 0, st>>>(a);
+        if (clear_pass) k_map_clear<false><<<G->n, 128, 0, st>>>(a);
         k_map_scatter<false><<<sgrid, 256, 0, st>>>(a);
     }
     P->have_prev = 1;
@@ -679,6 +694,7 @@ extern "C" int lbdem_psc_near_blocks(const lbdem_lattice *L, const lbdem_psc *P,
     if (cudaMemsetAsync(near, 0, nblocks, st) != cudaSuccess) return check_launch("near_blocks");
     MapArgs a;
     a.keys_only = 0;
+    a.table_in_scatter = 0;
     memset(&a, 0, sizeof(a));
     a.n = G->n; a.nx = L->nx; a.ny = L->ny; a.nz = L->nz;
     a.dx = P->dx; a.dt = P->dt; a.xmin = P->xmin; a.ymin = P->ymin; a.zmin = P->zmin;
