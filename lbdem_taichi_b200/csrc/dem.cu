@@ -84,12 +84,17 @@ __device__ M3 rot_to_x(const double *a) {
     return R;
 }
 
-constexpr int SLOTS_IN_REGS = 16;   // contact slots whose flags are fetched with the particle state
+constexpr int SLOTS_IN_REGS = 8;    // contact slots whose partners are fetched with the particle state
 
 struct DemArgs {
     lbdem_dem d;
     int ncell;
     int parity;
+    // Hertz constants of a contact, [0] particle-particle, [1] particle-wall
+    // (hertz.py:45-97, 99-153: effective Young's and shear moduli, damping
+    // ratio from the restitution), computed once per launch on the host in the
+    // reference's operation order instead of once per contact
+    double hz_ys[2], hz_gs[2], hz_beta[2];
 };
 
 __device__ __forceinline__ int cell_index(const lbdem_dem &d, int cx_, int cy_, int cz_) {
@@ -128,8 +133,9 @@ __global__ void k_bin(const __grid_constant__ DemArgs A) {
 // ------------------------------- contact laws ------------------------------
 // hertz.py:45-97 / linear.py:43-101 (particle-particle), hertz.py:99-153 /
 // linear.py:103-152 (particle-wall).  `wall` selects the wall variant.
-__device__ void contact_force(const lbdem_dem &d, double rad_i, double mass_i, double rad_j, double mass_j, bool wall,
+__device__ void contact_force(const DemArgs &A, double rad_i, double mass_i, double rad_j, double mass_j, bool wall,
                               double *shear, double delta_n, const double *vc, double *F) {
+    const lbdem_dem &d = A.d;
     const double gap = -1 * delta_n;
     const double dt = d.dt;
     double inc[3] = {vc[0] * dt, vc[1] * dt, vc[2] * dt};
@@ -137,23 +143,17 @@ __device__ void contact_force(const lbdem_dem &d, double rad_i, double mass_i, d
     double kt, gt, F0, mu;
     const int tj = wall ? 1 : 0;
     if (d.model == 0) {
-        const double Ys = 1.0 / ((1.0 - d.nu[0] * d.nu[0]) / d.E[0] + (1.0 - d.nu[tj] * d.nu[tj]) / d.E[tj]);
-        const double Gs = 1.0 / (2.0 * (2.0 - d.nu[0]) * (1.0 + d.nu[0]) / d.E[0] +
-                                 2.0 * (2.0 - d.nu[tj]) * (1.0 + d.nu[tj]) / d.E[tj]);
-        double Rs, ms, e;
+        const double Ys = A.hz_ys[tj], Gs = A.hz_gs[tj], beta = A.hz_beta[tj];
+        double Rs, ms;
         if (wall) {
             Rs = rad_i;
             ms = mass_i;
-            e = d.e[1];
             mu = d.mu[1];
         } else {
             Rs = 1.0 / (1.0 / rad_i + 1.0 / rad_j);
             ms = 1.0 / (1.0 / mass_i + 1.0 / mass_j);
-            e = 0.5 * (d.e[0] + d.e[0]);
             mu = 0.5 * (d.mu[0] + d.mu[0]);
         }
-        const double lne = log(e);
-        const double beta = lne / sqrt(lne * lne + M_PI * M_PI);
         const double Sn = 2.0 * Ys * sqrt(Rs * delta_n);
         const double St = 8.0 * Gs * sqrt(Rs * delta_n);
         const double kn = 4.0 / 3.0 * Ys * sqrt(Rs * delta_n);
@@ -218,8 +218,9 @@ struct PState {
 // forces on j added atomically.  hk: i's first contact slots (the partner of
 // an active slot, -1 for an inactive one) as they were when the sub-step
 // started (only i's lanes touch i's slots, each for its own partner).
-__device__ __forceinline__ void resolve_pair(const lbdem_dem &d, int i, const PState &P, int n_i, const int *hk,
+__device__ __forceinline__ void resolve_pair(const DemArgs &A, int i, const PState &P, int n_i, const int *hk,
                                              int j, double *Fi_acc, double *Mi_acc) {
+    const lbdem_dem &d = A.d;
     const size_t base = (size_t)i * d.maxc;
     // partner state: all loads issued together
     double pj[3], vj[3], wj[3];
@@ -289,7 +290,7 @@ __device__ __forceinline__ void resolve_pair(const lbdem_dem &d, int i, const PS
     }
     mv(R, dvc, vc);
     double F[3];
-    contact_force(d, P.rad, P.mass, rad_j, mass_j, false, sh, delta_n, vc, F);
+    contact_force(A, P.rad, P.mass, rad_j, mass_j, false, sh, delta_n, vc, F);
     for (int t = 0; t < 3; ++t) {
         d.cf_shear[3 * s + t] = sh[t];
         d.cf_force[3 * s + t] = F[t];
@@ -310,7 +311,8 @@ __device__ __forceinline__ void resolve_pair(const lbdem_dem &d, int i, const PS
 }
 
 // evaluate_wall (demsolver.py:742-807)
-__device__ void wall_contact(const lbdem_dem &d, int i, const PState &P, int w, double *Fi_acc, double *Mi_acc) {
+__device__ void wall_contact(const DemArgs &A, int i, const PState &P, int w, double *Fi_acc, double *Mi_acc) {
+    const lbdem_dem &d = A.d;
     const double *nrm = d.wall_n + 3 * w;
     const size_t s = (size_t)i * 6 + w;
     double sh[3] = {d.wcf_shear[3 * s], d.wcf_shear[3 * s + 1], d.wcf_shear[3 * s + 2]};
@@ -328,7 +330,7 @@ __device__ void wall_contact(const lbdem_dem &d, int i, const PState &P, int w, 
     for (int t = 0; t < 3; ++t) m[t] = -(vci[t] + P.v[t]);
     mv(R, m, vc);
     double F[3];
-    contact_force(d, P.rad, P.mass, 0.0, 0.0, true, sh, delta_n, vc, F);
+    contact_force(A, P.rad, P.mass, 0.0, 0.0, true, sh, delta_n, vc, F);
     for (int t = 0; t < 3; ++t) {
         d.wcf_shear[3 * s + t] = sh[t];
         d.wcf_force[3 * s + t] = F[t];
@@ -352,7 +354,8 @@ __device__ void wall_contact(const lbdem_dem &d, int i, const PState &P, int w, 
 // of the warp must call it together (shuffle reduction over groups of 8).
 // WRAP: also probe around the particle's periodic images (lbdem_dem.wrap_pairs).
 template <bool WRAP>
-__device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *count, int tid) {
+__device__ __forceinline__ void contact_lane(const DemArgs &A, const int32_t *count, int tid) {
+    const lbdem_dem &d = A.d;
     const int i = tid >> 3, k = tid & 7;
     const bool act = i < d.n;
     double Fi[3] = {0.0, 0.0, 0.0}, Mi[3] = {0.0, 0.0, 0.0};
@@ -394,7 +397,7 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
                 const int32_t *lst = d.cell_list + (size_t)c * d.cell_cap;
                 for (int t = 0; t < n; ++t) {
                     const int j = lst[t];
-                    if (j > i) resolve_pair(d, i, P, n_i, hk, j, Fi, Mi);
+                    if (j > i) resolve_pair(A, i, P, n_i, hk, j, Fi, Mi);
                 }
             }
         };
@@ -425,11 +428,11 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
             const double sep = -(dot3(P.p, d.wall_n + 3 * w) - d.wall_d[w]);
             if (wact) {
                 if (sep > P.rad) d.wcf_active[s] = 0;
-                else wall_contact(d, i, P, w, Fi, Mi);
+                else wall_contact(A, i, P, w, Fi, Mi);
             } else if (sep <= P.rad) {
                 d.wcf_active[s] = 1;
                 for (int t = 0; t < 3; ++t) d.wcf_shear[3 * s + t] = d.wcf_pos[3 * s + t] = d.wcf_force[3 * s + t] = 0.0;
-                wall_contact(d, i, P, w, Fi, Mi);
+                wall_contact(A, i, P, w, Fi, Mi);
             }
         }
     }
@@ -448,7 +451,7 @@ __device__ __forceinline__ void contact_lane(const lbdem_dem &d, const int32_t *
 
 template <bool WRAP>
 __global__ void __launch_bounds__(128) k_contacts(const __grid_constant__ DemArgs A) {
-    contact_lane<WRAP>(A.d, A.d.cell_count + (size_t)A.parity * A.ncell, blockIdx.x * blockDim.x + threadIdx.x);
+    contact_lane<WRAP>(A, A.d.cell_count + (size_t)A.parity * A.ncell, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // quaternion to rotation matrix (demsolver/utils.py:34-61)
@@ -652,7 +655,7 @@ __global__ void __launch_bounds__(512) k_dem_cluster(const __grid_constant__ Dem
     for (int s = 0; s < nsub; ++s) {
         const int parity = (A.parity + s) & 1;
         const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
-        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(d, count, base + me);
+        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(A, count, base + me);
         cl.sync();
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
@@ -673,7 +676,7 @@ __global__ void __launch_bounds__(128) k_dem_block(const __grid_constant__ DemAr
     for (int s = 0; s < nsub; ++s) {
         const int parity = (A.parity + s) & 1;
         const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
-        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(d, count, base + me);
+        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(A, count, base + me);
         __syncthreads();
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
@@ -728,7 +731,7 @@ __device__ __forceinline__ void grid_barrier(uint32_t *sync, unsigned &gen, int3
 }
 
 template <bool WRAP>
-__global__ void __launch_bounds__(128) k_dem_coop(const __grid_constant__ DemArgs A, int nsub) {
+__global__ void __launch_bounds__(128, 1) k_dem_coop(const __grid_constant__ DemArgs A, int nsub) {
     const lbdem_dem &d = A.d;
     const int nthr = gridDim.x * blockDim.x;
     const int me = blockIdx.x * blockDim.x + threadIdx.x;
@@ -737,12 +740,27 @@ __global__ void __launch_bounds__(128) k_dem_coop(const __grid_constant__ DemArg
     for (int s = 0; s < nsub; ++s) {
         const int parity = (A.parity + s) & 1;
         const int32_t *count = d.cell_count + (size_t)parity * A.ncell;
-        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(d, count, base + me);
+        for (int base = 0; base < nlanes; base += nthr) contact_lane<WRAP>(A, count, base + me);
         grid_barrier(d.sync, gen, d.status);
         int32_t *used = d.cell_count + (size_t)parity * A.ncell;
         for (int c = me; c < A.ncell; c += nthr) used[c] = 0;
         for (int u = me; u < 3 * d.n; u += nthr) integrate_unit(d, A.ncell, parity, u);
         grid_barrier(d.sync, gen, d.status);
+    }
+}
+
+// The per-material Hertz constants of DemArgs, in the operation order of
+// hertz.py:45-97 (particle-particle: the restitution 0.5 (e + e)) and
+// hertz.py:99-153 (particle-wall).
+static void contact_constants(DemArgs &A) {
+    const lbdem_dem &d = A.d;
+    for (int tj = 0; tj < 2; ++tj) {
+        A.hz_ys[tj] = 1.0 / ((1.0 - d.nu[0] * d.nu[0]) / d.E[0] + (1.0 - d.nu[tj] * d.nu[tj]) / d.E[tj]);
+        A.hz_gs[tj] = 1.0 / (2.0 * (2.0 - d.nu[0]) * (1.0 + d.nu[0]) / d.E[0] +
+                             2.0 * (2.0 - d.nu[tj]) * (1.0 + d.nu[tj]) / d.E[tj]);
+        const double e = tj == 0 ? 0.5 * (d.e[0] + d.e[0]) : d.e[1];
+        const double lne = log(e);
+        A.hz_beta[tj] = lne / sqrt(lne * lne + M_PI * M_PI);
     }
 }
 
@@ -806,6 +824,7 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     DemArgs A;
     A.d = *D;
     A.ncell = D->gdim[0] * D->gdim[1] * D->gdim[2];
+    contact_constants(A);
     const int nb_int = max((3 * D->n + 127) / 128, min(148, (A.ncell + 127) / 128));   // 3 units per particle
     const int nb_con = (int)((8ll * D->n + 127) / 128);
     // "cluster": all sub-steps in one launch of a single thread-block cluster

@@ -174,13 +174,15 @@ __device__ __forceinline__ bool subcell_inside_exact(double xc, double yc, doubl
 //     FP32 squared distance lies within 1e-4 (1 + r^2) of r^2 is re-tested
 //     with the reference's exact FP64 expression (|s32 - s64| < 2e-5 (1 + r^2)
 //     for these offsets), so counts are bit-exact.
-constexpr int MAP_CHUNK = 2048;
+constexpr int MAP_CHUNK = 2048;         // box cells classified per round (shared-memory lists)
+constexpr int MAP_THREADS = 256;
+constexpr int MAP_MIN_BLOCKS = 5;       // per SM (46 registers, 40 KB of shared memory each)
 constexpr int MAP_SPLIT_BELOW = 592;   // 148 SMs x 4 blocks
 
 // Five 256-thread blocks per SM (46 registers, 40 KB of shared memory each);
 // the image form keeps four (it would spill at five).
 template <bool WRAP>
-__global__ void __launch_bounds__(256, WRAP ? 4 : 5) k_map_scatter(const MapArgs a) {
+__global__ void __launch_bounds__(MAP_THREADS, WRAP ? 4 : MAP_MIN_BLOCKS) k_map_scatter(const MapArgs a) {
     __shared__ float4 s_off[MAP_CHUNK];   // (xc - i, yc - j, zc - k) in FP32; w = global cell index
     __shared__ int s_amb[MAP_CHUNK];      // partial cells needing the exact recount (index into s_off)
     __shared__ int s_n, s_na;
@@ -554,10 +556,10 @@ extern "C" int lbdem_psc_map(const lbdem_lattice *L, lbdem_psc *P, const lbdem_g
     a.table_in_scatter = !clear_pass;
     if (a.wrap[0] || a.wrap[1] || a.wrap[2]) {
         if (clear_pass) k_map_clear<true><<<G->n, 128, 0, st>>>(a);
-        k_map_scatter<true><<<sgrid, 256, 0, st>>>(a);
+        k_map_scatter<true><<<sgrid, MAP_THREADS, 0, st>>>(a);
     } else {
         if (clear_pass) k_map_clear<false><<<G->n, 128, 0, st>>>(a);
-        k_map_scatter<false><<<sgrid, 256, 0, st>>>(a);
+        k_map_scatter<false><<<sgrid, MAP_THREADS, 0, st>>>(a);
     }
     P->have_prev = 1;
     return check_launch("psc_map");
