@@ -402,7 +402,35 @@ __device__ __forceinline__ void contact_lane(const DemArgs &A, const int32_t *co
             }
         };
         if constexpr (!WRAP) {
-            probe(P.p);
+            // the union of the eight probed cells' lists (own cell + octant, in
+            // the reference's order), shared round-robin by the particle's eight
+            // lanes so that a crowded cell does not make one lane the phase's
+            // last: lane k takes candidates k, k + 8, ... of the concatenation
+            int ijk[3], dd[3];
+            ref_cell(d, P.p, ijk);
+            for (int a = 0; a < 3; ++a) {
+                const double center = (ijk[a] + 0.5) * d.cell_size + d.bp_min[a];
+                dd[a] = (P.p[a] > center) ? 1 : -1;
+            }
+            int cidx[8], pre[8], total = 0;   // cell and exclusive prefix of the counts (static indices only)
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                const int ox = (kk == 1 || kk == 5 || kk == 6 || kk == 7) ? dd[0] : 0;
+                const int oy = (kk == 2 || kk == 4 || kk == 6 || kk == 7) ? dd[1] : 0;
+                const int oz = (kk == 3 || kk == 4 || kk == 5 || kk == 7) ? dd[2] : 0;
+                cidx[kk] = cell_index(d, ijk[0] + ox, ijk[1] + oy, ijk[2] + oz);
+                pre[kk] = total;
+                total += cidx[kk] >= 0 ? min(count[cidx[kk]], d.cell_cap) : 0;
+            }
+            for (int t = k; t < total; t += 8) {
+                // the last probed cell whose first index is <= t holds candidate t
+                int cc = cidx[0], bb = 0;
+#pragma unroll
+                for (int kk = 1; kk < 8; ++kk)
+                    if (t >= pre[kk]) { cc = cidx[kk]; bb = pre[kk]; }
+                const int j = d.cell_list[(size_t)cc * d.cell_cap + (t - bb)];
+                if (j > i) resolve_pair(A, i, P, n_i, hk, j, Fi, Mi);
+            }
         } else {
             // the particle and its periodic images when it lies within one
             // broad-phase cell of a periodic face; the pair geometry is the
