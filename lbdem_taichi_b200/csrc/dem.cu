@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <cooperative_groups.h>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -841,6 +842,36 @@ int lbdem_dem_bin(lbdem_dem *D, void *stream) {
 
 static thread_local int g_dem_launches = 0;
 
+// Cooperative-launch support, SM count and resident blocks per SM of the
+// cooperative kernel (128 threads, no dynamic shared memory) on device `dev`:
+// constant for a device, so looked up once per device and form (the host
+// launch of every call would otherwise repeat three driver queries).
+static bool coop_residency(int dev, bool wrap, const void *kcoop, int &coop, int &nsm, int &per_sm) {
+    constexpr int MAXDEV = 64;
+    static std::mutex mu;
+    static int cached[2][MAXDEV][3];
+    static bool have[2][MAXDEV] = {};
+    if (dev < 0 || dev >= MAXDEV) return false;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!have[wrap][dev]) {
+        int c = 0, n = 0, p = 0;
+        cudaDeviceGetAttribute(&c, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, kcoop, 128, 0) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cached[wrap][dev][0] = c;
+        cached[wrap][dev][1] = n;
+        cached[wrap][dev][2] = p;
+        have[wrap][dev] = true;
+    }
+    coop = cached[wrap][dev][0];
+    nsm = cached[wrap][dev][1];
+    per_sm = cached[wrap][dev][2];
+    return true;
+}
+
 int lbdem_dem_launches_last(void) { return g_dem_launches; }
 
 int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
@@ -912,10 +943,7 @@ int lbdem_dem_substeps(lbdem_dem *D, int32_t nsub, void *stream) {
     if (D->sync && !(mode && strcmp(mode, "split") == 0)) {
         int dev = 0, coop = 0, nsm = 0, per_sm = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kcoop, 128, 0) == cudaSuccess &&
-            per_sm > 0) {
+        if (coop_residency(dev, wrap, (const void *)kcoop, coop, nsm, per_sm) && coop && per_sm > 0) {
             // one resident wave must cover every contact lane: beyond that the
             // grid-stride loop serialises the phases' memory-latency chains and
             // two launches per sub-step (all lanes in flight) are faster

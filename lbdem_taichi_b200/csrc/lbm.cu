@@ -2094,11 +2094,34 @@ static int launch_step_rows(const lbdem_lattice *L, const StepArgs &a, cudaStrea
     const int threads = (int)((PAIRS ? 16u : 32u) * nb) + 32;   // consumers + the producer warp
     int per_sm = 0, dev = 0, nsm = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 2) {
-        cudaGetLastError();
-        return ROWS_NOT_APPLICABLE;
+    {
+        // SM count and resident CTAs per SM for this kernel and CTA size: constant per device,
+        // looked up once (a few entries: CTA sizes differ only with the row width)
+        static std::mutex mu;
+        static int cache[8][4] = {};   // device, threads, nsm, per_sm
+        static int ncache = 0;
+        std::lock_guard<std::mutex> lock(mu);
+        int e = 0;
+        while (e < ncache && !(cache[e][0] == dev && cache[e][1] == threads)) ++e;
+        if (e == ncache) {
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess) {
+                cudaGetLastError();
+                return ROWS_NOT_APPLICABLE;
+            }
+            if (ncache < 8) {
+                cache[ncache][0] = dev;
+                cache[ncache][1] = threads;
+                cache[ncache][2] = nsm;
+                cache[ncache][3] = per_sm;
+                ++ncache;
+            }
+        } else {
+            nsm = cache[e][2];
+            per_sm = cache[e][3];
+        }
     }
+    if (per_sm < 2) return ROWS_NOT_APPLICABLE;
     const int nrows = a.ny * a.nz;
     const int grid = std::min(nrows, nsm * per_sm);
     kern<<<grid, threads, smem, st>>>(a, m);
